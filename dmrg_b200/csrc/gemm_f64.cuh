@@ -1,0 +1,237 @@
+// FP64 / complex128 batched GEMM on the sm_100a FP64 tensor pipe (DMMA, mma.sync.m16n8k4.f64).
+//
+// tcgen05.mma has no f64 kind, so the FP64 tensor path on Blackwell is the warp-level DMMA
+// instruction.  Operands are staged global -> shared through a multistage cp.async pipeline
+// (16-byte copies where the layout allows, zero-fill at the edges), fragments are read from
+// padded shared tiles whose leading dimensions make every fragment load bank-conflict free.
+//
+//   C[b] = alpha * op(A[b]) * op(B[b]) + beta * C[b]      (column-major, BLAS conventions)
+//   op(A) = A (M x K, m contiguous)   or  A^T (A stored K x M, k contiguous)   [TA]
+//   op(B) = B (K x N, k contiguous)   or  B^T (B stored N x K, n contiguous)   [TB]
+//   complex: 4 real DMMAs per fragment pair (4M), optional conjugation of A (CJA).
+#pragma once
+#include "heff_common.cuh"
+
+namespace heff {
+
+struct GemmArgs {
+    int         M, N, K, batch;
+    const void *A;
+    int64_t     lda, sA;
+    const void *B;
+    int64_t     ldb, sB;
+    void       *C;
+    int64_t     ldc, sC;
+    double2     alpha, beta;  // real GEMMs use .x
+};
+
+template<bool CPLX>
+struct GemmTile;
+template<>
+struct GemmTile<false> {
+    static constexpr int BM = 128, BN = 128, BK = 16, WM = 64, WN = 32, STAGES = 3;
+    static constexpr int PAD_MN = 4;  // leading dim == 4 (mod 16) doubles: conflict-free 8-byte fragment loads
+    static constexpr int PAD_K  = 4;
+};
+template<>
+struct GemmTile<true> {
+    static constexpr int BM = 64, BN = 64, BK = 16, WM = 32, WN = 16, STAGES = 3;
+    static constexpr int PAD_MN = 2;  // leading dim == 2 (mod 8) elements: conflict-free 16-byte loads, m/n-major tile
+    static constexpr int PAD_K  = 4;  // leading dim == 4 (mod 8) elements: conflict-free 16-byte loads, k-major tile
+};
+
+template<bool CPLX, bool TA, bool TB>
+struct GemmSmem {
+    using G                  = GemmTile<CPLX>;
+    using T                  = typename Scalar<CPLX>::T;
+    static constexpr int LDA = TA ? (G::BK + G::PAD_K) : (G::BM + G::PAD_MN);  // row length of the A tile
+    static constexpr int LDB = TB ? (G::BN + G::PAD_MN) : (G::BK + G::PAD_K);
+    static constexpr int A_ELEMS = TA ? G::BM * LDA : G::BK * LDA;
+    static constexpr int B_ELEMS = TB ? G::BK * LDB : G::BN * LDB;
+    static constexpr int STAGE   = A_ELEMS + B_ELEMS;
+    static constexpr size_t BYTES = (size_t)STAGE * G::STAGES * sizeof(T);
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template<int BYTES>
+__device__ __forceinline__ void cp_async(uint32_t dst, const void *src, bool valid) {
+    const int n = valid ? BYTES : 0;  // src-size 0 -> destination is zero-filled, nothing is read
+    if constexpr(BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template<int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// One 256-thread CTA computes a BM x BN tile of C.  VEC = elements per cp.async (2 doubles or 1).
+template<bool CPLX, bool TA, bool TB, bool CJA, int VEC>
+__global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const GemmArgs p) {
+    using G  = GemmTile<CPLX>;
+    using SM = GemmSmem<CPLX, TA, TB>;
+    using T  = typename Scalar<CPLX>::T;
+    constexpr int BM = G::BM, BN = G::BN, BK = G::BK, WM = G::WM, WN = G::WN, ST = G::STAGES;
+    constexpr int MT = WM / 16, NT = WN / 8;  // mma tiles per warp
+    constexpr int CPB = CPLX ? 16 : 8 * VEC;  // bytes per copy
+    constexpr int EPC = CPLX ? 1 : VEC;       // elements per copy
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *smem = reinterpret_cast<T *>(smem_raw);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm0 = (warp % (BM / WM)) * WM, wn0 = (warp / (BM / WM)) * WN;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int bz = blockIdx.z;
+    const T  *A  = reinterpret_cast<const T *>(p.A) + (int64_t)bz * p.sA;
+    const T  *B  = reinterpret_cast<const T *>(p.B) + (int64_t)bz * p.sB;
+    T        *C  = reinterpret_cast<T *>(p.C) + (int64_t)bz * p.sC;
+    const int M = p.M, N = p.N, K = p.K;
+    const int KT = (K + BK - 1) / BK;
+
+    auto load_stage = [&](int stage, int kt) {
+        T        *As = smem + stage * SM::STAGE;
+        T        *Bs = As + SM::A_ELEMS;
+        const int k0 = kt * BK;
+        // A tile
+        constexpr int A_CHUNKS = BM * BK / EPC;
+#pragma unroll
+        for(int c = tid; c < A_CHUNKS; c += 256) {
+            int mm, kk;
+            if constexpr(!TA) {
+                kk = c / (BM / EPC);
+                mm = (c % (BM / EPC)) * EPC;
+            } else {
+                mm = c / (BK / EPC);
+                kk = (c % (BK / EPC)) * EPC;
+            }
+            const int  gm = m0 + mm, gk = k0 + kk;
+            const bool v  = (gm < M) && (gk < K);
+            const T   *src = v ? (TA ? A + gk + (int64_t)gm * p.lda : A + gm + (int64_t)gk * p.lda) : A;
+            T         *dst = TA ? As + mm * SM::LDA + kk : As + kk * SM::LDA + mm;
+            cp_async<CPB>(smem_u32(dst), src, v);
+        }
+        constexpr int B_CHUNKS = BN * BK / EPC;
+#pragma unroll
+        for(int c = tid; c < B_CHUNKS; c += 256) {
+            int nn, kk;
+            if constexpr(!TB) {
+                nn = c / (BK / EPC);
+                kk = (c % (BK / EPC)) * EPC;
+            } else {
+                kk = c / (BN / EPC);
+                nn = (c % (BN / EPC)) * EPC;
+            }
+            const int  gn = n0 + nn, gk = k0 + kk;
+            const bool v  = (gn < N) && (gk < K);
+            const T   *src = v ? (TB ? B + gn + (int64_t)gk * p.ldb : B + gk + (int64_t)gn * p.ldb) : B;
+            T         *dst = TB ? Bs + kk * SM::LDB + nn : Bs + nn * SM::LDB + kk;
+            cp_async<CPB>(smem_u32(dst), src, v);
+        }
+    };
+
+    double acc[MT][NT][CPLX ? 2 : 1][4];
+#pragma unroll
+    for(int i = 0; i < MT; i++)
+#pragma unroll
+        for(int j = 0; j < NT; j++)
+#pragma unroll
+            for(int c = 0; c < (CPLX ? 2 : 1); c++)
+#pragma unroll
+                for(int r = 0; r < 4; r++) acc[i][j][c][r] = 0.0;
+
+#pragma unroll
+    for(int s = 0; s < ST - 1; s++) {
+        if(s < KT) load_stage(s, s);
+        cp_async_commit();
+    }
+
+    for(int kt = 0; kt < KT; kt++) {
+        cp_async_wait<ST - 2>();
+        __syncthreads();
+        {
+            const int nk = kt + ST - 1;
+            if(nk < KT) load_stage(nk % ST, nk);
+            cp_async_commit();
+        }
+        const T *As = smem + (kt % ST) * SM::STAGE;
+        const T *Bs = As + SM::A_ELEMS;
+#pragma unroll
+        for(int k4 = 0; k4 < BK; k4 += 4) {
+            T a[MT][2], b[NT];
+#pragma unroll
+            for(int i = 0; i < MT; i++) {
+                const int mr = wm0 + i * 16 + g;
+                if constexpr(TA) {
+                    a[i][0] = As[mr * SM::LDA + k4 + t];
+                    a[i][1] = As[(mr + 8) * SM::LDA + k4 + t];
+                } else {
+                    a[i][0] = As[(k4 + t) * SM::LDA + mr];
+                    a[i][1] = As[(k4 + t) * SM::LDA + mr + 8];
+                }
+            }
+#pragma unroll
+            for(int j = 0; j < NT; j++) {
+                const int nc = wn0 + j * 8 + g;
+                if constexpr(TB)
+                    b[j] = Bs[(k4 + t) * SM::LDB + nc];
+                else
+                    b[j] = Bs[nc * SM::LDB + k4 + t];
+            }
+#pragma unroll
+            for(int i = 0; i < MT; i++)
+#pragma unroll
+                for(int j = 0; j < NT; j++) {
+                    if constexpr(!CPLX) {
+                        dmma(acc[i][j][0], a[i][0], a[i][1], b[j]);
+                    } else {
+                        const double ai0 = CJA ? -a[i][0].y : a[i][0].y, ai1 = CJA ? -a[i][1].y : a[i][1].y;
+                        dmma(acc[i][j][0], a[i][0].x, a[i][1].x, b[j].x);  // re += ar*br
+                        dmma(acc[i][j][0], -ai0, -ai1, b[j].y);           // re -= ai*bi
+                        dmma(acc[i][j][1], a[i][0].x, a[i][1].x, b[j].y);  // im += ar*bi
+                        dmma(acc[i][j][1], ai0, ai1, b[j].x);             // im += ai*br
+                    }
+                }
+        }
+    }
+    cp_async_wait<0>();
+
+    // Epilogue: C = alpha*acc + beta*C (C is not read when beta == 0).
+    const bool use_beta = (p.beta.x != 0.0) || (p.beta.y != 0.0);
+#pragma unroll
+    for(int i = 0; i < MT; i++)
+#pragma unroll
+        for(int j = 0; j < NT; j++)
+#pragma unroll
+            for(int r = 0; r < 4; r++) {
+                const int gm = m0 + wm0 + i * 16 + g + ((r >> 1) << 3);
+                const int gn = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+                if(gm < M && gn < N) {
+                    T *cp = C + gm + (int64_t)gn * p.ldc;
+                    if constexpr(!CPLX) {
+                        double v = p.alpha.x * acc[i][j][0][r];
+                        if(use_beta) v += p.beta.x * (*cp);
+                        *cp = v;
+                    } else {
+                        double2 v = cmul(p.alpha, make_double2(acc[i][j][0][r], acc[i][j][1][r]));
+                        if(use_beta) v = cadd(v, cmul(p.beta, *cp));
+                        *cp = v;
+                    }
+                }
+            }
+}
+
+// Host launcher.  Returns HEFF_OK or a status code; never synchronises.
+template<bool CPLX>
+int gemm_f64(bool ta, bool tb, bool cja, const GemmArgs &args, cudaStream_t stream);
+
+}  // namespace heff

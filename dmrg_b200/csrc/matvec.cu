@@ -1,0 +1,326 @@
+// H_eff * theta: layout kernels, MPO mixing kernel, matvec driver, expectation value,
+// and the stateless C entry points heff_matvec_{d,z} / heff_expval_{d,z}.
+#include "matvec.cuh"
+#include "runtime.cuh"
+
+namespace heff {
+
+int check_matvec_dims(const int64_t md[3], const int64_t wd[4], const int64_t ld[3], const int64_t rd[3], MatvecDims &d) {
+    if(!md || !wd || !ld || !rd) return HEFF_BAD_ARG;
+    d = MatvecDims{md[0], md[1], md[2], wd[0], wd[1]};
+    // contraction_tblis.cpp:230-234
+    if(md[1] != ld[0] || md[2] != rd[0] || md[0] != wd[2] || ld[2] != wd[0] || rd[2] != wd[1]) {
+        set_last_error_msg("matvec: dimension mismatch mps [%lld,%lld,%lld] mpo [%lld,%lld,%lld,%lld] envL [%lld,%lld,%lld] envR [%lld,%lld,%lld]",
+                           (long long)md[0], (long long)md[1], (long long)md[2], (long long)wd[0], (long long)wd[1], (long long)wd[2],
+                           (long long)wd[3], (long long)ld[0], (long long)ld[1], (long long)ld[2], (long long)rd[0], (long long)rd[1],
+                           (long long)rd[2]);
+        return HEFF_BAD_SHAPE;
+    }
+    if(wd[3] != wd[2] || ld[1] != ld[0] || rd[1] != rd[0]) {
+        set_last_error_msg("matvec: mpo must be [mL,mR,d,d] and envs [chi,chi,m]");
+        return HEFF_BAD_SHAPE;
+    }
+    if(d.S <= 0 || d.cL <= 0 || d.cR <= 0 || d.DL <= 0 || d.DR <= 0) return HEFF_BAD_SHAPE;
+    if(d.S > 64 || d.DL * d.S > 256 || d.DR * d.S > 256) {
+        set_last_error_msg("matvec: spin*mpo bond dimension above 256 is not supported");
+        return HEFF_BAD_SHAPE;
+    }
+    if(d.cL > (1 << 20) || d.cR > (1 << 20)) return HEFF_BAD_SHAPE;
+    return HEFF_OK;
+}
+
+// x'[a + cL*(s + S*b)] = x[s + S*(a + cL*b)]   (output-linear: coalesced writes)
+template<class T>
+__global__ void permute_mps_kernel(const T *__restrict__ x, T *__restrict__ xp, int64_t S, int64_t cL, int64_t n) {
+    for(int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < n; o += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = o % cL, r = o / cL, s = r % S, b = r / S;
+        xp[o]           = x[s + S * (a + cL * b)];
+    }
+}
+
+// R'[b + cR*n + cR*DR*b'] = R[b + cR*(b' + cR*n)]
+template<class T>
+__global__ void permute_R_kernel(const T *__restrict__ R, T *__restrict__ Rp, int64_t cR, int64_t DR, int64_t n) {
+    for(int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < n; o += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = o % cR, r = o / cR, nn = r % DR, bp = r / DR;
+        Rp[o]           = R[b + cR * (bp + cR * nn)];
+    }
+}
+
+__device__ __forceinline__ bool is_zero(double w) { return w == 0.0; }
+__device__ __forceinline__ bool is_zero(double2 w) { return w.x == 0.0 && w.y == 0.0; }
+__device__ __forceinline__ double fma_s(double w, double v, double acc) { return fma(w, v, acc); }
+__device__ __forceinline__ double2 fma_s(double2 w, double2 v, double2 acc) {
+    return make_double2(fma(w.x, v.x, fma(-w.y, v.y, acc.x)), fma(w.x, v.y, fma(w.y, v.x, acc.y)));
+}
+__device__ __forceinline__ void zero(double &v) { v = 0.0; }
+__device__ __forceinline__ void zero(double2 &v) { v = make_double2(0.0, 0.0); }
+
+// T2[(s' + S a') + S cL (b + cR n)] = sum_{m,s} W[m + DL(n + DR(s + S s'))] T1[(a' + cL m) + cL DL (s + S b)]
+// One CTA: 128 consecutive a' at one b.  W and the CTA's T1 column block are staged in shared memory;
+// zero MPO entries (most of them for Ising-type MPOs) are skipped with a warp-uniform branch.
+constexpr int MIX_THREADS = 128;
+template<class T>
+__global__ void __launch_bounds__(MIX_THREADS) mix_kernel(const T *__restrict__ T1, T *__restrict__ T2, const T *__restrict__ W, int S, int cL,
+                                                         int cR, int DL, int DR) {
+    extern __shared__ __align__(16) unsigned char mix_smem[];
+    T        *sW  = reinterpret_cast<T *>(mix_smem);
+    const int nW  = DL * DR * S * S;
+    T        *sIn = sW + nW;
+    for(int i = threadIdx.x; i < nW; i += blockDim.x) sW[i] = W[i];
+    const int     b   = blockIdx.y;
+    const int     ap  = blockIdx.x * MIX_THREADS + threadIdx.x;
+    const bool    act = ap < cL;
+    const int64_t cLD = (int64_t)cL * DL;
+    for(int s = 0; s < S; s++)
+        for(int m = 0; m < DL; m++) {
+            T v;
+            zero(v);
+            if(act) v = T1[(ap + (int64_t)cL * m) + cLD * (s + (int64_t)S * b)];
+            sIn[(m * S + s) * MIX_THREADS + threadIdx.x] = v;
+        }
+    __syncthreads();
+    if(!act) return;
+    T acc[16];
+    for(int n = 0; n < DR; n++) {
+        for(int sp0 = 0; sp0 < S; sp0 += 16) {
+            const int ns = min(16, S - sp0);
+            for(int q = 0; q < ns; q++) zero(acc[q]);
+            for(int q = 0; q < ns; q++) {
+                const int sp = sp0 + q;
+                for(int s = 0; s < S; s++)
+                    for(int m = 0; m < DL; m++) {
+                        const T w = sW[m + DL * (n + DR * (s + S * sp))];
+                        if(!is_zero(w)) acc[q] = fma_s(w, sIn[(m * S + s) * MIX_THREADS + threadIdx.x], acc[q]);
+                    }
+            }
+            T *out = T2 + (sp0 + (int64_t)S * ap) + (int64_t)S * cL * (b + (int64_t)cR * n);
+            for(int q = 0; q < ns; q++) out[q] = acc[q];
+        }
+    }
+}
+
+static int grid_1d(int64_t n) {
+    int64_t g = (n + 255) / 256;
+    int64_t cap = (int64_t)device_sm_count() * 16;
+    return (int)(g < cap ? (g > 0 ? g : 1) : cap);
+}
+
+template<bool CPLX>
+int permute_R(const typename Scalar<CPLX>::T *R, typename Scalar<CPLX>::T *Rp, const MatvecDims &d, cudaStream_t s) {
+    const int64_t n = d.size_Rp();
+    permute_R_kernel<<<grid_1d(n), 256, 0, s>>>(R, Rp, d.cR, d.DR, n);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+static int launch_mix(const MatvecDims &d, const typename Scalar<CPLX>::T *T1, typename Scalar<CPLX>::T *T2, const typename Scalar<CPLX>::T *W,
+                      cudaStream_t s) {
+    using T           = typename Scalar<CPLX>::T;
+    const size_t smem = sizeof(T) * ((size_t)d.DL * d.DR * d.S * d.S + (size_t)d.DL * d.S * MIX_THREADS);
+    if(smem > 200 * 1024) return HEFF_BAD_SHAPE;
+    static int attr_done[64] = {0};
+    int        dev           = 0;
+    HEFF_CUDA(cudaGetDevice(&dev));
+    if(dev < 0 || dev >= 64 || !attr_done[dev]) {
+        HEFF_CUDA(cudaFuncSetAttribute(mix_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        if(dev >= 0 && dev < 64) attr_done[dev] = 1;
+    }
+    if(d.cR > 65535) return HEFF_BAD_SHAPE;
+    dim3 grid((unsigned)cdiv(d.cL, MIX_THREADS), (unsigned)d.cR);
+    mix_kernel<T><<<grid, MIX_THREADS, smem, s>>>(T1, T2, W, (int)d.S, (int)d.cL, (int)d.cR, (int)d.DL, (int)d.DR);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename Scalar<CPLX>::T *y, const typename Scalar<CPLX>::T *L,
+                const typename Scalar<CPLX>::T *Rp, const typename Scalar<CPLX>::T *W, const MatvecScratch<CPLX> &ws, cudaStream_t s) {
+    const int64_t n = d.size_mps();
+    permute_mps_kernel<<<grid_1d(n), 256, 0, s>>>(x, ws.xp, d.S, d.cL, n);
+    HEFF_LAUNCH_CHECK();
+    GemmArgs g1{};
+    g1.M     = (int)(d.cL * d.DL);
+    g1.N     = (int)(d.S * d.cR);
+    g1.K     = (int)d.cL;
+    g1.batch = 1;
+    g1.A     = L;
+    g1.lda   = d.cL;
+    g1.B     = ws.xp;
+    g1.ldb   = d.cL;
+    g1.C     = ws.T1;
+    g1.ldc   = d.cL * d.DL;
+    g1.alpha = make_double2(1.0, 0.0);
+    g1.beta  = make_double2(0.0, 0.0);
+    HEFF_TRY(gemm_f64<CPLX>(/*ta=*/true, /*tb=*/false, false, g1, s));
+    HEFF_TRY(launch_mix<CPLX>(d, ws.T1, ws.T2, W, s));
+    GemmArgs g2{};
+    g2.M     = (int)(d.S * d.cL);
+    g2.N     = (int)d.cR;
+    g2.K     = (int)(d.cR * d.DR);
+    g2.batch = 1;
+    g2.A     = ws.T2;
+    g2.lda   = d.S * d.cL;
+    g2.B     = Rp;
+    g2.ldb   = d.cR * d.DR;
+    g2.C     = y;
+    g2.ldc   = d.S * d.cL;
+    g2.alpha = make_double2(1.0, 0.0);
+    g2.beta  = make_double2(0.0, 0.0);
+    HEFF_TRY(gemm_f64<CPLX>(false, false, false, g2, s));
+    return HEFF_OK;
+}
+
+// ---- deterministic dot product ----
+constexpr int DOT_BLOCKS = 1024;
+template<bool CPLX>
+__global__ void dot_partial_kernel(const typename Scalar<CPLX>::T *__restrict__ x, const typename Scalar<CPLX>::T *__restrict__ y, int64_t n,
+                                   double *partials) {
+    __shared__ double sre[256], sim[256];
+    double            re = 0, im = 0;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if constexpr(CPLX) {
+            double2 a = x[i], b = y[i];
+            re += a.x * b.x + a.y * b.y;  // conj(a) * b
+            im += a.x * b.y - a.y * b.x;
+        } else {
+            re += x[i] * y[i];
+        }
+    }
+    sre[threadIdx.x] = re;
+    sim[threadIdx.x] = im;
+    __syncthreads();
+    for(int w = 128; w > 0; w >>= 1) {
+        if(threadIdx.x < w) {
+            sre[threadIdx.x] += sre[threadIdx.x + w];
+            sim[threadIdx.x] += sim[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) {
+        partials[blockIdx.x]              = sre[0];
+        partials[DOT_BLOCKS + blockIdx.x] = sim[0];
+    }
+}
+template<bool CPLX>
+__global__ void dot_final_kernel(const double *partials, int nb, typename Scalar<CPLX>::T *out) {
+    __shared__ double sre[256], sim[256];
+    double            re = 0, im = 0;
+    for(int i = threadIdx.x; i < nb; i += 256) {
+        re += partials[i];
+        im += partials[DOT_BLOCKS + i];
+    }
+    sre[threadIdx.x] = re;
+    sim[threadIdx.x] = im;
+    __syncthreads();
+    for(int w = 128; w > 0; w >>= 1) {
+        if(threadIdx.x < w) {
+            sre[threadIdx.x] += sre[threadIdx.x + w];
+            sim[threadIdx.x] += sim[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) {
+        if constexpr(CPLX)
+            *out = make_double2(sre[0], sim[0]);
+        else
+            *out = sre[0];
+    }
+}
+
+template<bool CPLX>
+int dot_device(const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T *y, int64_t n, typename Scalar<CPLX>::T *out, double *partials,
+               cudaStream_t s) {
+    int nb = (int)std::min<int64_t>(DOT_BLOCKS, std::max<int64_t>(1, (n + 255) / 256));
+    dot_partial_kernel<CPLX><<<nb, 256, 0, s>>>(x, y, n, partials);
+    HEFF_LAUNCH_CHECK();
+    dot_final_kernel<CPLX><<<1, 256, 0, s>>>(partials, nb, out);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template int permute_R<false>(const double *, double *, const MatvecDims &, cudaStream_t);
+template int permute_R<true>(const double2 *, double2 *, const MatvecDims &, cudaStream_t);
+template int matvec_fp64<false>(const MatvecDims &, const double *, double *, const double *, const double *, const double *,
+                                const MatvecScratch<false> &, cudaStream_t);
+template int matvec_fp64<true>(const MatvecDims &, const double2 *, double2 *, const double2 *, const double2 *, const double2 *,
+                               const MatvecScratch<true> &, cudaStream_t);
+template int dot_device<false>(const double *, const double *, int64_t, double *, double *, cudaStream_t);
+template int dot_device<true>(const double2 *, const double2 *, int64_t, double2 *, double *, cudaStream_t);
+
+// ---- stateless entry points ----
+template<bool CPLX>
+static int matvec_stateless(void *res, const void *mps, const int64_t md[3], const void *mpo, const int64_t wd[4], const void *envL,
+                            const int64_t ld[3], const void *envR, const int64_t rd[3], cudaStream_t s) {
+    using T = typename Scalar<CPLX>::T;
+    MatvecDims d;
+    HEFF_TRY(check_matvec_dims(md, wd, ld, rd, d));
+    if(!res || !mps || !mpo || !envL || !envR) return HEFF_BAD_ARG;
+    if(res == mps) {
+        set_last_error_msg("matvec: res must not alias mps");
+        return HEFF_BAD_ARG;
+    }
+    const int64_t elems = MatvecScratch<CPLX>::elems(d) + d.size_Rp();
+    void         *base  = nullptr;
+    HEFF_TRY(stream_workspace(s, (size_t)elems * sizeof(T), &base));
+    MatvecScratch<CPLX> ws;
+    T                  *Rp = ws.carve(reinterpret_cast<T *>(base), d);
+    HEFF_TRY(permute_R<CPLX>(reinterpret_cast<const T *>(envR), Rp, d, s));
+    return matvec_fp64<CPLX>(d, reinterpret_cast<const T *>(mps), reinterpret_cast<T *>(res), reinterpret_cast<const T *>(envL), Rp,
+                             reinterpret_cast<const T *>(mpo), ws, s);
+}
+
+template<bool CPLX>
+static int expval_stateless(double *result, const void *mps, const int64_t md[3], const void *mpo, const int64_t wd[4], const void *envL,
+                            const int64_t ld[3], const void *envR, const int64_t rd[3], cudaStream_t s) {
+    using T = typename Scalar<CPLX>::T;
+    MatvecDims d;
+    HEFF_TRY(check_matvec_dims(md, wd, ld, rd, d));
+    if(!result || !mps || !mpo || !envL || !envR) return HEFF_BAD_ARG;
+    const int64_t extra = MatvecScratch<CPLX>::pad(d.size_Rp()) + MatvecScratch<CPLX>::pad(d.size_mps()) + 1;
+    const int64_t elems = MatvecScratch<CPLX>::elems(d) + extra;
+    void         *base  = nullptr;
+    HEFF_TRY(stream_workspace(s, (size_t)elems * sizeof(T) + 2 * DOT_BLOCKS * sizeof(double), &base));
+    MatvecScratch<CPLX> ws;
+    T      *Rp       = ws.carve(reinterpret_cast<T *>(base), d);
+    T      *y        = Rp + MatvecScratch<CPLX>::pad(d.size_Rp());
+    T      *dres     = y + d.size_mps();
+    double *partials = reinterpret_cast<double *>(dres + 1);
+    HEFF_TRY(permute_R<CPLX>(reinterpret_cast<const T *>(envR), Rp, d, s));
+    HEFF_TRY(matvec_fp64<CPLX>(d, reinterpret_cast<const T *>(mps), y, reinterpret_cast<const T *>(envL), Rp, reinterpret_cast<const T *>(mpo),
+                               ws, s));
+    HEFF_TRY(dot_device<CPLX>(reinterpret_cast<const T *>(mps), y, d.size_mps(), dres, partials, s));
+    T h;
+    HEFF_CUDA(cudaMemcpyAsync(&h, dres, sizeof(T), cudaMemcpyDeviceToHost, s));
+    HEFF_CUDA(cudaStreamSynchronize(s));
+    if constexpr(CPLX) {
+        result[0] = h.x;
+        result[1] = h.y;
+    } else {
+        result[0] = h;
+        result[1] = 0.0;
+    }
+    return HEFF_OK;
+}
+
+}  // namespace heff
+
+using namespace heff;
+
+extern "C" int heff_matvec_d(double *res, const double *mps, const int64_t mps_dims[3], const double *mpo, const int64_t mpo_dims[4],
+                             const double *envL, const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3], void *stream) {
+    return matvec_stateless<false>(res, mps, mps_dims, mpo, mpo_dims, envL, envL_dims, envR, envR_dims, (cudaStream_t)stream);
+}
+extern "C" int heff_matvec_z(heff_z *res, const heff_z *mps, const int64_t mps_dims[3], const heff_z *mpo, const int64_t mpo_dims[4],
+                             const heff_z *envL, const int64_t envL_dims[3], const heff_z *envR, const int64_t envR_dims[3], void *stream) {
+    return matvec_stateless<true>(res, mps, mps_dims, mpo, mpo_dims, envL, envL_dims, envR, envR_dims, (cudaStream_t)stream);
+}
+extern "C" int heff_expval_d(double *result, const double *mps, const int64_t mps_dims[3], const double *mpo, const int64_t mpo_dims[4],
+                             const double *envL, const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3], void *stream) {
+    return expval_stateless<false>(result, mps, mps_dims, mpo, mpo_dims, envL, envL_dims, envR, envR_dims, (cudaStream_t)stream);
+}
+extern "C" int heff_expval_z(double *result, const heff_z *mps, const int64_t mps_dims[3], const heff_z *mpo, const int64_t mpo_dims[4],
+                             const heff_z *envL, const int64_t envL_dims[3], const heff_z *envR, const int64_t envR_dims[3], void *stream) {
+    return expval_stateless<true>(result, mps, mps_dims, mpo, mpo_dims, envL, envL_dims, envR, envR_dims, (cudaStream_t)stream);
+}

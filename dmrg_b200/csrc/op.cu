@@ -1,0 +1,228 @@
+// heff_op: the MatVecMPOS<T> / MatVecMPO<T> operator object behind the C ABI
+// (source/math/eig/matvec/matvec_mpos.h:23-180, matvec_mpos.cpp:40-130, 963-984).
+#include <cstring>
+#include <vector>
+
+#include "matvec.cuh"
+#include "op.cuh"
+#include "runtime.cuh"
+
+namespace heff {
+
+// Merge site MPOs like matvec_mpos.cpp:104-119:
+//   W2[mL, mR', s1 + dA*s2, t1 + dA*t2] = sum_c WA[mL, c, s1, t1] WB[c, mR', s2, t2]
+template<class T>
+static void merge_two(std::vector<T> &out, int64_t od[4], const std::vector<T> &A, const int64_t da[4], const std::vector<T> &B, const int64_t db[4]) {
+    const int64_t mL = da[0], c = da[1], sA = da[2], tA = da[3], mR = db[1], sB = db[2], tB = db[3];
+    const int64_t S = sA * sB, TT = tA * tB;
+    out.assign((size_t)(mL * mR * S * TT), T{});
+    for(int64_t t2 = 0; t2 < tB; t2++)
+        for(int64_t t1 = 0; t1 < tA; t1++)
+            for(int64_t s2 = 0; s2 < sB; s2++)
+                for(int64_t s1 = 0; s1 < sA; s1++)
+                    for(int64_t n = 0; n < mR; n++)
+                        for(int64_t m = 0; m < mL; m++) {
+                            T acc{};
+                            for(int64_t k = 0; k < c; k++) {
+                                const T &a = A[m + mL * (k + c * (s1 + sA * t1))];
+                                const T &b = B[k + db[0] * (n + mR * (s2 + sB * t2))];
+                                acc        = acc + a * b;
+                            }
+                            out[m + mL * (n + mR * ((s1 + sA * s2) + S * (t1 + tA * t2)))] = acc;
+                        }
+    od[0] = mL;
+    od[1] = mR;
+    od[2] = S;
+    od[3] = TT;
+}
+
+struct HostC {
+    double re = 0, im = 0;
+    HostC() = default;
+    HostC(double r, double i) : re(r), im(i) {}
+    HostC operator+(const HostC &o) const { return {re + o.re, im + o.im}; }
+    HostC operator*(const HostC &o) const { return {re * o.re - im * o.im, re * o.im + im * o.re}; }
+};
+
+template<bool CPLX>
+static int create_impl(heff_op **out, int nsites, const void *const *mpos, const int64_t *mdims, const void *envL, const int64_t ld[3],
+                       const void *envR, const int64_t rd[3], heff_mem where, heff_precision prec, cudaStream_t stream) {
+    using T  = typename Scalar<CPLX>::T;
+    using HT = typename std::conditional<CPLX, HostC, double>::type;
+    static_assert(sizeof(HT) == sizeof(T), "host/device scalar size");
+    if(!out || nsites < 1 || nsites > 5 || !mpos || !mdims || !envL || !envR || !ld || !rd) return HEFF_BAD_ARG;
+    // --- gather the site MPOs on the host and merge them (setup only, tiny) ---
+    std::vector<HT> W;
+    int64_t         wd[4];
+    for(int i = 0; i < nsites; i++) {
+        const int64_t *di = mdims + 4 * i;
+        if(di[0] <= 0 || di[1] <= 0 || di[2] <= 0 || di[3] <= 0 || di[2] != di[3]) return HEFF_BAD_SHAPE;
+        size_t          n = (size_t)(di[0] * di[1] * di[2] * di[3]);
+        std::vector<HT> Wi(n);
+        if(where == HEFF_MEM_HOST)
+            std::memcpy(Wi.data(), mpos[i], n * sizeof(HT));
+        else {
+            HEFF_CUDA(cudaMemcpyAsync(Wi.data(), mpos[i], n * sizeof(HT), cudaMemcpyDeviceToHost, stream));
+            HEFF_CUDA(cudaStreamSynchronize(stream));
+        }
+        if(i == 0) {
+            W = std::move(Wi);
+            std::memcpy(wd, di, sizeof(wd));
+        } else {
+            if(wd[1] != di[0]) return HEFF_BAD_SHAPE;
+            std::vector<HT> M2;
+            int64_t         nd[4];
+            merge_two(M2, nd, W, wd, Wi, di);
+            W = std::move(M2);
+            std::memcpy(wd, nd, sizeof(wd));
+        }
+    }
+    const int64_t md[3] = {wd[2], ld[0], rd[0]};
+    MatvecDims    d;
+    HEFF_TRY(check_matvec_dims(md, wd, ld, rd, d));
+
+    heff_op *op   = new heff_op();
+    op->cplx      = CPLX;
+    op->d         = d;
+    op->precision = prec;
+    op->stream    = stream;
+    std::memcpy(op->mpo_dims, wd, sizeof(wd));
+    const size_t es   = sizeof(T);
+    auto         fail = [&](int rc) {
+        heff_op_destroy(op);
+        return rc;
+    };
+    // device buffers: L (reference layout), R' (permuted), W, scratch, staging for host MultAx
+    const int64_t nL = d.cL * d.cL * d.DL, nR = d.size_Rp(), nW = wd[0] * wd[1] * wd[2] * wd[3];
+    if(cudaMalloc(&op->L, nL * es) != cudaSuccess) return fail(HEFF_OOM);
+    if(cudaMalloc(&op->Rp, nR * es) != cudaSuccess) return fail(HEFF_OOM);
+    if(cudaMalloc(&op->W, nW * es) != cudaSuccess) return fail(HEFF_OOM);
+    const int64_t nscr = MatvecScratch<CPLX>::elems(d);
+    if(cudaMalloc(&op->scratch, nscr * es) != cudaSuccess) return fail(HEFF_OOM);
+    op->scratch_bytes = (size_t)nscr * es;
+    void *Rtmp        = nullptr;
+    if(cudaMalloc(&Rtmp, nR * es) != cudaSuccess) return fail(HEFF_OOM);
+    const cudaMemcpyKind kind = (where == HEFF_MEM_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    cudaError_t          e    = cudaMemcpyAsync(op->L, envL, nL * es, kind, stream);
+    if(e == cudaSuccess) e = cudaMemcpyAsync(Rtmp, envR, nR * es, kind, stream);
+    if(e == cudaSuccess) e = cudaMemcpyAsync(op->W, W.data(), nW * es, cudaMemcpyHostToDevice, stream);
+    if(e != cudaSuccess) {
+        cudaFree(Rtmp);
+        set_last_cuda_error(e, "heff_op_create copies", __FILE__, __LINE__);
+        return fail(HEFF_CUDA_ERROR);
+    }
+    int rc = permute_R<CPLX>(reinterpret_cast<const T *>(Rtmp), reinterpret_cast<T *>(op->Rp), d, stream);
+    e      = cudaStreamSynchronize(stream);  // W's host vector and Rtmp must outlive the copies
+    cudaFree(Rtmp);
+    if(rc != HEFF_OK) return fail(rc);
+    if(e != cudaSuccess) {
+        set_last_cuda_error(e, "heff_op_create sync", __FILE__, __LINE__);
+        return fail(HEFF_CUDA_ERROR);
+    }
+    *out = op;
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+static int apply_impl(heff_op *op, const void *x, void *y) {
+    using T = typename Scalar<CPLX>::T;
+    if(x == y) {
+        set_last_error_msg("MultAx: in and out must not alias");
+        return HEFF_BAD_ARG;
+    }
+    MatvecScratch<CPLX> ws;
+    ws.carve(reinterpret_cast<T *>(op->scratch), op->d);
+    HEFF_TRY(matvec_fp64<CPLX>(op->d, reinterpret_cast<const T *>(x), reinterpret_cast<T *>(y), reinterpret_cast<const T *>(op->L),
+                               reinterpret_cast<const T *>(op->Rp), reinterpret_cast<const T *>(op->W), ws, op->stream));
+    op->num_mv++;
+    return HEFF_OK;
+}
+
+int op_apply(heff_op *op, const void *x, void *y) {
+    if(!op || !x || !y) return HEFF_BAD_ARG;
+    if(op->precision == HEFF_PREC_MIXED && op->mixed_apply) return op->mixed_apply(op, x, y);
+    return op->cplx ? apply_impl<true>(op, x, y) : apply_impl<false>(op, x, y);
+}
+
+}  // namespace heff
+
+using namespace heff;
+
+extern "C" int heff_op_create(heff_op **op, heff_dtype dtype, int nsites, const void *const *mpos, const int64_t *mpo_dims, const void *envL,
+                              const int64_t envL_dims[3], const void *envR, const int64_t envR_dims[3], heff_mem where, heff_precision precision,
+                              void *stream) {
+    if(dtype == HEFF_F64)
+        return create_impl<false>(op, nsites, mpos, mpo_dims, envL, envL_dims, envR, envR_dims, where, precision, (cudaStream_t)stream);
+    if(dtype == HEFF_C128)
+        return create_impl<true>(op, nsites, mpos, mpo_dims, envL, envL_dims, envR, envR_dims, where, precision, (cudaStream_t)stream);
+    return HEFF_BAD_ARG;
+}
+
+extern "C" int heff_op_destroy(heff_op *op) {
+    if(!op) return HEFF_OK;
+    if(op->destroy_hook) op->destroy_hook(op);
+    if(op->L) cudaFree(op->L);
+    if(op->Rp) cudaFree(op->Rp);
+    if(op->W) cudaFree(op->W);
+    if(op->scratch) cudaFree(op->scratch);
+    if(op->stage_x) cudaFree(op->stage_x);
+    delete op;
+    return HEFF_OK;
+}
+
+extern "C" int64_t heff_op_rows(const heff_op *op) { return op ? op->d.size_mps() : -1; }
+
+extern "C" int heff_op_shape(const heff_op *op, int64_t shape[3]) {
+    if(!op || !shape) return HEFF_BAD_ARG;
+    shape[0] = op->d.S;
+    shape[1] = op->d.cL;
+    shape[2] = op->d.cR;
+    return HEFF_OK;
+}
+
+extern "C" int heff_op_multax(heff_op *op, const void *x, void *y) { return op_apply(op, x, y); }
+extern "C" int heff_perform_op(heff_op *op, const void *x, void *y) { return op_apply(op, x, y); }
+
+extern "C" int heff_op_multax_block(heff_op *op, const void *x, int64_t ldx, void *y, int64_t ldy, int block_size) {
+    if(!op || !x || !y || block_size < 0) return HEFF_BAD_ARG;
+    const int64_t n  = op->d.size_mps();
+    const size_t  es = op->cplx ? 16 : 8;
+    if(ldx < n || ldy < n) return HEFF_BAD_SHAPE;
+    for(int i = 0; i < block_size; i++) {
+        const char *xi = reinterpret_cast<const char *>(x) + (size_t)ldx * i * es;
+        char       *yi = reinterpret_cast<char *>(y) + (size_t)ldy * i * es;
+        HEFF_TRY(op_apply(op, xi, yi));
+    }
+    return HEFF_OK;
+}
+
+extern "C" int heff_op_multax_host(heff_op *op, const void *x_host, void *y_host) {
+    if(!op || !x_host || !y_host) return HEFF_BAD_ARG;
+    const int64_t n     = op->d.size_mps();
+    const size_t  bytes = (size_t)n * (op->cplx ? 16 : 8);
+    if(!op->stage_x) {
+        HEFF_CUDA(cudaMalloc(&op->stage_x, 2 * bytes + 256));
+    }
+    void *dx = op->stage_x;
+    void *dy = reinterpret_cast<char *>(op->stage_x) + ((bytes + 255) / 256) * 256;
+    HEFF_CUDA(cudaMemcpyAsync(dx, x_host, bytes, cudaMemcpyHostToDevice, op->stream));
+    HEFF_TRY(op_apply(op, dx, dy));
+    HEFF_CUDA(cudaMemcpyAsync(y_host, dy, bytes, cudaMemcpyDeviceToHost, op->stream));
+    HEFF_CUDA(cudaStreamSynchronize(op->stream));
+    return HEFF_OK;
+}
+
+extern "C" int heff_op_set_stream(heff_op *op, void *stream) {
+    if(!op) return HEFF_BAD_ARG;
+    op->stream = (cudaStream_t)stream;
+    return HEFF_OK;
+}
+
+extern "C" int heff_op_set_precision(heff_op *op, heff_precision precision) {
+    if(!op) return HEFF_BAD_ARG;
+    if(precision != HEFF_PREC_FP64 && precision != HEFF_PREC_MIXED) return HEFF_BAD_ARG;
+    op->precision = precision;
+    return HEFF_OK;
+}
+
+extern "C" int64_t heff_op_num_mv(const heff_op *op) { return op ? op->num_mv : -1; }
