@@ -79,6 +79,8 @@ def lib():
         _sig(L, "heff_op_set_stream", ctypes.c_int, [_P, _P])
         _sig(L, "heff_op_set_precision", ctypes.c_int, [_P, ctypes.c_int])
         _sig(L, "heff_op_num_mv", _I64, [_P])
+        _sig(L, "heff_op_set_profiling", ctypes.c_int, [_P, ctypes.c_int])
+        _sig(L, "heff_op_stage_times", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), _I64P, ctypes.c_int])
         _lib = L
         _extend_signatures(L)
     return _lib
@@ -204,6 +206,16 @@ class MatVecMPOS:
 
     def set_precision(self, precision):
         check(lib().heff_op_set_precision(self.handle, int(precision)), "set_precision")
+
+    def set_profiling(self, enable=True):
+        check(lib().heff_op_set_profiling(self.handle, int(bool(enable))), "set_profiling")
+
+    def stage_times(self, reset=False):
+        """Summed milliseconds of (layout, GEMM1, mix, GEMM2) over profiled matvecs, and their count."""
+        ms = (ctypes.c_double * 4)()
+        cnt = ctypes.c_int64(0)
+        check(lib().heff_op_stage_times(self.handle, ms, ctypes.byref(cnt), int(bool(reset))), "stage_times")
+        return list(ms), int(cnt.value)
 
     @property
     def num_mv(self):

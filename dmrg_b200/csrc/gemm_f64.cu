@@ -15,7 +15,9 @@ static int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
         HEFF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::BYTES));
         if(dev >= 0 && dev < 64) attr_done[dev] = 1;
     }
-    dim3 grid((unsigned)cdiv(a.M, G::BM), (unsigned)cdiv(a.N, G::BN), (unsigned)a.batch);
+    const int64_t tiles = cdiv(a.M, G::BM) * cdiv(a.N, G::BN);
+    if(tiles > 0x7fffffffLL) return HEFF_BAD_SHAPE;
+    dim3 grid((unsigned)tiles, 1u, (unsigned)a.batch);
     kern<<<grid, 256, SM::BYTES, stream>>>(a);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;

@@ -52,6 +52,8 @@ struct GemmSmem {
     static constexpr size_t BYTES = (size_t)STAGE * G::STAGES * sizeof(T);
 };
 
+constexpr int GROUP_M = 16;  // row panels per rasterisation group
+
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 template<int BYTES>
@@ -90,7 +92,18 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const GemmArgs p) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wm0 = (warp % (BM / WM)) * WM, wn0 = (warp / (BM / WM)) * WN;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // Grouped rasterisation: consecutive CTAs walk GROUP_M row panels for every column panel, so the
+    // CTAs resident at one time share their A and B panels in L2 instead of re-reading them from HBM.
+    int tile_m, tile_n;
+    {
+        const int num_m = (p.M + BM - 1) / BM, num_n = (p.N + BN - 1) / BN;
+        const int pid = blockIdx.x, per_group = GROUP_M * num_n;
+        const int first_m = (pid / per_group) * GROUP_M;
+        const int gsize   = min(num_m - first_m, GROUP_M);
+        tile_m            = first_m + (pid % per_group) % gsize;
+        tile_n            = (pid % per_group) / gsize;
+    }
+    const int m0 = tile_m * BM, n0 = tile_n * BN;
     const int bz = blockIdx.z;
     const T  *A  = reinterpret_cast<const T *>(p.A) + (int64_t)bz * p.sA;
     const T  *B  = reinterpret_cast<const T *>(p.B) + (int64_t)bz * p.sB;

@@ -136,10 +136,13 @@ static int launch_mix(const MatvecDims &d, const typename Scalar<CPLX>::T *T1, t
 
 template<bool CPLX>
 int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename Scalar<CPLX>::T *y, const typename Scalar<CPLX>::T *L,
-                const typename Scalar<CPLX>::T *Rp, const typename Scalar<CPLX>::T *W, const MatvecScratch<CPLX> &ws, cudaStream_t s) {
+                const typename Scalar<CPLX>::T *Rp, const typename Scalar<CPLX>::T *W, const MatvecScratch<CPLX> &ws, cudaStream_t s,
+                cudaEvent_t *ev) {
     const int64_t n = d.size_mps();
+    if(ev) HEFF_CUDA(cudaEventRecord(ev[0], s));
     permute_mps_kernel<<<grid_1d(n), 256, 0, s>>>(x, ws.xp, d.S, d.cL, n);
     HEFF_LAUNCH_CHECK();
+    if(ev) HEFF_CUDA(cudaEventRecord(ev[1], s));
     GemmArgs g1{};
     g1.M     = (int)(d.cL * d.DL);
     g1.N     = (int)(d.S * d.cR);
@@ -154,7 +157,9 @@ int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename
     g1.alpha = make_double2(1.0, 0.0);
     g1.beta  = make_double2(0.0, 0.0);
     HEFF_TRY(gemm_f64<CPLX>(/*ta=*/true, /*tb=*/false, false, g1, s));
+    if(ev) HEFF_CUDA(cudaEventRecord(ev[2], s));
     HEFF_TRY(launch_mix<CPLX>(d, ws.T1, ws.T2, W, s));
+    if(ev) HEFF_CUDA(cudaEventRecord(ev[3], s));
     GemmArgs g2{};
     g2.M     = (int)(d.S * d.cL);
     g2.N     = (int)d.cR;
@@ -169,6 +174,7 @@ int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename
     g2.alpha = make_double2(1.0, 0.0);
     g2.beta  = make_double2(0.0, 0.0);
     HEFF_TRY(gemm_f64<CPLX>(false, false, false, g2, s));
+    if(ev) HEFF_CUDA(cudaEventRecord(ev[4], s));
     return HEFF_OK;
 }
 
@@ -243,9 +249,9 @@ int dot_device(const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T
 template int permute_R<false>(const double *, double *, const MatvecDims &, cudaStream_t);
 template int permute_R<true>(const double2 *, double2 *, const MatvecDims &, cudaStream_t);
 template int matvec_fp64<false>(const MatvecDims &, const double *, double *, const double *, const double *, const double *,
-                                const MatvecScratch<false> &, cudaStream_t);
+                                const MatvecScratch<false> &, cudaStream_t, cudaEvent_t *);
 template int matvec_fp64<true>(const MatvecDims &, const double2 *, double2 *, const double2 *, const double2 *, const double2 *,
-                               const MatvecScratch<true> &, cudaStream_t);
+                               const MatvecScratch<true> &, cudaStream_t, cudaEvent_t *);
 template int dot_device<false>(const double *, const double *, int64_t, double *, double *, cudaStream_t);
 template int dot_device<true>(const double2 *, const double2 *, int64_t, double2 *, double *, cudaStream_t);
 

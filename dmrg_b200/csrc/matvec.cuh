@@ -44,9 +44,11 @@ struct MatvecScratch {
 };
 
 // y = H_eff x with pre-permuted R'.  L and W in reference layout.  Launches 4 kernels on s.
+// ev (optional): 5 events recorded before P and after P, G1, MIX, G2 (stage timing).
 template<bool CPLX>
 int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename Scalar<CPLX>::T *y, const typename Scalar<CPLX>::T *L,
-                const typename Scalar<CPLX>::T *Rp, const typename Scalar<CPLX>::T *W, const MatvecScratch<CPLX> &ws, cudaStream_t s);
+                const typename Scalar<CPLX>::T *Rp, const typename Scalar<CPLX>::T *W, const MatvecScratch<CPLX> &ws, cudaStream_t s,
+                cudaEvent_t *ev = nullptr);
 
 // Deterministic dot product sum_i conj(x_i) y_i (conj only for complex) into a device scalar.
 template<bool CPLX>

@@ -123,6 +123,28 @@ static int create_impl(heff_op **out, int nsites, const void *const *mpos, const
     return HEFF_OK;
 }
 
+int op_prof_flush(heff_op *op) {
+    if(op->prof_used == 0) return HEFF_OK;
+    HEFF_CUDA(cudaStreamSynchronize(op->stream));
+    for(int k = 0; k < op->prof_used; k++) {
+        cudaEvent_t *e = op->prof_events.data() + 5 * k;
+        for(int st = 0; st < 4; st++) {
+            float ms = 0;
+            HEFF_CUDA(cudaEventElapsedTime(&ms, e[st], e[st + 1]));
+            op->prof_ms[st] += ms;
+        }
+        op->prof_count++;
+    }
+    op->prof_used = 0;
+    return HEFF_OK;
+}
+
+cudaEvent_t *op_prof_slot(heff_op *op) {
+    if(!op->profiling || op->prof_cap == 0) return nullptr;
+    if(op->prof_used == op->prof_cap && op_prof_flush(op) != HEFF_OK) return nullptr;
+    return op->prof_events.data() + 5 * (op->prof_used++);
+}
+
 template<bool CPLX>
 static int apply_impl(heff_op *op, const void *x, void *y) {
     using T = typename Scalar<CPLX>::T;
@@ -133,7 +155,7 @@ static int apply_impl(heff_op *op, const void *x, void *y) {
     MatvecScratch<CPLX> ws;
     ws.carve(reinterpret_cast<T *>(op->scratch), op->d);
     HEFF_TRY(matvec_fp64<CPLX>(op->d, reinterpret_cast<const T *>(x), reinterpret_cast<T *>(y), reinterpret_cast<const T *>(op->L),
-                               reinterpret_cast<const T *>(op->Rp), reinterpret_cast<const T *>(op->W), ws, op->stream));
+                               reinterpret_cast<const T *>(op->Rp), reinterpret_cast<const T *>(op->W), ws, op->stream, op_prof_slot(op)));
     op->num_mv++;
     return HEFF_OK;
 }
@@ -161,6 +183,7 @@ extern "C" int heff_op_create(heff_op **op, heff_dtype dtype, int nsites, const 
 extern "C" int heff_op_destroy(heff_op *op) {
     if(!op) return HEFF_OK;
     if(op->destroy_hook) op->destroy_hook(op);
+    for(cudaEvent_t e : op->prof_events) cudaEventDestroy(e);
     if(op->L) cudaFree(op->L);
     if(op->Rp) cudaFree(op->Rp);
     if(op->W) cudaFree(op->W);
@@ -226,3 +249,27 @@ extern "C" int heff_op_set_precision(heff_op *op, heff_precision precision) {
 }
 
 extern "C" int64_t heff_op_num_mv(const heff_op *op) { return op ? op->num_mv : -1; }
+
+extern "C" int heff_op_set_profiling(heff_op *op, int enable) {
+    if(!op) return HEFF_BAD_ARG;
+    if(enable && op->prof_cap == 0) {
+        op->prof_cap = 1024;
+        op->prof_events.resize(5 * op->prof_cap);
+        for(auto &e : op->prof_events) HEFF_CUDA(cudaEventCreate(&e));
+    }
+    if(!enable) HEFF_TRY(op_prof_flush(op));
+    op->profiling = enable != 0;
+    return HEFF_OK;
+}
+
+extern "C" int heff_op_stage_times(heff_op *op, double ms[4], int64_t *count, int reset) {
+    if(!op || !ms) return HEFF_BAD_ARG;
+    HEFF_TRY(op_prof_flush(op));
+    for(int i = 0; i < 4; i++) ms[i] = op->prof_ms[i];
+    if(count) *count = op->prof_count;
+    if(reset) {
+        for(int i = 0; i < 4; i++) op->prof_ms[i] = 0;
+        op->prof_count = 0;
+    }
+    return HEFF_OK;
+}

@@ -1,5 +1,7 @@
 // Internal definition of the heff_op operator object (opaque in include/heff.h).
 #pragma once
+#include <vector>
+
 #include "matvec.cuh"
 
 struct heff_op {
@@ -13,6 +15,12 @@ struct heff_op {
     size_t             scratch_bytes = 0;
     void              *stage_x       = nullptr;  // device staging for MultAx with host buffers
     int64_t            num_mv        = 0;
+    // stage profiling (heff_op_set_profiling): ring of 5-event sets, summed on query
+    bool               profiling     = false;
+    std::vector<cudaEvent_t> prof_events;  // 5 * prof_cap
+    int                prof_cap      = 0, prof_used = 0;
+    double             prof_ms[4]    = {0, 0, 0, 0};
+    int64_t            prof_count    = 0;
     // mixed-precision state (owned by the mixed path; null until first use)
     void              *mixed         = nullptr;
     int (*mixed_apply)(heff_op *, const void *, void *) = nullptr;
@@ -21,4 +29,6 @@ struct heff_op {
 
 namespace heff {
 int op_apply(heff_op *op, const void *x, void *y);
+int op_prof_flush(heff_op *op);  // synchronises the op's stream and folds recorded events into prof_ms
+cudaEvent_t *op_prof_slot(heff_op *op);  // next free 5-event set or nullptr (profiling off)
 }

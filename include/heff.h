@@ -104,6 +104,12 @@ int heff_op_set_stream(heff_op *op, void *stream);
 int heff_op_set_precision(heff_op *op, heff_precision precision);
 /* Number of matvecs applied so far (MatVecMPOS::num_mv). */
 int64_t heff_op_num_mv(const heff_op *op);
+/* Stage timing (the reference's tid:: timers around MultAx, matvec_mpo.h:70-102):
+ * when enabled, every FP64 matvec records CUDA events around its four kernels
+ * (layout, GEMM 1, MPO mix, GEMM 2).  heff_op_stage_times synchronises the op's
+ * stream and returns the summed milliseconds per stage and the matvec count. */
+int heff_op_set_profiling(heff_op *op, int enable);
+int heff_op_stage_times(heff_op *op, double ms[4], int64_t *count, int reset);
 
 #ifdef __cplusplus
 }
