@@ -61,6 +61,19 @@ int heff_matvec_d(double *res, const double *mps, const int64_t mps_dims[3], con
 int heff_matvec_z(heff_z *res, const heff_z *mps, const int64_t mps_dims[3], const heff_z *mpo, const int64_t mpo_dims[4], const heff_z *envL,
                   const int64_t envL_dims[3], const heff_z *envR, const int64_t envR_dims[3], void *stream);
 
+/* Same product and arguments as heff_matvec_d, but allocating no device memory.
+ * No counterpart in the reference: it exists for callers that cannot let a
+ * library call cudaMalloc (a process that has already split all device memory
+ * among its own pools, or that cannot afford the device-wide synchronisation a
+ * cudaMalloc/cudaFree implies).  Scratch comes from one fixed 32 MiB array
+ * inside the library (held on every GPU that loads the library until exit);
+ * calls needing more return HEFF_BAD_SHAPE (real two-site D=3 fits up to about
+ * chi=360).  All calls on a device share that array: calls that may overlap on
+ * the GPU race, so serialise them.  The first call on a device looks up the
+ * array's device address; make it before any stream capture. */
+int heff_matvec_d_noalloc(double *res, const double *mps, const int64_t mps_dims[3], const double *mpo, const int64_t mpo_dims[4],
+                          const double *envL, const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3], void *stream);
+
 /* <mps| mpo |mps> with environments.  Replaces
  * tools::common::contraction::expectation_value (contraction.h:18-22,
  * contraction_tblis.cpp:30-87).  result is a HOST pointer: result[0]=re,
