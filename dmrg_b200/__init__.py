@@ -157,6 +157,75 @@ def expectation_value(mps, mps_dims, mpo, mpo_dims, envL, envL_dims, envR, envR_
     return complex(out[0], out[1]) if cplx else float(out[0])
 
 
+def env_update(side, out, env, env_dims, mps, mps_dims, mpo, mpo_dims, stream=None):
+    """EnvBase::build_block (EnvBase.cpp:67-151) on device tensors; side 'L' or 'R'."""
+    cplx = mps.is_complex()
+    fn = lib().heff_env_update_z if cplx else lib().heff_env_update_d
+    sd = 0 if side in ("L", 0) else 1
+    rc = fn(sd, ptr(out), ptr(env), dims(env_dims), ptr(mps), dims(mps_dims), ptr(mpo), dims(mpo_dims), _stream_handle(stream))
+    check(rc, "heff_env_update")
+    return out
+
+
+def svd(A, rows, cols, rank_max=0, trunc_lim=1e-12, stream=None):
+    """svd::solver::do_svd_ptr + truncation (svd.cpp:113-206, 257-280) on a device matrix.
+
+    Returns (U [rows x k], S [k], VT [k x cols]) as flat device tensors plus (k, truncation_error)."""
+    torch = _torch()
+    kmax = min(rows, cols, rank_max if rank_max > 0 else rows * cols)
+    U = torch.empty(rows * kmax, dtype=torch.float64, device=A.device)
+    S = torch.empty(kmax, dtype=torch.float64, device=A.device)
+    VT = torch.empty(kmax * cols, dtype=torch.float64, device=A.device)
+    k = ctypes.c_int64(0)
+    err = ctypes.c_double(0)
+    check(lib().heff_svd_d(ptr(A), rows, cols, rank_max, trunc_lim, ptr(U), ptr(S), ptr(VT), ctypes.byref(k), ctypes.byref(err),
+                           _stream_handle(stream)), "heff_svd_d")
+    k = int(k.value)
+    return U[: rows * k], S[:k], VT[: k * cols], k, float(err.value)
+
+
+def schmidt_multisite(theta, dL, dR, chiL, chiR, rank_max=0, trunc_lim=1e-12, stream=None):
+    """svd::solver::schmidt_multisite (svd.h:189-220): returns U [dL,chiL,k], S [k] (unit norm), V [dR,k,chiR]
+    as flat device tensors, and (k, truncation_error)."""
+    torch = _torch()
+    m, n = dL * chiL, dR * chiR
+    kmax = min(m, n, rank_max if rank_max > 0 else m * n)
+    U = torch.empty(m * kmax, dtype=torch.float64, device=theta.device)
+    S = torch.empty(kmax, dtype=torch.float64, device=theta.device)
+    V = torch.empty(kmax * n, dtype=torch.float64, device=theta.device)
+    k = ctypes.c_int64(0)
+    err = ctypes.c_double(0)
+    check(lib().heff_schmidt_d(ptr(theta), dL, dR, chiL, chiR, rank_max, trunc_lim, ptr(U), ptr(S), ptr(V), ctypes.byref(k), ctypes.byref(err),
+                               _stream_handle(stream)), "heff_schmidt_d")
+    k = int(k.value)
+    return U[: m * k], S[:k], V[: k * n], k, float(err.value)
+
+
+def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, precision=PREC_FP64, seed=0, ritz="SA", target=0.0,
+          energy_shift_per_site=0.0, stream=None):
+    """Two-site DMRG of the random-field Ising chain on the device (heff_dmrg_run); returns the result dict."""
+    from ._sigs import DmrgConfig, DmrgResult
+
+    hs = np.ascontiguousarray(np.asarray(h, dtype=np.float64))
+    cfg = DmrgConfig()
+    lib().heff_dmrg_config_default(ctypes.byref(cfg))
+    cfg.L = len(hs)
+    cfg.J = J
+    cfg.h = hs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    cfg.chi_max = chi_max
+    cfg.sweeps = sweeps
+    cfg.trunc_lim = trunc_lim
+    cfg.eig_tol = eig_tol
+    cfg.precision = precision
+    cfg.seed = seed
+    cfg.ritz = {"SA": 0, "LA": 1, "TARGET": 2}[ritz]
+    cfg.target = target
+    cfg.energy_shift_per_site = energy_shift_per_site
+    res = DmrgResult()
+    check(lib().heff_dmrg_run(ctypes.byref(cfg), ctypes.byref(res), _stream_handle(stream)), "heff_dmrg_run")
+    return res.as_dict()
+
+
 class MatVecMPOS:
     """MatVecMPOS<T> (matvec_mpos.h:23-180): operator object handed to an eigensolver.
 
@@ -216,6 +285,26 @@ class MatVecMPOS:
         cnt = ctypes.c_int64(0)
         check(lib().heff_op_stage_times(self.handle, ms, ctypes.byref(cnt), int(bool(reset))), "stage_times")
         return list(ms), int(cnt.value)
+
+    def eigs(self, x0=None, x_out=None, ritz="SA", target=0.0, tol=1e-12, mixed=True, **kw):
+        """Eigenpair through the device Davidson solver (heff_eigs).  x0/x_out: device tensors or None.
+        Returns (eigval, result dict); raises on errors other than non-convergence."""
+        from ._sigs import EigConfig, EigResult
+
+        cfg = EigConfig()
+        lib().heff_eig_config_default(ctypes.byref(cfg))
+        cfg.ritz = {"SA": 0, "LA": 1, "TARGET": 2}[ritz]
+        cfg.target = float(target)
+        cfg.tol = float(tol)
+        cfg.mixed = int(bool(mixed))
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        res = EigResult()
+        rc = lib().heff_eigs(self.handle, ctypes.byref(cfg), ptr(x0) if x0 is not None else None, ptr(x_out) if x_out is not None else None,
+                             ctypes.byref(res))
+        if rc not in (HEFF_OK, 5):
+            check(rc, "heff_eigs")
+        return res.eigval, res.as_dict()
 
     @property
     def num_mv(self):

@@ -1,0 +1,190 @@
+// Tall-skinny vector kernels for the eigensolver (see blas1.cuh).  All reductions run in a fixed
+// order (per-block partial sums, then one block), so results do not depend on scheduling: the same
+// eigensolve gives bit-identical output alone or next to other work on the device.
+#include "blas1.cuh"
+
+namespace heff {
+
+__device__ __forceinline__ double cj_mul_re(double a, double b) { return a * b; }
+template<class T>
+struct VOps;
+template<>
+struct VOps<double> {
+    static __device__ __forceinline__ void dot_acc(double &re, double &im, double v, double t) { re = fma(v, t, re); }
+    static __device__ __forceinline__ double axpy(double acc, double v, double h) { return fma(v, h, acc); }
+    static __device__ __forceinline__ double zero() { return 0.0; }
+    static __device__ __forceinline__ double scale(double x, double a) { return x * a; }
+    static __device__ __forceinline__ double make(double re, double) { return re; }
+    static __device__ __forceinline__ double addscaled(double y, double a, double x) { return fma(a, x, y); }
+};
+template<>
+struct VOps<double2> {
+    static __device__ __forceinline__ void dot_acc(double &re, double &im, double2 v, double2 t) {
+        re = fma(v.x, t.x, fma(v.y, t.y, re));  // conj(v) * t
+        im = fma(v.x, t.y, fma(-v.y, t.x, im));
+    }
+    static __device__ __forceinline__ double2 axpy(double2 acc, double2 v, double2 h) {
+        return make_double2(fma(v.x, h.x, fma(-v.y, h.y, acc.x)), fma(v.x, h.y, fma(v.y, h.x, acc.y)));
+    }
+    static __device__ __forceinline__ double2 zero() { return make_double2(0, 0); }
+    static __device__ __forceinline__ double2 scale(double2 x, double a) { return make_double2(x.x * a, x.y * a); }
+    static __device__ __forceinline__ double2 make(double re, double im) { return make_double2(re, im); }
+    static __device__ __forceinline__ double2 addscaled(double2 y, double a, double2 x) { return make_double2(fma(a, x.x, y.x), fma(a, x.y, y.y)); }
+};
+
+// partials[(blk * k + j) * 2 + {0,1}]
+template<class T>
+__global__ void __launch_bounds__(256) multi_dot_partial(const T *__restrict__ V, int64_t ldv, int64_t n, int k, const T *__restrict__ t,
+                                                        double *__restrict__ partials) {
+    __shared__ double sre[8][MD_MAXK], sim[8][MD_MAXK];
+    const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for(int j0 = 0; j0 < k; j0 += 32) {
+        const int jn = min(32, k - j0);
+        double    re[32], im[32];
+#pragma unroll
+        for(int q = 0; q < 32; q++) re[q] = im[q] = 0.0;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            const T tv = t[i];
+#pragma unroll
+            for(int q = 0; q < 32; q++)
+                if(q < jn) VOps<T>::dot_acc(re[q], im[q], V[i + ldv * (j0 + q)], tv);
+        }
+#pragma unroll
+        for(int q = 0; q < 32; q++) {
+            double a = re[q], b = im[q];
+            for(int o = 16; o > 0; o >>= 1) {
+                a += __shfl_xor_sync(0xffffffffu, a, o);
+                b += __shfl_xor_sync(0xffffffffu, b, o);
+            }
+            if(lane == 0 && q < jn) {
+                sre[warp][j0 + q] = a;
+                sim[warp][j0 + q] = b;
+            }
+        }
+    }
+    __syncthreads();
+    for(int j = threadIdx.x; j < k; j += blockDim.x) {
+        double a = 0, b = 0;
+        for(int w = 0; w < 8; w++) {
+            a += sre[w][j];
+            b += sim[w][j];
+        }
+        partials[((int64_t)blockIdx.x * k + j) * 2 + 0] = a;
+        partials[((int64_t)blockIdx.x * k + j) * 2 + 1] = b;
+    }
+}
+
+template<class T>
+__global__ void multi_dot_final(const double *__restrict__ partials, int nb, int k, T *__restrict__ h) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if(j >= k) return;
+    double a = 0, b = 0;
+    for(int blk = 0; blk < nb; blk++) {
+        a += partials[((int64_t)blk * k + j) * 2 + 0];
+        b += partials[((int64_t)blk * k + j) * 2 + 1];
+    }
+    h[j] = VOps<T>::make(a, b);
+}
+
+template<class T>
+__global__ void multi_axpy_kernel(const T *__restrict__ V, int64_t ldv, int64_t n, int k, const T *__restrict__ h, double alpha, T *__restrict__ t) {
+    extern __shared__ __align__(16) unsigned char hsm[];
+    T *sh = reinterpret_cast<T *>(hsm);
+    for(int j = threadIdx.x; j < k; j += blockDim.x) sh[j] = h[j];
+    __syncthreads();
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T acc = VOps<T>::zero();
+        for(int j = 0; j < k; j++) acc = VOps<T>::axpy(acc, V[i + ldv * j], sh[j]);
+        t[i] = VOps<T>::addscaled(t[i], alpha, acc);
+    }
+}
+
+template<class T>
+__global__ void combine_kernel(const T *__restrict__ V, int64_t ldv, int64_t n, int k, const T *__restrict__ c, T *__restrict__ x) {
+    extern __shared__ __align__(16) unsigned char csm[];
+    T *sc = reinterpret_cast<T *>(csm);
+    for(int j = threadIdx.x; j < k; j += blockDim.x) sc[j] = c[j];
+    __syncthreads();
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T acc = VOps<T>::zero();
+        for(int j = 0; j < k; j++) acc = VOps<T>::axpy(acc, V[i + ldv * j], sc[j]);
+        x[i] = acc;
+    }
+}
+
+template<class T>
+__global__ void scale_kernel(T *__restrict__ x, int64_t n, const double *__restrict__ a, bool inv_sqrt) {
+    const double v = inv_sqrt ? (a[0] > 0 ? rsqrt(a[0]) : 0.0) : a[0];
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] = VOps<T>::scale(x[i], v);
+}
+
+template<class T>
+__global__ void residual_kernel(const T *__restrict__ ax, const T *__restrict__ x, double theta, T *__restrict__ r, int64_t n) {
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        r[i] = VOps<T>::addscaled(ax[i], -theta, x[i]);
+}
+
+static int grid_for(int64_t n, int cap_per_sm = 8) {
+    int64_t g = (n + 255) / 256, cap = (int64_t)device_sm_count() * cap_per_sm;
+    return (int)(g < 1 ? 1 : (g < cap ? g : cap));
+}
+
+template<bool CPLX>
+int multi_dot(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *t, typename Scalar<CPLX>::T *h,
+              double *partials, cudaStream_t s) {
+    using T = typename Scalar<CPLX>::T;
+    if(k <= 0) return HEFF_OK;
+    if(k > MD_MAXK) return HEFF_BAD_ARG;
+    const int nb = (int)std::min<int64_t>(MD_BLOCKS, std::max<int64_t>(1, (n + 255) / 256));
+    multi_dot_partial<T><<<nb, 256, 0, s>>>(V, ldv, n, k, t, partials);
+    HEFF_LAUNCH_CHECK();
+    multi_dot_final<T><<<(k + 127) / 128, 128, 0, s>>>(partials, nb, k, h);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+int multi_axpy(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *h, double alpha,
+               typename Scalar<CPLX>::T *t, cudaStream_t s) {
+    using T = typename Scalar<CPLX>::T;
+    if(k <= 0) return HEFF_OK;
+    multi_axpy_kernel<T><<<grid_for(n), 256, sizeof(T) * k, s>>>(V, ldv, n, k, h, alpha, t);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+int combine(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *c, typename Scalar<CPLX>::T *x,
+            cudaStream_t s) {
+    using T = typename Scalar<CPLX>::T;
+    combine_kernel<T><<<grid_for(n), 256, sizeof(T) * std::max(k, 1), s>>>(V, ldv, n, k, c, x);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+int scale_dev(typename Scalar<CPLX>::T *x, int64_t n, const double *a, bool inv_sqrt, cudaStream_t s) {
+    scale_kernel<typename Scalar<CPLX>::T><<<grid_for(n), 256, 0, s>>>(x, n, a, inv_sqrt);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+int residual(const typename Scalar<CPLX>::T *ax, const typename Scalar<CPLX>::T *x, double theta, typename Scalar<CPLX>::T *r, int64_t n,
+             cudaStream_t s) {
+    residual_kernel<typename Scalar<CPLX>::T><<<grid_for(n), 256, 0, s>>>(ax, x, theta, r, n);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+#define INST(C)                                                                                                                              \
+    template int multi_dot<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, double *, cudaStream_t);   \
+    template int multi_axpy<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, double, Scalar<C>::T *, cudaStream_t);   \
+    template int combine<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, cudaStream_t);              \
+    template int scale_dev<C>(Scalar<C>::T *, int64_t, const double *, bool, cudaStream_t);                                             \
+    template int residual<C>(const Scalar<C>::T *, const Scalar<C>::T *, double, Scalar<C>::T *, int64_t, cudaStream_t);
+INST(false)
+INST(true)
+#undef INST
+
+}  // namespace heff

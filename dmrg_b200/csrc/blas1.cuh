@@ -1,0 +1,30 @@
+// Deterministic level-1/"tall-skinny" vector kernels for the eigensolver (FP64, real or complex):
+//   multi_dot:  h[j]  = sum_i conj(V[i,j]) t[i]        (j < k)     two-pass, fixed reduction order
+//   multi_axpy: t[i] += alpha * sum_j V[i,j] h[j]
+//   combine:    x[i]  = sum_j V[i,j] c[j]
+#pragma once
+#include "heff_common.cuh"
+
+namespace heff {
+
+constexpr int MD_BLOCKS = 512;  // partial-sum rows of multi_dot
+constexpr int MD_MAXK   = 128;  // max columns handled by one multi_dot call
+
+template<bool CPLX>
+int multi_dot(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *t, typename Scalar<CPLX>::T *h,
+              double *partials /* >= MD_BLOCKS * MD_MAXK * 2 doubles */, cudaStream_t s);
+template<bool CPLX>
+int multi_axpy(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *h, double alpha,
+               typename Scalar<CPLX>::T *t, cudaStream_t s);
+template<bool CPLX>
+int combine(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *c, typename Scalar<CPLX>::T *x,
+            cudaStream_t s);
+// x *= a (real scalar a read from device memory: a = *scale_dev, or 1/sqrt(*scale_dev) when inv_sqrt)
+template<bool CPLX>
+int scale_dev(typename Scalar<CPLX>::T *x, int64_t n, const double *scale_dev, bool inv_sqrt, cudaStream_t s);
+// y = x - theta*z  (residual), theta real on the host
+template<bool CPLX>
+int residual(const typename Scalar<CPLX>::T *ax, const typename Scalar<CPLX>::T *x, double theta, typename Scalar<CPLX>::T *r, int64_t n,
+             cudaStream_t s);
+
+}  // namespace heff

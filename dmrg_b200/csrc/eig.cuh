@@ -1,0 +1,7 @@
+// Device eigensolver (see eig.cu).
+#pragma once
+#include "heff_common.cuh"
+
+namespace heff {
+int eigs(heff_op *op, const heff_eig_config *cfg, const void *x0, void *x_out, heff_eig_result *res);
+}

@@ -84,6 +84,45 @@ int heff_expval_z(double *result, const heff_z *mps, const int64_t mps_dims[3], 
                   const int64_t envL_dims[3], const heff_z *envR, const int64_t envR_dims[3], void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Environment update
+ * ------------------------------------------------------------------------- */
+
+/* out = EnvBase::build_block(env, mps, mpo) (source/tensors/site/env/EnvBase.cpp:67-151):
+ *   side 0 ('L', :109-112): out[b,b',n] = sum env[a,a',m] mps[s,a,b] conj(mps)[s',a',b'] mpo[m,n,s,s']
+ *   side 1 ('R', :146-149): out[a,a',m] = sum env[b,b',n] mps[s,a,b] conj(mps)[s',a',b'] mpo[m,n,s,s']
+ * env [chi,chi,D] (chi = mps dim 1 for L, dim 2 for R), mps [d,chiL,chiR], mpo [DL,DR,d,d];
+ * out is [chiR,chiR,DR] (L) or [chiL,chiL,DL] (R).  The reference keeps environments complex
+ * (EnvBase.h:26); the _d form is for environments whose imaginary part is identically zero.
+ * Dimension checks follow EnvBase.cpp:93-101 / :130-138 (HEFF_BAD_SHAPE). */
+int heff_env_update_d(int side, double *out, const double *env, const int64_t env_dims[3], const double *mps, const int64_t mps_dims[3],
+                      const double *mpo, const int64_t mpo_dims[4], void *stream);
+int heff_env_update_z(int side, heff_z *out, const heff_z *env, const int64_t env_dims[3], const heff_z *mps, const int64_t mps_dims[3],
+                      const heff_z *mpo, const int64_t mpo_dims[4], void *stream);
+
+/* ---------------------------------------------------------------------------
+ * SVD truncation
+ * ------------------------------------------------------------------------- */
+
+/* Truncated SVD A = U S VT of a rows x cols column-major matrix, replacing
+ * svd::solver::do_svd_ptr (source/math/svd/svd.cpp:113-206; geauto resolves to
+ * LAPACK ?gesdd for the two-site split).  FP64 one-sided block Jacobi on the
+ * device.  The rank follows get_rank_from_truncation_error (svd.cpp:257-280):
+ * keep singular values while the norm of the discarded tail stays >= trunc_lim,
+ * at most rank_max (<= 0: no limit).  U [rows x k], S [k] (not normalised, like
+ * svd_lapacke.cpp:457), VT [k x cols] are device buffers sized for
+ * k = min(rows, cols, rank_max); *rank and *trunc_err are host outputs.
+ * Synchronises the stream. */
+int heff_svd_d(const double *A, int64_t rows, int64_t cols, int64_t rank_max, double trunc_lim, double *U, double *S, double *VT, int64_t *rank,
+               double *trunc_err, void *stream);
+/* Two-site Schmidt split, replacing svd::solver::schmidt_multisite
+ * (source/math/svd.h:189-220): theta [dL*dR, chiL, chiR] is reshaped to
+ * [dL, dR, chiL, chiR], shuffled {0,2,1,3} and decomposed as a (dL chiL) x
+ * (dR chiR) matrix.  Outputs U [dL, chiL, k], S [k] normalised to unit norm
+ * (svd.h:172), V [dR, k, chiR] (svd.h:173).  Synchronises the stream. */
+int heff_schmidt_d(const double *theta, int64_t dL, int64_t dR, int64_t chiL, int64_t chiR, int64_t rank_max, double trunc_lim, double *U,
+                   double *S, double *V, int64_t *rank, double *trunc_err, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Operator object: MatVecMPOS<T> / MatVecMPO<T>
  * (source/math/eig/matvec/matvec_mpos.h:23-180, matvec_mpo.h:18-103)
  * ------------------------------------------------------------------------- */
@@ -123,6 +162,69 @@ int64_t heff_op_num_mv(const heff_op *op);
  * stream and returns the summed milliseconds per stage and the matvec count. */
 int heff_op_set_profiling(heff_op *op, int enable);
 int heff_op_stage_times(heff_op *op, double ms[4], int64_t *count, int reset);
+
+/* ---------------------------------------------------------------------------
+ * Eigensolver (the caller side of MultAx: eig::solver, source/math/eig/solver.h:15-88)
+ * ------------------------------------------------------------------------- */
+typedef enum { HEFF_RITZ_SA = 0, HEFF_RITZ_LA = 1, HEFF_RITZ_TARGET = 2 } heff_ritz;
+
+typedef struct {
+    int     ritz;        /* heff_ritz: smallest / largest algebraic, or closest to `target` */
+    double  target;      /* target eigenvalue for HEFF_RITZ_TARGET */
+    double  tol;         /* ||H x - theta x|| <= tol * ||H||_est (PRIMME eps, solver_primme.cpp:364); default 1e-12 */
+    int     max_basis;   /* Davidson basis size (<= 128), default 32 */
+    int     min_basis;   /* vectors kept at a thick restart, default 8 */
+    int64_t max_matvecs; /* default 20000 */
+    int     mixed;       /* 1: when the operator is HEFF_PREC_MIXED, split-BF16 phase then FP64 refinement */
+    double  mixed_tol;   /* relative residual at which the mixed phase hands over, default 1e-6 */
+    int     inner_iters; /* CG iterations of one refinement correction (mixed operator), default 40 */
+    double  inner_tol;   /* relative CG residual that ends a correction, default 1e-4 */
+    int64_t seed;        /* start vector seed when x0 is NULL */
+} heff_eig_config;
+
+typedef struct {
+    double  eigval, resnorm, anorm, seconds;
+    int64_t num_mv, num_mv_fp64, num_mv_mixed, num_mv_phase1;
+    int     iters, restarts, refine_steps, converged;
+} heff_eig_result;
+
+void heff_eig_config_default(heff_eig_config *cfg);
+/* One extremal/interior eigenpair of the operator (Davidson, thick restart, FP64 CGS2
+ * re-orthogonalisation and Rayleigh-Ritz).  x0: device start vector or NULL; x_out:
+ * device output (normalised), may be NULL.  Returns HEFF_NOT_CONVERGED (result still
+ * filled) when max_matvecs is reached first.  Synchronises the operator's stream. */
+int heff_eigs(heff_op *op, const heff_eig_config *cfg, const void *x0, void *x_out, heff_eig_result *res);
+
+/* ---------------------------------------------------------------------------
+ * Minimal two-site DMRG sweep driver over the hot path (random-field Ising chain
+ * H = -sum J sz_i sz_{i+1} - sum h_i sx_i, IsingRandomField.cpp:93-136, open chain,
+ * real FP64).  Stands in for the caller layer (fdmrg::update_state, fdmrg.cpp:282-360)
+ * so whole calculations can run and be checked; not a port of the algorithm layer.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int           L;
+    double        J;
+    const double *h;                     /* host array of L fields */
+    int64_t       chi_max;               /* bond dimension limit (svd rank_max) */
+    int           sweeps;                /* full left-right-left sweeps */
+    double        trunc_lim;             /* svd truncation limit (svd.cpp:257-280), default 1e-12 */
+    double        eig_tol;               /* eigensolver tolerance, default 1e-12 */
+    int           ritz;                  /* heff_ritz */
+    double        target;                /* target for HEFF_RITZ_TARGET */
+    int           precision;             /* heff_precision of the matvecs */
+    int64_t       seed;                  /* random product-state initialisation */
+    double        energy_shift_per_site; /* MPO energy shift (IsingRandomField.cpp:127) */
+} heff_dmrg_config;
+
+typedef struct {
+    double  energy, entropy_mid, trunc_err_max, seconds, t_eig, t_svd, t_env;
+    int64_t chi_mid, num_mv, num_mv_mixed, unconverged_solves;
+    int     sweeps_done;
+    double  energy_per_sweep[64];
+} heff_dmrg_result;
+
+void heff_dmrg_config_default(heff_dmrg_config *cfg);
+int  heff_dmrg_run(const heff_dmrg_config *cfg, heff_dmrg_result *res, void *stream);
 
 #ifdef __cplusplus
 }

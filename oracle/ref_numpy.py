@@ -83,6 +83,71 @@ def matvec_blas(mps, mpo, envL, envR):
     return np.asfortranarray(T3.transpose(1, 2, 0))
 
 
+def env_update_blas(side, env, mps, mpo):
+    """EnvBase::build_block with the reference's contraction order, each step one GEMM.
+
+    L (EnvBase.cpp:109-112): X[a,m,s',b'] = L.contract(conj(M),{1},{1}); Y[a,b',n,s] = X.contract(W,{1,2},{0,3});
+                             L'[b,b',n] = M.contract(Y,{0,1},{3,0})
+    R (EnvBase.cpp:146-149): X[b,n,s',a'] = R.contract(conj(M),{1},{2}); Y[b,a',m,s] = X.contract(W,{1,2},{1,3});
+                             R'[a,a',m] = M.contract(Y,{0,2},{3,0})"""
+    d, cL, cR = mps.shape
+    DL, DR = mpo.shape[0], mpo.shape[1]
+    Mc = mps.conj()
+    if side == "L":
+        # X[(a,m),(s',b')] = sum_a' L[(a),(a'),m] conj(M)[s',a',b']
+        Lp = np.asfortranarray(env.transpose(0, 2, 1))  # [a,m,a']
+        Mp = np.asfortranarray(Mc.transpose(1, 0, 2))  # [a',s',b']
+        X = _mat(Lp, cL * DL) @ _mat(Mp, cL)  # [(a,m),(s',b')]
+        X = X.reshape(cL, DL, d, cR, order="F")
+        # Y[(a,b'),(n,s)] = sum_{m,s'} X[a,m,s',b'] W[m,n,s,s']
+        Xp = np.asfortranarray(X.transpose(0, 3, 1, 2))  # [a,b',m,s']
+        Wp = np.asfortranarray(mpo.transpose(0, 3, 1, 2))  # [m,s',n,s]
+        Y = _mat(Xp, cL * cR) @ _mat(Wp, DL * d)
+        Y = Y.reshape(cL, cR, DR, d, order="F")
+        # L'[b,(b',n)] = sum_{s,a} M[s,a,b] Y[a,b',n,s]
+        Mq = np.asfortranarray(mps.transpose(2, 0, 1))  # [b,s,a]
+        Yp = np.asfortranarray(Y.transpose(3, 0, 1, 2))  # [s,a,b',n]
+        out = _mat(Mq, cR) @ _mat(Yp, d * cL)
+        return out.reshape(cR, cR, DR, order="F")
+    # R side
+    Rp = np.asfortranarray(env.transpose(0, 2, 1))  # [b,n,b']
+    Mp = np.asfortranarray(Mc.transpose(2, 0, 1))  # [b',s',a']
+    X = _mat(Rp, cR * DR) @ _mat(Mp, cR)  # [(b,n),(s',a')]
+    X = X.reshape(cR, DR, d, cL, order="F")
+    Xp = np.asfortranarray(X.transpose(0, 3, 1, 2))  # [b,a',n,s']
+    Wp = np.asfortranarray(mpo.transpose(1, 3, 0, 2))  # [n,s',m,s]
+    Y = _mat(Xp, cR * cL) @ _mat(Wp, DR * d)
+    Y = Y.reshape(cR, cL, DL, d, order="F")  # [b,a',m,s]
+    Mq = np.asfortranarray(mps.transpose(1, 0, 2))  # [a,s,b]
+    Yp = np.asfortranarray(Y.transpose(3, 0, 1, 2))  # [s,b,a',m]
+    out = _mat(Mq, cL) @ _mat(Yp, d * cR)
+    return out.reshape(cL, cL, DL, order="F")
+
+
+def svd_truncated(A, rank_max=0, trunc_lim=1e-12):
+    """svd::solver::do_svd_ptr for the two-site split: geauto resolves to LAPACK ?gesdd for
+    rows*cols >= 256 (svd.cpp:127-140); numpy.linalg.svd calls the same LAPACK routine.  Then the
+    rank rule of svd.cpp:257-280 on the nonzero singular values (svd_lapacke.cpp:453-458)."""
+    from . import clib
+
+    U, S, VT = np.linalg.svd(A, full_matrices=False)
+    nz = int(np.count_nonzero(S))
+    r, err = clib.truncation_rank(S[:nz], rank_max, trunc_lim)
+    return U[:, :r], S[:r], VT[:r, :], r, err
+
+
+def schmidt_multisite(theta, dL, dR, rank_max=0, trunc_lim=1e-12):
+    """svd.h:189-220 (dR > 1 branch): reshape [dL,dR,chiL,chiR], shuffle {0,2,1,3}, SVD, S normalised,
+    V = VT reshaped [k,dR,chiR] shuffled {1,0,2}."""
+    S_, cL, cR = theta.shape
+    T4 = theta.reshape(dL, dR, cL, cR, order="F").transpose(0, 2, 1, 3)
+    A = np.asfortranarray(T4).reshape(dL * cL, dR * cR, order="F")
+    U, S, VT, r, err = svd_truncated(A, rank_max, trunc_lim)
+    Ut = U.reshape(dL, cL, r, order="F")
+    V = VT.reshape(r, dR, cR, order="F").transpose(1, 0, 2)
+    return np.asfortranarray(Ut), S / np.linalg.norm(S), np.asfortranarray(V), r, err
+
+
 def matvec_flops(S, cL, cR, DL, DR, cplx=False):
     """Algorithmic real FLOPs of one H_eff matvec (dense, as the reference computes it).
 

@@ -114,3 +114,11 @@ def test_mpo_chain_reproduces_ed(physics):
     Hd = H[0]
     w = np.linalg.eigvalsh(Hd)
     assert w[0] == pytest.approx(case["E0"], abs=1e-10)
+
+
+@pytest.mark.parametrize("i", range(N_ENV))
+@pytest.mark.parametrize("side", ["L", "R"])
+def test_env_update_blas_baseline_golden(golden, i, side):
+    g = lambda k: golden[f"env{i}_{k}"]
+    env = g("L") if side == "L" else g("R")
+    assert relerr(rn.env_update_blas(side, env, g("M"), g("W")), g("out" + side)) < 1e-13
