@@ -1,0 +1,287 @@
+// tcgen05 BF16 GEMM (see gemm_bf16x.cuh).
+#include <cstring>
+
+#include "gemm_bf16x.cuh"
+#include "runtime.cuh"
+
+namespace heff {
+
+__device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(saddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2 s of wall time (a correct kernel never gets near it).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if(mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while(!mbar_try_wait(bar, parity))
+        if(global_ns() - t0 > 2000000000ull) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *bar, void *dst, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(saddr(dst)),
+                 "l"((uint64_t)map), "r"(x), "r"(y), "r"(saddr(bar))
+                 : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major tile, 128-byte swizzle, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFFu) >> 4);  // start address
+    d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                   // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;                   // layout: 128-byte swizzle
+    return d;
+}
+
+// kind::f16 instruction descriptor: D=F32, A=B=BF16, both K-major, N=256, M=128
+constexpr uint32_t X_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(X_BN >> 3) << 17) | ((uint32_t)(X_BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(X_IDESC), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,"
+        "%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),
+          "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+constexpr int X_GROUP_M = 8;
+
+__global__ void __launch_bounds__(X_THREADS, 1)
+    gemm_bf16x_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const XGemmArgs p) {
+    extern __shared__ __align__(1024) unsigned char xsm_raw[];
+    unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(xsm_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t      *full      = reinterpret_cast<uint64_t *>(smem + X_STAGES * X_STAGE_BYTES);
+    uint64_t      *empty     = full + X_STAGES;
+    uint64_t      *tmem_full = empty + X_STAGES;
+    uint32_t      *tmem_slot = reinterpret_cast<uint32_t *>(tmem_full + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int       tile_m, tile_n;
+    {
+        const int num_m = (p.M + X_BM - 1) / X_BM, num_n = (p.N + X_BN - 1) / X_BN;
+        const int pid = blockIdx.x, per_group = X_GROUP_M * num_n;
+        const int first_m = (pid / per_group) * X_GROUP_M;
+        const int gsize   = min(num_m - first_m, X_GROUP_M);
+        tile_m            = first_m + (pid % per_group) % gsize;
+        tile_n            = (pid % per_group) / gsize;
+    }
+    const int m0 = tile_m * X_BM, n0 = tile_n * X_BN;
+    const int KB = (p.K + X_BK - 1) / X_BK;
+
+    if(threadIdx.x == 0) {
+        for(int s = 0; s < X_STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(tmem_full, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if(warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)), "r"(X_BN) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if(warp == 0) {
+        if(lane == 0) {
+            // TMA producer
+            for(int kb = 0; kb < KB; kb++) {
+                const int      st = kb % X_STAGES;
+                const uint32_t ph = (kb / X_STAGES) & 1;
+                if(!mbar_wait(&empty[st], ph ^ 1)) {
+                    atomicExch(p.err, 1);
+                    break;
+                }
+                unsigned char *a = smem + st * X_STAGE_BYTES, *b = a + X_A_BYTES;
+                mbar_expect_tx(&full[st], X_STAGE_BYTES);
+                tma_load_2d(&tmA, &full[st], a, kb * X_BK, m0);
+                tma_load_2d(&tmB, &full[st], b, kb * X_BK, n0);
+            }
+        }
+    } else if(warp == 1) {
+        if(lane == 0) {
+            // MMA issuer
+            for(int kb = 0; kb < KB; kb++) {
+                const int      st = kb % X_STAGES;
+                const uint32_t ph = (kb / X_STAGES) & 1;
+                if(!mbar_wait(&full[st], ph)) {
+                    atomicExch(p.err, 2);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a = saddr(smem + st * X_STAGE_BYTES), b = a + X_A_BYTES;
+#pragma unroll
+                for(int k = 0; k < X_BK / 16; k++) umma_bf16(tmem_base, sdesc_sw128(a + 32 * k), sdesc_sw128(b + 32 * k), (kb | k) != 0);
+                umma_commit(&empty[st]);
+            }
+            umma_commit(tmem_full);  // fires when every MMA issued above has completed
+        }
+    } else {
+        // epilogue: warps 2..5 -> TMEM lane quarters 2,3,0,1
+        const int  q   = warp & 3;
+        const int  row = m0 + q * 32 + lane;
+        const bool ok  = mbar_wait(tmem_full, 0);
+        if(!ok) atomicExch(p.err, 3);
+        tc_fence_after();
+        if(ok && KB > 0) {
+            for(int c = 0; c < X_BN; c += 32) {
+                if(n0 + c >= p.N) break;
+                uint32_t r[32];
+                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)c, r);
+                if(row < p.M) {
+#pragma unroll
+                    for(int j = 0; j < 32; j++) {
+                        const int n = n0 + c + j;
+                        if(n < p.N) {
+                            const float v = __uint_as_float(r[j]);
+                            if(p.mode == X_OUT_F32)
+                                reinterpret_cast<float *>(p.C)[row + p.ldc * n] = v;
+                            else if(p.mode == X_OUT_F32_ACC)
+                                reinterpret_cast<float *>(p.C)[row + p.ldc * n] += v;
+                            else if(p.mode == X_OUT_F64)
+                                reinterpret_cast<double *>(p.C)[row + p.ldc * n] = (double)v;
+                            else {
+                                const bool im = n >= p.n_half;
+                                const int  nn = im ? n - p.n_half : n;
+                                reinterpret_cast<double *>(p.C)[2 * (row + p.ldc * nn) + (im ? 1 : 0)] = (double)v;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if(warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(X_BN) : "memory");
+    }
+}
+
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,
+                                    const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                    CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled encode_fn() {
+    static PFN_encodeTiled fn = nullptr;
+    if(!fn) {
+        void                            *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_encodeTiled>(p);
+    }
+    return fn;
+}
+
+int make_tmap_bf16(CUtensorMap *map, const void *base, int64_t rows, int64_t kcols, int64_t ld_elems, int box_rows) {
+    PFN_encodeTiled fn = encode_fn();
+    if(!fn) {
+        set_last_error_msg("cuTensorMapEncodeTiled is not available from the driver");
+        return HEFF_CUDA_ERROR;
+    }
+    if(((uintptr_t)base & 15) || (ld_elems * 2) % 16 || kcols % 8) return HEFF_BAD_ARG;
+    std::memset(map, 0, sizeof(*map));
+    cuuint64_t dims[2]    = {(cuuint64_t)kcols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld_elems * 2)};
+    cuuint32_t box[2]     = {(cuuint32_t)X_BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2]    = {1, 1};
+    CUresult   r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if(r != CUDA_SUCCESS) {
+        set_last_error_msg("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return HEFF_CUDA_ERROR;
+    }
+    return HEFF_OK;
+}
+
+int gemm_bf16x(const CUtensorMap &tmA, const CUtensorMap &tmB, const XGemmArgs &a, cudaStream_t s) {
+    if(a.M <= 0 || a.N <= 0) return HEFF_OK;
+    if(a.K <= 0 || a.K % 8) return HEFF_BAD_ARG;  // K tail beyond a multiple of 64 is zero-filled by TMA
+    static int attr_done[64] = {0};
+    int        dev           = 0;
+    HEFF_CUDA(cudaGetDevice(&dev));
+    if(dev < 0 || dev >= 64 || !attr_done[dev]) {
+        HEFF_CUDA(cudaFuncSetAttribute(gemm_bf16x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, X_SMEM_BYTES));
+        if(dev >= 0 && dev < 64) attr_done[dev] = 1;
+    }
+    const int64_t tiles = cdiv(a.M, X_BM) * cdiv(a.N, X_BN);
+    if(tiles > 0x7fffffff) return HEFF_BAD_SHAPE;
+    gemm_bf16x_kernel<<<(unsigned)tiles, X_THREADS, X_SMEM_BYTES, s>>>(tmA, tmB, a);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+}  // namespace heff
+
+using namespace heff;
+
+extern "C" int heff_gemm_bf16_f32(const void *A, const void *B, float *C, int64_t M, int64_t N, int64_t K, void *stream) {
+    if(!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return HEFF_BAD_ARG;
+    if(K % 8 || M > 0x7fffffff || N > 0x7fffffff || K > 0x7fffffff) {
+        set_last_error_msg("heff_gemm_bf16_f32: K must be a multiple of 8");
+        return HEFF_BAD_SHAPE;
+    }
+    CUtensorMap ta, tb;
+    HEFF_TRY(make_tmap_bf16(&ta, A, M, K, K, X_BM));
+    HEFF_TRY(make_tmap_bf16(&tb, B, N, K, K, X_BN));
+    void *err = nullptr;
+    HEFF_TRY(stream_workspace((cudaStream_t)stream, 256, &err));
+    HEFF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), (cudaStream_t)stream));
+    XGemmArgs g{};
+    g.M = (int)M, g.N = (int)N, g.K = (int)K, g.C = C, g.ldc = M, g.mode = X_OUT_F32, g.err = reinterpret_cast<int *>(err);
+    HEFF_TRY(gemm_bf16x(ta, tb, g, (cudaStream_t)stream));
+    int h = 0;
+    HEFF_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    HEFF_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if(h) {
+        set_last_error_msg("heff_gemm_bf16_f32: pipeline wait timed out (code %d)", h);
+        return HEFF_TIMEOUT;
+    }
+    return HEFF_OK;
+}

@@ -1,0 +1,315 @@
+// Mixed-precision H_eff matvec: split-BF16 operands on tcgen05 tensor cores with FP32 accumulation.
+//
+// Same contraction order as the FP64 path (matvec.cuh):
+//   G1  T1[(a',m),(s,b)]   = sum_a L[a,(a',m)] x[s,a,b]              BF16 GEMM, K = chiL
+//   MIX T2[(s',a'),(b,n)]  = sum_{m,s} W[m,n,s,s'] T1[(a',m),(s,b)]  FP64 arithmetic on FP32 inputs
+//   G2  y[(s',a'),b']      = sum_{(b,n)} T2[(s',a'),(b,n)] R[b,b',n]  BF16 GEMM, K = chiR*D, FP64 output
+// Each FP64 operand v is split into v_hi = bf16(v), v_mid = bf16(v - v_hi) (16 significant bits) and the
+// three leading split products are folded into the GEMM's K dimension (segments):
+//   real:    A' = [a_h | a_h | a_m]                    B' = [b_h | b_m | b_h]
+//   complex: A' = [ar_h | ar_h | ar_m | ai_h | ai_h | ai_m]
+//            B' rows of Re(C): [br_h | br_m | br_h | -bi_h | -bi_m | -bi_h],  rows of Im(C): [bi_h | bi_m | bi_h | br_h | br_m | br_h]
+// so one K-major BF16 GEMM per stage computes the product to ~2^-16 relative accuracy (FP32 accumulation
+// adds ~sqrt(K) 2^-24).  The eigensolver uses this path for its inner iterations and restores FP64
+// accuracy by refinement with the FP64 matvec.  The environment operands (L, R') are split once per
+// operator; x and T2 are split per matvec.
+#include <cuda_bf16.h>
+
+#include "gemm_bf16x.cuh"
+#include "matvec.cuh"
+#include "op.cuh"
+#include "runtime.cuh"
+
+namespace heff {
+
+struct MixedState {
+    int            cplx, nseg;
+    int64_t        M1, N1, K1, Kp1, Kx1;  // GEMM1: rows (a',m), cols (s,b), K = a
+    int64_t        M2, N2, K2, Kp2, Kx2;  // GEMM2: rows (s',a'), cols b', K = (b,n)
+    __nv_bfloat16 *A1 = nullptr, *B1 = nullptr, *A2 = nullptr, *B2 = nullptr;
+    float         *T1  = nullptr;
+    int           *err = nullptr;
+    CUtensorMap    tA1, tB1, tA2, tB2;
+};
+
+__device__ __forceinline__ void split2(double v, __nv_bfloat16 &h, __nv_bfloat16 &m) {
+    h = __double2bfloat16(v);
+    m = __double2bfloat16(v - (double)__bfloat162float(h));
+}
+
+// Segment tables.  A: (component, part); B for Re rows and Im rows: (component, part, sign).
+struct SegA {
+    int comp, part;
+};
+struct SegB {
+    int comp, part, sign;
+};
+__constant__ SegA c_segA_real[3] = {{0, 0}, {0, 0}, {0, 1}};
+__constant__ SegB c_segB_real[3] = {{0, 0, 1}, {0, 1, 1}, {0, 0, 1}};
+__constant__ SegA c_segA_cplx[6] = {{0, 0}, {0, 0}, {0, 1}, {1, 0}, {1, 0}, {1, 1}};
+__constant__ SegB c_segB_re[6]   = {{0, 0, 1}, {0, 1, 1}, {0, 0, 1}, {1, 0, -1}, {1, 1, -1}, {1, 0, -1}};
+__constant__ SegB c_segB_im[6]   = {{1, 0, 1}, {1, 1, 1}, {1, 0, 1}, {0, 0, 1}, {0, 1, 1}, {0, 0, 1}};
+
+// Writes the A'-segments of one value pair (re, im) at row base `dst` (column k of each segment).
+template<bool CPLX>
+__device__ __forceinline__ void put_A(__nv_bfloat16 *dst, int64_t Kp, int64_t k, double re, double im) {
+    __nv_bfloat16 rh, rm, ih, imm;
+    split2(re, rh, rm);
+    if constexpr(!CPLX) {
+        dst[k]          = rh;
+        dst[Kp + k]     = rh;
+        dst[2 * Kp + k] = rm;
+    } else {
+        split2(im, ih, imm);
+        dst[k]          = rh;
+        dst[Kp + k]     = rh;
+        dst[2 * Kp + k] = rm;
+        dst[3 * Kp + k] = ih;
+        dst[4 * Kp + k] = ih;
+        dst[5 * Kp + k] = imm;
+    }
+}
+// B'-segments: Re-output row at dst_re, Im-output row at dst_im (complex only).
+template<bool CPLX>
+__device__ __forceinline__ void put_B(__nv_bfloat16 *dst_re, __nv_bfloat16 *dst_im, int64_t Kp, int64_t k, double re, double im) {
+    __nv_bfloat16 rh, rm;
+    split2(re, rh, rm);
+    if constexpr(!CPLX) {
+        dst_re[k]          = rh;
+        dst_re[Kp + k]     = rm;
+        dst_re[2 * Kp + k] = rh;
+    } else {
+        __nv_bfloat16 ih, imm, nih, nim;
+        split2(im, ih, imm);
+        split2(-im, nih, nim);
+        dst_re[k]          = rh;
+        dst_re[Kp + k]     = rm;
+        dst_re[2 * Kp + k] = rh;
+        dst_re[3 * Kp + k] = nih;
+        dst_re[4 * Kp + k] = nim;
+        dst_re[5 * Kp + k] = nih;
+        dst_im[k]          = ih;
+        dst_im[Kp + k]     = imm;
+        dst_im[2 * Kp + k] = ih;
+        dst_im[3 * Kp + k] = rh;
+        dst_im[4 * Kp + k] = rm;
+        dst_im[5 * Kp + k] = rh;
+    }
+}
+
+__device__ __forceinline__ double re_of(double v) { return v; }
+__device__ __forceinline__ double im_of(double) { return 0.0; }
+__device__ __forceinline__ double re_of(double2 v) { return v.x; }
+__device__ __forceinline__ double im_of(double2 v) { return v.y; }
+
+// A1'[r][seg*Kp1 + a] from L[a + cL*r]   (r = a' + cL*m)
+template<bool CPLX>
+__global__ void split_L_kernel(const typename Scalar<CPLX>::T *__restrict__ L, __nv_bfloat16 *__restrict__ A1, int64_t cL, int64_t M1, int64_t Kp1,
+                               int64_t Kx1) {
+    const int64_t tot = cL * M1;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = e % cL, r = e / cL;
+        const auto    v = L[e];
+        put_A<CPLX>(A1 + r * Kx1, Kp1, a, re_of(v), im_of(v));
+    }
+}
+// B2'[b'][seg*Kp2 + k] from R'[k + K2*b'] (k = b + cR*n); complex: Im rows at b' + cR
+template<bool CPLX>
+__global__ void split_R_kernel(const typename Scalar<CPLX>::T *__restrict__ Rp, __nv_bfloat16 *__restrict__ B2, int64_t K2, int64_t cR, int64_t Kp2,
+                               int64_t Kx2) {
+    const int64_t tot = K2 * cR;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e % K2, bp = e / K2;
+        const auto    v = Rp[e];
+        put_B<CPLX>(B2 + bp * Kx2, CPLX ? B2 + (bp + cR) * Kx2 : nullptr, Kp2, k, re_of(v), im_of(v));
+    }
+}
+// B1'[(s + S b)][seg*Kp1 + a] from x[s + S*(a + cL*b)]; complex: Im rows at + N1
+template<bool CPLX>
+__global__ void split_x_kernel(const typename Scalar<CPLX>::T *__restrict__ x, __nv_bfloat16 *__restrict__ B1, int64_t S, int64_t cL, int64_t N1,
+                               int64_t Kp1, int64_t Kx1) {
+    const int64_t tot = cL * N1;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = e % cL, n = e / cL, s = n % S, b = n / S;
+        const auto    v = x[s + S * (a + cL * b)];
+        put_B<CPLX>(B1 + n * Kx1, CPLX ? B1 + (n + N1) * Kx1 : nullptr, Kp1, a, re_of(v), im_of(v));
+    }
+}
+
+// MIX: tile of 16 a' x 32 b.  Load phase a'-fastest (coalesced T1 reads) into shared memory; compute
+// phase b-fastest so the split T2 segments are written contiguously along k = b + cR*n.
+constexpr int MX_TA = 16, MX_TB = 32, MX_THREADS = MX_TA * MX_TB;
+template<bool CPLX>
+__global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__restrict__ T1, const typename Scalar<CPLX>::T *__restrict__ W,
+                                                              __nv_bfloat16 *__restrict__ A2, int S, int cL, int cR, int DL, int DR, int64_t M1,
+                                                              int64_t N1, int64_t Kp2, int64_t Kx2) {
+    using T = typename Scalar<CPLX>::T;
+    extern __shared__ __align__(16) unsigned char mxs[];
+    T     *sW  = reinterpret_cast<T *>(mxs);
+    const int nW = DL * DR * S * S;
+    float *sRe = reinterpret_cast<float *>(sW + nW);
+    const int NP = DL * S;
+    float *sIm = sRe + NP * MX_THREADS;
+    for(int i = threadIdx.x; i < nW; i += blockDim.x) sW[i] = W[i];
+    const int a0 = blockIdx.x * MX_TA, b0 = blockIdx.y * MX_TB;
+    {
+        const int al = threadIdx.x % MX_TA, bl = threadIdx.x / MX_TA;
+        const int ap = a0 + al, b = b0 + bl;
+        for(int ms = 0; ms < NP; ms++) {
+            const int m = ms / S, s = ms % S;
+            float     vr = 0.f, vi = 0.f;
+            if(ap < cL && b < cR) {
+                const int64_t idx = (ap + (int64_t)cL * m) + M1 * (s + (int64_t)S * b);
+                vr                = T1[idx];
+                if(CPLX) vi = T1[idx + M1 * N1];
+            }
+            sRe[ms * MX_THREADS + al * MX_TB + bl] = vr;
+            if(CPLX) sIm[ms * MX_THREADS + al * MX_TB + bl] = vi;
+        }
+    }
+    __syncthreads();
+    const int bl = threadIdx.x % MX_TB, al = threadIdx.x / MX_TB;
+    const int ap = a0 + al, b = b0 + bl;
+    if(ap >= cL || b >= cR) return;
+    for(int n = 0; n < DR; n++)
+        for(int sp = 0; sp < S; sp++) {
+            double re = 0, im = 0;
+            for(int s = 0; s < S; s++)
+                for(int m = 0; m < DL; m++) {
+                    const T w = sW[m + DL * (n + DR * (s + S * sp))];
+                    const int   slot = (m * S + s) * MX_THREADS + al * MX_TB + bl;
+                    const double xr  = sRe[slot];
+                    if constexpr(CPLX) {
+                        const double xi = sIm[slot];
+                        re += w.x * xr - w.y * xi;
+                        im += w.x * xi + w.y * xr;
+                    } else {
+                        re += w * xr;
+                    }
+                }
+            const int64_t row = sp + (int64_t)S * ap, k = b + (int64_t)cR * n;
+            put_A<CPLX>(A2 + row * Kx2, Kp2, k, re, im);
+        }
+}
+
+static int g1(int64_t n) {
+    int64_t g = (n + 255) / 256, cap = (int64_t)device_sm_count() * 16;
+    return (int)(g < 1 ? 1 : (g < cap ? g : cap));
+}
+static int64_t r64(int64_t v) { return (v + 63) / 64 * 64; }
+
+static void mixed_destroy(heff_op *op) {
+    MixedState *m = reinterpret_cast<MixedState *>(op->mixed);
+    if(!m) return;
+    if(m->A1) cudaFree(m->A1);
+    if(m->B1) cudaFree(m->B1);
+    if(m->A2) cudaFree(m->A2);
+    if(m->B2) cudaFree(m->B2);
+    if(m->T1) cudaFree(m->T1);
+    if(m->err) cudaFree(m->err);
+    delete m;
+    op->mixed = nullptr;
+}
+
+template<bool CPLX>
+static int mixed_setup(heff_op *op) {
+    using T         = typename Scalar<CPLX>::T;
+    const auto &d   = op->d;
+    MixedState *m   = new MixedState();
+    op->mixed       = m;
+    op->destroy_hook = mixed_destroy;
+    m->cplx         = CPLX;
+    m->nseg         = CPLX ? 6 : 3;
+    const int cf    = CPLX ? 2 : 1;
+    m->M1           = d.cL * d.DL;
+    m->N1           = d.S * d.cR;
+    m->K1           = d.cL;
+    m->Kp1          = r64(m->K1);
+    m->Kx1          = m->nseg * m->Kp1;
+    m->M2           = d.S * d.cL;
+    m->N2           = d.cR;
+    m->K2           = d.cR * d.DR;
+    m->Kp2          = r64(m->K2);
+    m->Kx2          = m->nseg * m->Kp2;
+    const size_t bA1 = 2 * (size_t)m->M1 * m->Kx1, bB1 = 2 * (size_t)(cf * m->N1) * m->Kx1;
+    const size_t bA2 = 2 * (size_t)m->M2 * m->Kx2, bB2 = 2 * (size_t)(cf * m->N2) * m->Kx2;
+    const size_t bT1 = 4 * (size_t)m->M1 * (cf * m->N1);
+    auto         al  = [&](void **p, size_t b) -> int {
+        cudaError_t e = cudaMalloc(p, b);
+        if(e != cudaSuccess) {
+            set_last_cuda_error(e, "mixed-precision buffers", __FILE__, __LINE__);
+            return HEFF_OOM;
+        }
+        return HEFF_OK;
+    };
+    HEFF_TRY(al((void **)&m->A1, bA1));
+    HEFF_TRY(al((void **)&m->B1, bB1));
+    HEFF_TRY(al((void **)&m->A2, bA2));
+    HEFF_TRY(al((void **)&m->B2, bB2));
+    HEFF_TRY(al((void **)&m->T1, bT1));
+    HEFF_TRY(al((void **)&m->err, sizeof(int)));
+    cudaStream_t s = op->stream;
+    // K padding of every segment stays zero for the life of the buffers
+    HEFF_CUDA(cudaMemsetAsync(m->A1, 0, bA1, s));
+    HEFF_CUDA(cudaMemsetAsync(m->B1, 0, bB1, s));
+    HEFF_CUDA(cudaMemsetAsync(m->A2, 0, bA2, s));
+    HEFF_CUDA(cudaMemsetAsync(m->B2, 0, bB2, s));
+    HEFF_CUDA(cudaMemsetAsync(m->err, 0, sizeof(int), s));
+    split_L_kernel<CPLX><<<g1(m->K1 * m->M1), 256, 0, s>>>(reinterpret_cast<const T *>(op->L), m->A1, d.cL, m->M1, m->Kp1, m->Kx1);
+    HEFF_LAUNCH_CHECK();
+    split_R_kernel<CPLX><<<g1(m->K2 * m->N2), 256, 0, s>>>(reinterpret_cast<const T *>(op->Rp), m->B2, m->K2, d.cR, m->Kp2, m->Kx2);
+    HEFF_LAUNCH_CHECK();
+    HEFF_TRY(make_tmap_bf16(&m->tA1, m->A1, m->M1, m->Kx1, m->Kx1, X_BM));
+    HEFF_TRY(make_tmap_bf16(&m->tB1, m->B1, cf * m->N1, m->Kx1, m->Kx1, X_BN));
+    HEFF_TRY(make_tmap_bf16(&m->tA2, m->A2, m->M2, m->Kx2, m->Kx2, X_BM));
+    HEFF_TRY(make_tmap_bf16(&m->tB2, m->B2, cf * m->N2, m->Kx2, m->Kx2, X_BN));
+    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS;
+    if(mix_smem > 200 * 1024) return HEFF_BAD_SHAPE;
+    HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    HEFF_CUDA(cudaStreamSynchronize(s));
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+static int mixed_apply_impl(heff_op *op, const void *x, void *y) {
+    using T = typename Scalar<CPLX>::T;
+    if(!op->mixed) HEFF_TRY(mixed_setup<CPLX>(op));
+    MixedState  *m  = reinterpret_cast<MixedState *>(op->mixed);
+    const auto  &d  = op->d;
+    cudaStream_t s  = op->stream;
+    const int    cf = CPLX ? 2 : 1;
+    split_x_kernel<CPLX><<<g1(m->K1 * m->N1), 256, 0, s>>>(reinterpret_cast<const T *>(x), m->B1, d.S, d.cL, m->N1, m->Kp1, m->Kx1);
+    HEFF_LAUNCH_CHECK();
+    XGemmArgs g1a{};
+    g1a.M = (int)m->M1, g1a.N = (int)(cf * m->N1), g1a.K = (int)m->Kx1, g1a.C = m->T1, g1a.ldc = m->M1, g1a.mode = X_OUT_F32, g1a.err = m->err;
+    HEFF_TRY(gemm_bf16x(m->tA1, m->tB1, g1a, s));
+    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS;
+    if(d.cR / MX_TB + 1 > 65535) return HEFF_BAD_SHAPE;
+    dim3 grid((unsigned)cdiv(d.cL, MX_TA), (unsigned)cdiv(d.cR, MX_TB));
+    mix_mixed_kernel<CPLX><<<grid, MX_THREADS, mix_smem, s>>>(m->T1, reinterpret_cast<const T *>(op->W), m->A2, (int)d.S, (int)d.cL, (int)d.cR,
+                                                             (int)d.DL, (int)d.DR, m->M1, m->N1, m->Kp2, m->Kx2);
+    HEFF_LAUNCH_CHECK();
+    XGemmArgs g2{};
+    g2.M = (int)m->M2, g2.N = (int)(cf * m->N2), g2.K = (int)m->Kx2, g2.C = y, g2.ldc = m->M2, g2.err = m->err;
+    g2.mode   = CPLX ? X_OUT_C128 : X_OUT_F64;
+    g2.n_half = (int)m->N2;
+    HEFF_TRY(gemm_bf16x(m->tA2, m->tB2, g2, s));
+    op->num_mv++;
+    return HEFF_OK;
+}
+
+int mixed_apply(heff_op *op, const void *x, void *y) {
+    if(x == y) return HEFF_BAD_ARG;
+    return op->cplx ? mixed_apply_impl<true>(op, x, y) : mixed_apply_impl<false>(op, x, y);
+}
+
+int mixed_error_flag(heff_op *op, int *flag) {
+    *flag = 0;
+    MixedState *m = reinterpret_cast<MixedState *>(op->mixed);
+    if(!m) return HEFF_OK;
+    HEFF_CUDA(cudaMemcpyAsync(flag, m->err, sizeof(int), cudaMemcpyDeviceToHost, op->stream));
+    HEFF_CUDA(cudaStreamSynchronize(op->stream));
+    return HEFF_OK;
+}
+
+}  // namespace heff

@@ -84,8 +84,9 @@ static int create_impl(heff_op **out, int nsites, const void *const *mpos, const
     heff_op *op   = new heff_op();
     op->cplx      = CPLX;
     op->d         = d;
-    op->precision = prec;
-    op->stream    = stream;
+    op->precision   = prec;
+    op->stream      = stream;
+    op->mixed_apply = mixed_apply;  // split-BF16 tcgen05 path; its state is built on first use
     std::memcpy(op->mpo_dims, wd, sizeof(wd));
     const size_t es   = sizeof(T);
     auto         fail = [&](int rc) {
@@ -249,6 +250,11 @@ extern "C" int heff_op_set_precision(heff_op *op, heff_precision precision) {
 }
 
 extern "C" int64_t heff_op_num_mv(const heff_op *op) { return op ? op->num_mv : -1; }
+
+extern "C" int heff_op_device_error(heff_op *op, int *code) {
+    if(!op || !code) return HEFF_BAD_ARG;
+    return mixed_error_flag(op, code);
+}
 
 extern "C" int heff_op_set_profiling(heff_op *op, int enable) {
     if(!op) return HEFF_BAD_ARG;

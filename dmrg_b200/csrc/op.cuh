@@ -29,6 +29,8 @@ struct heff_op {
 
 namespace heff {
 int op_apply(heff_op *op, const void *x, void *y);
+int mixed_apply(heff_op *op, const void *x, void *y);     // mixed.cu
+int mixed_error_flag(heff_op *op, int *flag);              // mixed.cu
 int op_prof_flush(heff_op *op);  // synchronises the op's stream and folds recorded events into prof_ms
 cudaEvent_t *op_prof_slot(heff_op *op);  // next free 5-event set or nullptr (profiling off)
 }

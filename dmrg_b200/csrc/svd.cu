@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(double *__restrict__
     __shared__ double cs_c[JP / 2], cs_s[JP / 2];
     __shared__ int    s_idx[JP];
     __shared__ double s_red[JTHR];
-    __shared__ int    s_flag;
+    __shared__ int    s_rot[2];
 
     int p, q;
     rr_pair(B, round, blockIdx.x, p, q);
@@ -110,24 +110,32 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(double *__restrict__
     if(off0 <= tol) return;  // uniform across the CTA
     if(tid == 0) atomicAdd(rotated, 1);
 
-    // ---- 2. cyclic Jacobi on sG, accumulating sQ
+    // ---- 2. cyclic Jacobi on sG, accumulating sQ.  Rotations are applied in Rutishauser's form
+    //      x' = x - s (y + tau x), y' = y + s (x - tau y), tau = s / (1 + c), which keeps the rounding of c
+    //      (c -> 1 for tiny angles) from inflating column norms; only numerically significant
+    //      off-diagonals (|g_ab| > tol sqrt(g_aa g_bb)) are rotated, at most 8 sweeps (the outer sweep
+    //      re-checks every pair on a freshly computed Gram matrix).
     for(int e = tid; e < JP * JP; e += JTHR) sQ[e / JP][e % JP] = (e / JP == e % JP) ? 1.0 : 0.0;
+    if(tid < 2) s_rot[tid] = 0;
     __syncthreads();
-    for(int sweep = 0; sweep < 20; sweep++) {
+    for(int sweep = 0; sweep < 8; sweep++) {
+        const int par = sweep & 1;
         for(int step = 0; step < JP - 1; step++) {
             if(tid < JP / 2) {
                 int a, b;
                 rr_pair(JP, step, tid, a, b);
                 const double app = sG[a][a], aqq = sG[b][b], apq = sG[a][b];
-                double       c = 1.0, s = 0.0;
-                if(fabs(apq) > 1e-300 && fabs(apq) > 0.25 * tol * sqrt(fabs(app) * fabs(aqq))) {
+                double       sn = 0.0, tau = 0.0;
+                if(fabs(apq) > 1e-300 && fabs(apq) > tol * sqrt(fabs(app) * fabs(aqq))) {
                     const double th = (aqq - app) / (2.0 * apq);
                     const double t  = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(1.0 + th * th));
-                    c               = 1.0 / sqrt(1.0 + t * t);
-                    s               = t * c;
+                    const double c  = 1.0 / sqrt(1.0 + t * t);
+                    sn              = t * c;
+                    tau             = sn / (1.0 + c);
+                    s_rot[par]      = 1;
                 }
-                cs_c[tid] = c;
-                cs_s[tid] = s;
+                cs_c[tid] = tau;
+                cs_s[tid] = sn;
             }
             __syncthreads();
             // columns of G and Q: col_a' = c col_a - s col_b ; col_b' = s col_a + c col_b
@@ -135,14 +143,14 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(double *__restrict__
                 const int k = e / JP, row = e % JP;
                 int       a, b;
                 rr_pair(JP, step, k, a, b);
-                const double c = cs_c[k], s = cs_s[k];
-                if(s != 0.0) {
+                const double tau = cs_c[k], sn = cs_s[k];
+                if(sn != 0.0) {
                     const double ga = sG[row][a], gb = sG[row][b];
-                    sG[row][a]      = c * ga - s * gb;
-                    sG[row][b]      = s * ga + c * gb;
+                    sG[row][a]      = ga - sn * (gb + tau * ga);
+                    sG[row][b]      = gb + sn * (ga - tau * gb);
                     const double qa = sQ[row][a], qb = sQ[row][b];
-                    sQ[row][a]      = c * qa - s * qb;
-                    sQ[row][b]      = s * qa + c * qb;
+                    sQ[row][a]      = qa - sn * (qb + tau * qa);
+                    sQ[row][b]      = qb + sn * (qa - tau * qb);
                 }
             }
             __syncthreads();
@@ -151,19 +159,19 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(double *__restrict__
                 const int k = e / JP, col = e % JP;
                 int       a, b;
                 rr_pair(JP, step, k, a, b);
-                const double c = cs_c[k], s = cs_s[k];
-                if(s != 0.0) {
+                const double tau = cs_c[k], sn = cs_s[k];
+                if(sn != 0.0) {
                     const double ga = sG[a][col], gb = sG[b][col];
-                    sG[a][col]      = c * ga - s * gb;
-                    sG[b][col]      = s * ga + c * gb;
+                    sG[a][col]      = ga - sn * (gb + tau * ga);
+                    sG[b][col]      = gb + sn * (ga - tau * gb);
                 }
             }
             __syncthreads();
         }
-        const double off = off_measure();
-        if(tid == 0) s_flag = off <= 0.25 * tol;
+        const int rotated_this_sweep = s_rot[par];
         __syncthreads();
-        if(s_flag) break;
+        if(tid == 0) s_rot[par] = 0;  // reused two sweeps later; read above before this reset
+        if(!rotated_this_sweep) break;
     }
 
     // ---- 3. apply Q to the pair's columns of G (m rows) and V (nv rows)
@@ -286,7 +294,8 @@ int svd_truncated(const double *A, int64_t lda, int64_t m, int64_t n, int64_t ra
     eye_kernel<<<g1((int64_t)npad * npad), 256, 0, s>>>(V, npad, npad);
     HEFF_LAUNCH_CHECK();
     const int    B   = npad / JB;  // even
-    const double tol = std::max(1e-15, 2.2e-16 * std::sqrt((double)m));
+    // off-diagonal tolerance just above the rounding noise of a length-m dot product
+    const double tol = std::max(1e-14, 8.0 * 2.2e-16 * std::sqrt((double)m));
     int          sweep = 0;
     for(; sweep < 40; sweep++) {
         HEFF_CUDA(cudaMemsetAsync(dmax, 0, 8 * 8 + sizeof(int), s));

@@ -162,6 +162,20 @@ int64_t heff_op_num_mv(const heff_op *op);
  * stream and returns the summed milliseconds per stage and the matvec count. */
 int heff_op_set_profiling(heff_op *op, int enable);
 int heff_op_stage_times(heff_op *op, double ms[4], int64_t *count, int reset);
+/* Device-side status of the operator's tensor-core pipeline: *code = 0 when every
+ * bounded wait in the mixed-precision kernels completed, nonzero when one timed out
+ * (the kernel then skipped its work and returned).  Synchronises the stream. */
+int heff_op_device_error(heff_op *op, int *code);
+
+/* ---------------------------------------------------------------------------
+ * BF16 tensor-core GEMM used by the mixed-precision path (tcgen05 + TMA)
+ * ------------------------------------------------------------------------- */
+/* C[m + M*n] (float, column-major) = sum_k A[m*K + k] * B[n*K + k]; A (M x K) and
+ * B (N x K) bf16 row-major (K contiguous), K a multiple of 8, 16-byte aligned
+ * buffers.  No counterpart in the reference (its matvec is FP64/cx64 only); exposed
+ * so the split-precision building block can be validated on its own.
+ * Synchronises the stream; HEFF_TIMEOUT if a pipeline wait timed out. */
+int heff_gemm_bf16_f32(const void *A, const void *B, float *C, int64_t M, int64_t N, int64_t K, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Eigensolver (the caller side of MultAx: eig::solver, source/math/eig/solver.h:15-88)
