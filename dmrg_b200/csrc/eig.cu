@@ -1,19 +1,28 @@
-// Device eigensolver for H_eff: thick-restart Davidson (no preconditioner, i.e. a restarted Krylov
-// method) in FP64, driving the operator through the same apply path the reference's PRIMME/ARPACK
-// callback uses (MatVecMPOS::MultAx, solver_primme.cpp:122-128).  Re-orthogonalisation is classical
-// Gram-Schmidt applied twice (CGS2) in FP64; the Rayleigh-Ritz problem is solved on the host in FP64.
+// Device eigensolver for H_eff, driving the operator through the same apply path the reference's
+// PRIMME/ARPACK callback uses (MatVecMPOS::MultAx, solver_primme.cpp:122-128).
 //
-// Convergence (PRIMME-style, eps = tol, solver_primme.cpp:364): ||H x - theta x|| <= tol * ||H||_est,
-// ||H||_est = largest |Ritz value| seen.  Ritz selection: smallest algebraic (ground state,
-// optimize_energy.cpp:74-81), largest algebraic, or closest to a target (interior states).
+// Phase 1 -- thick-restart Davidson without preconditioner (a restarted Krylov method):
+//   * expansion with A v_last (for a Hermitian operator this spans the same Krylov space as expanding
+//     with the Ritz residual, also after a thick restart, and needs no extra pass over the basis),
+//   * FP64 Gram-Schmidt with DGKS selective re-orthogonalisation (a second pass only when the first
+//     removed more than ~30% of the vector),
+//   * Rayleigh-Ritz on the host in FP64; Ritz selection smallest / largest algebraic or closest to a target,
+//   * residual norm from ||r||^2 = s^H (AV^H AV) s - theta^2 while it is large, explicitly (x = V s,
+//     r = AV s - theta x) once it approaches the tolerance.
+// With an FP64 operator this phase runs to the tolerance: ||H x - theta x|| <= tol * ||H||_est
+// (PRIMME eps, solver_primme.cpp:364; ||H||_est = largest |Ritz value| seen).
 //
-// Mixed precision (op precision HEFF_PREC_MIXED, see mixed.cu): the Davidson phase runs on the
-// split-BF16 matvec until ||r|| <= mixed_tol * ||H||_est; then FP64 refinement steps follow, each one
-// FP64 matvec for the true residual r plus a correction (I - xx^H)(H - theta)(I - xx^H) d = -r solved
-// with the mixed matvec by a few MINRES-like (CG on the projected operator) iterations, x <- x + d.
+// Mixed precision (operator HEFF_PREC_MIXED): phase 1 runs on the split-BF16 matvec until its residual
+// reaches mixed_tol * ||H||_est or stops improving (the inexact operator floors it), then
+// Phase 2 -- Jacobi-Davidson refinement in FP64: an FP64 search space starting from the phase-1 Ritz
+// vector, FP64 products of every basis vector, FP64 Rayleigh-Ritz (so the energy can only improve);
+// each expansion vector is an approximate solution of the correction equation
+//   (I - u u^H)(H - theta)(I - u u^H) t = -r
+// by a few CG iterations on the mixed (cheap) matvec.  One FP64 matvec per refinement step.
 #include <chrono>
 #include <complex>
 #include <cstring>
+#include <numeric>
 #include <vector>
 
 #include "blas1.cuh"
@@ -41,16 +50,16 @@ template<>
 struct HostScalar<false> {
     using T = double;
     static double conj(double v) { return v; }
-    static double real(double v) { return v; }
+    static double re(double v) { return v; }
 };
 template<>
 struct HostScalar<true> {
     using T = std::complex<double>;
     static T      conj(T v) { return std::conj(v); }
-    static double real(T v) { return v.real(); }
+    static double re(T v) { return v.real(); }
 };
 
-// Ritz decomposition of the k x k projected matrix; returns ascending eigenvalues and vectors (column-major).
+// Ritz decomposition of the k x k projected matrix (leading dimension ld): ascending w, vectors column-major.
 template<bool CPLX>
 static int ritz(int k, const std::vector<typename HostScalar<CPLX>::T> &Hk, int ld, std::vector<double> &w,
                 std::vector<typename HostScalar<CPLX>::T> &vecs) {
@@ -69,7 +78,6 @@ static int ritz(int k, const std::vector<typename HostScalar<CPLX>::T> &Hk, int 
     return HEFF_OK;
 }
 
-// Order of Ritz values by the selection rule: indices into ascending w.
 static std::vector<int> ritz_order(const std::vector<double> &w, int rule, double target) {
     std::vector<int> o(w.size());
     std::iota(o.begin(), o.end(), 0);
@@ -82,18 +90,19 @@ template<bool CPLX>
 struct Davidson {
     using T  = typename Scalar<CPLX>::T;
     using HT = typename HostScalar<CPLX>::T;
-    heff_op                 *op;
-    const heff_eig_config   &cfg;
-    heff_eig_result         &res;
-    cudaStream_t             s;
-    int64_t                  n;
-    int                      maxb, minb;
-    T                       *V = nullptr, *AV = nullptr, *V2 = nullptr, *AV2 = nullptr, *t = nullptr, *x = nullptr, *ax = nullptr, *r = nullptr;
-    T                       *dh = nullptr, *dc = nullptr;
-    double                  *partials = nullptr, *dscal = nullptr;
-    std::vector<HT>          Hk;
-    std::vector<void *>      allocs;
-    double                   anorm = 0.0;
+    heff_op               *op;
+    const heff_eig_config &cfg;
+    heff_eig_result       &res;
+    cudaStream_t           s;
+    int64_t                n;
+    int                    maxb, minb;
+    T *V = nullptr, *AV = nullptr, *V2 = nullptr, *AV2 = nullptr, *t = nullptr, *x = nullptr, *ax = nullptr, *r = nullptr;
+    T *cg_p = nullptr, *cg_q = nullptr, *cg_z = nullptr, *cg_d = nullptr, *cg_r = nullptr;
+    T *dh = nullptr, *dc = nullptr;
+    double             *partials = nullptr, *dscal = nullptr;
+    std::vector<HT>     Hk, G2;
+    std::vector<void *> allocs;
+    double              anorm = 0.0;
 
     Davidson(heff_op *o, const heff_eig_config &c, heff_eig_result &r_) : op(o), cfg(c), res(r_), s(o->stream), n(o->d.size_mps()) {
         maxb = std::max(4, std::min(cfg.max_basis > 0 ? cfg.max_basis : 32, (int)MD_MAXK));
@@ -113,39 +122,62 @@ struct Davidson {
         allocs.push_back(*p);
         return HEFF_OK;
     }
-    int setup() {
+    int setup(bool mixed) {
         const size_t es = sizeof(T);
         HEFF_TRY(alloc((void **)&V, es * n * maxb));
         HEFF_TRY(alloc((void **)&AV, es * n * maxb));
         HEFF_TRY(alloc((void **)&V2, es * n * maxb));
         HEFF_TRY(alloc((void **)&AV2, es * n * maxb));
-        HEFF_TRY(alloc((void **)&t, es * n));
-        HEFF_TRY(alloc((void **)&x, es * n));
-        HEFF_TRY(alloc((void **)&ax, es * n));
-        HEFF_TRY(alloc((void **)&r, es * n));
-        HEFF_TRY(alloc((void **)&dh, es * MD_MAXK * 2));
+        for(T **p : {&t, &x, &ax, &r}) HEFF_TRY(alloc((void **)p, es * n));
+        if(mixed)
+            for(T **p : {&cg_p, &cg_q, &cg_z, &cg_d, &cg_r}) HEFF_TRY(alloc((void **)p, es * n));
+        HEFF_TRY(alloc((void **)&dh, es * MD_MAXK * 3));
         HEFF_TRY(alloc((void **)&dc, es * MD_MAXK * MD_MAXK));
-        HEFF_TRY(alloc((void **)&partials, sizeof(double) * MD_BLOCKS * MD_MAXK * 2));
-        HEFF_TRY(alloc((void **)&dscal, sizeof(double) * 8));
+        HEFF_TRY(alloc((void **)&partials, sizeof(double) * MD_BLOCKS * MD_MAXK * 4));
+        HEFF_TRY(alloc((void **)&dscal, sizeof(double) * 16));
         Hk.assign((size_t)maxb * maxb, HT(0));
+        G2.assign((size_t)maxb * maxb, HT(0));
         return HEFF_OK;
     }
-    // ||v||^2 -> host (synchronises)
-    int norm2(const T *v, double &out) {
-        T d;
-        HEFF_TRY(dot_device<CPLX>(v, v, n, reinterpret_cast<T *>(dscal), partials, s));
-        HEFF_CUDA(cudaMemcpyAsync(&d, dscal, sizeof(T), cudaMemcpyDeviceToHost, s));
+    int sync() {
         HEFF_CUDA(cudaStreamSynchronize(s));
-        if constexpr(CPLX)
-            out = d.x;
-        else
-            out = d;
         return HEFF_OK;
+    }
+    int dot(const T *a, const T *b, HT &out) {  // <a, b> -> host
+        T d;
+        HEFF_TRY(dot_device<CPLX>(a, b, n, reinterpret_cast<T *>(dscal), partials, s));
+        HEFF_CUDA(cudaMemcpyAsync(&d, dscal, sizeof(T), cudaMemcpyDeviceToHost, s));
+        HEFF_TRY(sync());
+        std::memcpy((void *)&out, (void *)&d, sizeof(T));
+        return HEFF_OK;
+    }
+    int norm2(const T *v, double &out) {
+        HT d;
+        HEFF_TRY(dot(v, v, d));
+        out = HostScalar<CPLX>::re(d);
+        return HEFF_OK;
+    }
+    // y += a * v (a real, host value)
+    int axpy(double a, const T *v, T *y) {
+        const T one = one_value();
+        HEFF_CUDA(cudaMemcpyAsync(dh + 2 * MD_MAXK, &one, sizeof(T), cudaMemcpyHostToDevice, s));
+        return multi_axpy<CPLX>(v, n, n, 1, dh + 2 * MD_MAXK, a, y, s);
+    }
+    int scale(T *v, double a) {
+        HEFF_CUDA(cudaMemcpyAsync(dscal + 8, &a, sizeof(double), cudaMemcpyHostToDevice, s));
+        HEFF_TRY(scale_dev<CPLX>(v, n, dscal + 8, false, s));
+        return sync();  // the host scalar above must stay valid until the copy ran
+    }
+    static T one_value() {
+        if constexpr(CPLX)
+            return make_double2(1.0, 0.0);
+        else
+            return 1.0;
     }
     int apply(const T *in, T *out, bool fp64) {
         const heff_precision keep = op->precision;
         if(fp64) op->precision = HEFF_PREC_FP64;
-        int rc = op_apply(op, in, out);
+        int rc        = op_apply(op, in, out);
         op->precision = keep;
         if(fp64 || keep == HEFF_PREC_FP64)
             res.num_mv_fp64++;
@@ -154,21 +186,26 @@ struct Davidson {
         res.num_mv++;
         return rc;
     }
-    // orthonormalise t against V[:, :k] (CGS2); returns the norm before normalisation (host)
-    int orthonormalize(int k, double &nrm) {
-        for(int pass = 0; pass < 2; pass++) {
-            HEFF_TRY(multi_dot<CPLX>(V, n, n, k, t, dh, partials, s));
-            HEFF_TRY(multi_axpy<CPLX>(V, n, n, k, dh, -1.0, t, s));
-        }
+    // Orthonormalise t against V[:, :k] (Gram-Schmidt, DGKS second pass when needed).
+    // nrm0: norm before, nrm: norm after (before normalisation).
+    int orthonormalize(T *Vb, int k, double &nrm0, double &nrm) {
         double n2 = 0;
         HEFF_TRY(norm2(t, n2));
-        nrm = std::sqrt(n2);
-        if(nrm > 0) {
-            const double inv = 1.0 / nrm;
-            HEFF_CUDA(cudaMemcpyAsync(dscal + 1, &inv, sizeof(double), cudaMemcpyHostToDevice, s));
-            HEFF_TRY(scale_dev<CPLX>(t, n, dscal + 1, false, s));
-            HEFF_CUDA(cudaStreamSynchronize(s));
+        nrm0 = std::sqrt(n2);
+        nrm  = nrm0;
+        for(int pass = 0; pass < 2 && k > 0; pass++) {
+            HEFF_TRY(multi_dot<CPLX>(Vb, n, n, k, t, dh, partials, s));
+            HEFF_TRY(multi_axpy<CPLX>(Vb, n, n, k, dh, -1.0, t, s));
+            const double before = nrm;
+            HEFF_TRY(norm2(t, n2));
+            nrm = std::sqrt(n2);
+            if(nrm > 0.7 * before) break;
         }
+        if(!std::isfinite(nrm)) {
+            set_last_error_msg("eigensolver: non-finite vector (NaN/Inf in the operator or start vector)");
+            return HEFF_NAN_INPUT;
+        }
+        if(nrm > 0) HEFF_TRY(scale(t, 1.0 / nrm));
         return HEFF_OK;
     }
     int random_vector(T *v, uint64_t seed) {
@@ -177,8 +214,78 @@ struct Davidson {
         HEFF_LAUNCH_CHECK();
         return HEFF_OK;
     }
+    // Append column k: V[:,k] = t (normalised), AV[:,k] = A t, projected-matrix column, AV-Gram column.
+    int append(int k, bool fp64, bool track_g2) {
+        HEFF_CUDA(cudaMemcpyAsync(V + (int64_t)k * n, t, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+        HEFF_TRY(apply(V + (int64_t)k * n, AV + (int64_t)k * n, fp64));
+        HEFF_TRY(multi_dot<CPLX>(V, n, n, k + 1, AV + (int64_t)k * n, dh, partials, s));
+        if(track_g2) HEFF_TRY(multi_dot<CPLX>(AV, n, n, k + 1, AV + (int64_t)k * n, dh + MD_MAXK, partials + 2 * MD_BLOCKS * MD_MAXK, s));
+        std::vector<T> col(2 * (k + 1));
+        HEFF_CUDA(cudaMemcpyAsync(col.data(), dh, sizeof(T) * (k + 1), cudaMemcpyDeviceToHost, s));
+        if(track_g2) HEFF_CUDA(cudaMemcpyAsync(col.data() + (k + 1), dh + MD_MAXK, sizeof(T) * (k + 1), cudaMemcpyDeviceToHost, s));
+        HEFF_TRY(sync());
+        for(int i = 0; i <= k; i++) {
+            HT v;
+            std::memcpy((void *)&v, (void *)&col[i], sizeof(T));
+            Hk[i + (size_t)maxb * k] = v;
+            Hk[k + (size_t)maxb * i] = HostScalar<CPLX>::conj(v);
+            if(track_g2) {
+                std::memcpy((void *)&v, (void *)&col[k + 1 + i], sizeof(T));
+                G2[i + (size_t)maxb * k] = v;
+                G2[k + (size_t)maxb * i] = HostScalar<CPLX>::conj(v);
+            }
+        }
+        return HEFF_OK;
+    }
+    // x = V s, ax = AV s, r = ax - theta x ; returns ||r||
+    int explicit_residual(int k, const HT *svec, double theta, double &rn) {
+        HEFF_CUDA(cudaMemcpyAsync(dc, (const void *)svec, sizeof(T) * k, cudaMemcpyHostToDevice, s));
+        HEFF_TRY(combine<CPLX>(V, n, n, k, dc, x, s));
+        HEFF_TRY(combine<CPLX>(AV, n, n, k, dc, ax, s));
+        HEFF_TRY(residual<CPLX>(ax, x, theta, r, n, s));
+        double r2 = 0;
+        HEFF_TRY(norm2(r, r2));
+        rn = std::sqrt(r2);
+        return HEFF_OK;
+    }
+    // thick restart to the m best Ritz vectors
+    int restart(int k, int m, const std::vector<double> &w, const std::vector<HT> &vecs, const std::vector<int> &ord, bool track_g2) {
+        std::vector<HT> S((size_t)k * m);
+        for(int q = 0; q < m; q++)
+            for(int i = 0; i < k; i++) S[i + (size_t)k * q] = vecs[i + (size_t)k * ord[q]];
+        HEFF_CUDA(cudaMemcpyAsync(dc, (const void *)S.data(), sizeof(T) * k * m, cudaMemcpyHostToDevice, s));
+        GemmArgs g{};
+        g.M = (int)n, g.N = m, g.K = k, g.batch = 1;
+        g.A = V, g.lda = n, g.B = dc, g.ldb = k, g.C = V2, g.ldc = n;
+        g.alpha = make_double2(1, 0), g.beta = make_double2(0, 0);
+        HEFF_TRY(gemm_f64<CPLX>(false, false, false, g, s));
+        g.A = AV, g.C = AV2;
+        HEFF_TRY(gemm_f64<CPLX>(false, false, false, g, s));
+        std::swap(V, V2);
+        std::swap(AV, AV2);
+        if(track_g2) {  // G2 <- S^H G2 S
+            std::vector<HT> tmp((size_t)k * m, HT(0)), g2n((size_t)maxb * maxb, HT(0));
+            for(int q = 0; q < m; q++)
+                for(int i = 0; i < k; i++) {
+                    HT acc(0);
+                    for(int j = 0; j < k; j++) acc += G2[i + (size_t)maxb * j] * S[j + (size_t)k * q];
+                    tmp[i + (size_t)k * q] = acc;
+                }
+            for(int q = 0; q < m; q++)
+                for(int p = 0; p < m; p++) {
+                    HT acc(0);
+                    for(int i = 0; i < k; i++) acc += HostScalar<CPLX>::conj(S[i + (size_t)k * p]) * tmp[i + (size_t)k * q];
+                    g2n[p + (size_t)maxb * q] = acc;
+                }
+            G2.swap(g2n);
+        }
+        std::fill(Hk.begin(), Hk.end(), HT(0));
+        for(int q = 0; q < m; q++) Hk[q + (size_t)maxb * q] = HT(w[ord[q]]);
+        res.restarts++;
+        return sync();  // S must outlive its copy
+    }
 
-    // Davidson phase.  fp64_only forces FP64 matvecs.  stop_tol: relative residual target.
+    // Phase 1.  Returns with x = Ritz vector (normalised), theta, rnorm (explicit when conv).
     int run(const void *x0, bool use_mixed, double stop_tol, int64_t max_mv, double &theta, double &rnorm, bool &conv) {
         int k = 0;
         if(x0)
@@ -192,202 +299,145 @@ struct Davidson {
         std::vector<HT>     vecs;
         int                 stagn = 0;
         double              best  = INFINITY;
+        const bool          track = true;
+        std::vector<HT>     sbest;
         while(true) {
-            double nrm = 0;
-            HEFF_TRY(orthonormalize(k, nrm));
-            if(!(nrm > 1e-14) || !std::isfinite(nrm)) {
-                if(!std::isfinite(nrm)) {
-                    set_last_error_msg("eigensolver: non-finite vector (NaN/Inf in the operator or start vector)");
-                    return HEFF_NAN_INPUT;
-                }
-                // breakdown: the residual lies in the basis; continue with a fresh random direction
+            double n0 = 0, nrm = 0;
+            HEFF_TRY(orthonormalize(V, k, n0, nrm));
+            if(!(nrm > 1e-10 * n0) || !(nrm > 0)) {
+                // breakdown (invariant subspace): continue with a fresh random direction
                 HEFF_TRY(random_vector(t, 0xabcdefULL + (uint64_t)res.num_mv));
-                HEFF_TRY(orthonormalize(k, nrm));
-                if(!(nrm > 1e-14)) break;
+                HEFF_TRY(orthonormalize(V, k, n0, nrm));
+                if(!(nrm > 1e-10 * n0)) break;
             }
-            HEFF_CUDA(cudaMemcpyAsync(V + (int64_t)k * n, t, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-            HEFF_TRY(apply(V + (int64_t)k * n, AV + (int64_t)k * n, !use_mixed));
-            // new column of the projected matrix
-            HEFF_TRY(multi_dot<CPLX>(V, n, n, k + 1, AV + (int64_t)k * n, dh, partials, s));
-            std::vector<T> col(k + 1);
-            HEFF_CUDA(cudaMemcpyAsync(col.data(), dh, sizeof(T) * (k + 1), cudaMemcpyDeviceToHost, s));
-            HEFF_CUDA(cudaStreamSynchronize(s));
-            for(int i = 0; i <= k; i++) {
-                HT v;
-                std::memcpy((void *)&v, (void *)&col[i], sizeof(T));
-                Hk[i + (size_t)maxb * k] = v;
-                Hk[k + (size_t)maxb * i] = HostScalar<CPLX>::conj(v);
-            }
+            HEFF_TRY(append(k, !use_mixed, track));
             k++;
             HEFF_TRY(ritz<CPLX>(k, Hk, maxb, w, vecs));
             for(double wi : w) anorm = std::max(anorm, std::fabs(wi));
             const std::vector<int> ord = ritz_order(w, cfg.ritz, cfg.target);
             const int              j0  = ord[0];
             theta                      = w[j0];
-            // x = V s, ax = AV s, r = ax - theta x
-            HEFF_CUDA(cudaMemcpyAsync(dc, (const void *)(vecs.data() + (size_t)k * j0), sizeof(T) * k, cudaMemcpyHostToDevice, s));
-            HEFF_TRY(combine<CPLX>(V, n, n, k, dc, x, s));
-            HEFF_TRY(combine<CPLX>(AV, n, n, k, dc, ax, s));
-            HEFF_TRY(residual<CPLX>(ax, x, theta, r, n, s));
-            double r2 = 0;
-            HEFF_TRY(norm2(r, r2));
-            rnorm = std::sqrt(r2);
+            const HT              *sv  = vecs.data() + (size_t)k * j0;
+            // residual estimate ||r||^2 = s^H G2 s - theta^2
+            double q = 0;
+            for(int jj = 0; jj < k; jj++)
+                for(int ii = 0; ii < k; ii++) q += HostScalar<CPLX>::re(HostScalar<CPLX>::conj(sv[ii]) * G2[ii + (size_t)maxb * jj] * sv[jj]);
+            double       rest   = std::sqrt(std::max(0.0, q - theta * theta));
+            const double floor_ = 3e-8 * std::max(anorm, std::fabs(theta));  // where the estimate loses accuracy
+            if(rest <= std::max(floor_, 4 * stop_tol * anorm) || res.num_mv >= max_mv) {
+                HEFF_TRY(explicit_residual(k, sv, theta, rest));
+            }
+            rnorm = rest;
             res.iters++;
             if(!std::isfinite(rnorm)) {
                 set_last_error_msg("eigensolver: non-finite residual");
                 return HEFF_NAN_INPUT;
             }
             if(rnorm <= stop_tol * std::max(anorm, 1e-300)) {
+                if(rnorm != rest) HEFF_TRY(explicit_residual(k, sv, theta, rnorm));
                 conv = true;
                 break;
             }
-            // stagnation guard for the mixed phase (the inexact operator floors the residual)
-            if(use_mixed) {
-                if(rnorm < 0.9 * best) {
+            if(use_mixed) {  // stop when the inexact operator floors the residual
+                if(rnorm < 0.5 * best) {
                     best  = rnorm;
                     stagn = 0;
-                } else if(++stagn >= 12) {
+                } else if(++stagn >= 20) {
+                    HEFF_TRY(explicit_residual(k, sv, theta, rnorm));
                     break;
                 }
             }
             if(res.num_mv >= max_mv) break;
+            int kk = k;
             if(k == maxb) {
-                // thick restart: keep the minb best Ritz vectors
-                std::vector<HT> S((size_t)maxb * minb);
-                for(int q = 0; q < minb; q++)
-                    for(int i = 0; i < k; i++) S[i + (size_t)maxb * q] = vecs[i + (size_t)k * ord[q]];
-                HEFF_CUDA(cudaMemcpyAsync(dc, (const void *)S.data(), sizeof(T) * maxb * minb, cudaMemcpyHostToDevice, s));
-                GemmArgs g{};
-                g.M = (int)n, g.N = minb, g.K = k, g.batch = 1;
-                g.A = V, g.lda = n, g.B = dc, g.ldb = maxb, g.C = V2, g.ldc = n;
-                g.alpha = make_double2(1, 0), g.beta = make_double2(0, 0);
-                HEFF_TRY(gemm_f64<CPLX>(false, false, false, g, s));
-                g.A = AV, g.C = AV2;
-                HEFF_TRY(gemm_f64<CPLX>(false, false, false, g, s));
-                std::swap(V, V2);
-                std::swap(AV, AV2);
-                std::fill(Hk.begin(), Hk.end(), HT(0));
-                for(int q = 0; q < minb; q++) Hk[q + (size_t)maxb * q] = HT(w[ord[q]]);
-                k = minb;
-                res.restarts++;
-                HEFF_CUDA(cudaStreamSynchronize(s));  // S must outlive the copy
+                HEFF_TRY(restart(k, minb, w, vecs, ord, track));
+                kk = minb;
             }
-            HEFF_CUDA(cudaMemcpyAsync(t, r, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+            // expansion: A v_last (already computed)
+            HEFF_CUDA(cudaMemcpyAsync(t, AV + (int64_t)(kk - 1) * n, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+            k = kk;
         }
         return HEFF_OK;
     }
 
-    // FP64 refinement of (x, theta): each step one FP64 matvec for the true residual and a correction
-    // solved with the mixed operator by CG on (I - xx^H)(H - theta)(I - xx^H), restricted to x^perp.
+    // CG on (I - u u^H)(H_mixed - theta)(I - u u^H) d = -r0 restricted to u^perp; d -> cg_d
+    int correction(const T *u, const T *r0, double theta, double r0n) {
+        HEFF_CUDA(cudaMemsetAsync(cg_d, 0, sizeof(T) * n, s));
+        HEFF_CUDA(cudaMemcpyAsync(cg_r, r0, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+        HEFF_TRY(scale(cg_r, -1.0));
+        HEFF_CUDA(cudaMemcpyAsync(cg_p, cg_r, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+        double rho = r0n * r0n;
+        const double rho0 = rho;
+        for(int it = 0; it < cfg.inner_iters; it++) {
+            HEFF_TRY(apply(cg_p, cg_z, false));
+            HEFF_TRY(residual<CPLX>(cg_z, cg_p, theta, cg_q, n, s));  // q = (H - theta) p
+            HEFF_TRY(multi_dot<CPLX>(u, n, n, 1, cg_q, dh, partials, s));
+            HEFF_TRY(multi_axpy<CPLX>(u, n, n, 1, dh, -1.0, cg_q, s));  // q <- P q
+            HT pq;
+            HEFF_TRY(dot(cg_p, cg_q, pq));
+            const double pqr = HostScalar<CPLX>::re(pq);
+            if(!(pqr > 0)) break;  // indefinite direction: keep what we have
+            const double alpha = rho / pqr;
+            HEFF_TRY(axpy(alpha, cg_p, cg_d));
+            HEFF_TRY(axpy(-alpha, cg_q, cg_r));
+            double rho_new = 0;
+            HEFF_TRY(norm2(cg_r, rho_new));
+            if(rho_new <= cfg.inner_tol * cfg.inner_tol * rho0) break;
+            HEFF_TRY(scale(cg_p, rho_new / rho));
+            HEFF_TRY(axpy(1.0, cg_r, cg_p));
+            rho = rho_new;
+        }
+        return HEFF_OK;
+    }
+
+    // Phase 2: Jacobi-Davidson in FP64 starting from x (normalised).
     int refine(double &theta, double &rnorm, bool &conv) {
-        T *p = V, *q = V + n, *z = V + 2 * n, *d = V + 3 * n, *rr = V + 4 * n;  // reuse the basis storage
-        for(int outer = 0; outer < 12; outer++) {
-            HEFF_TRY(apply(x, ax, true));
-            // theta = <x, Hx> (x normalised), r = Hx - theta x
-            T th;
-            HEFF_TRY(dot_device<CPLX>(x, ax, n, reinterpret_cast<T *>(dscal), partials, s));
-            HEFF_CUDA(cudaMemcpyAsync(&th, dscal, sizeof(T), cudaMemcpyDeviceToHost, s));
-            HEFF_CUDA(cudaStreamSynchronize(s));
-            if constexpr(CPLX)
-                theta = th.x;
-            else
-                theta = th;
-            HEFF_TRY(residual<CPLX>(ax, x, theta, r, n, s));
-            double r2 = 0;
-            HEFF_TRY(norm2(r, r2));
-            rnorm = std::sqrt(r2);
-            anorm = std::max(anorm, std::fabs(theta));
+        conv  = false;
+        int k = 0;
+        HEFF_CUDA(cudaMemcpyAsync(t, x, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+        std::fill(Hk.begin(), Hk.end(), HT(0));
+        std::vector<double> w;
+        std::vector<HT>     vecs;
+        const int           kmax = std::min(maxb, 24);
+        for(int outer = 0; outer < 60; outer++) {
+            double n0 = 0, nrm = 0;
+            HEFF_TRY(orthonormalize(V, k, n0, nrm));
+            if(!(nrm > 1e-12 * n0) || !(nrm > 0)) break;  // correction lies in the space: nothing new
+            HEFF_TRY(append(k, true, false));
+            k++;
+            HEFF_TRY(ritz<CPLX>(k, Hk, maxb, w, vecs));
+            for(double wi : w) anorm = std::max(anorm, std::fabs(wi));
+            const std::vector<int> ord = ritz_order(w, cfg.ritz, cfg.target);
+            theta                      = w[ord[0]];
+            HEFF_TRY(explicit_residual(k, vecs.data() + (size_t)k * ord[0], theta, rnorm));
             res.refine_steps++;
             if(rnorm <= cfg.tol * anorm) {
                 conv = true;
                 return HEFF_OK;
             }
             if(res.num_mv >= cfg.max_matvecs) return HEFF_OK;
-            // CG for A d = -r with A = P (H_mixed - theta) P, P = I - x x^H; d starts at 0
-            HEFF_CUDA(cudaMemcpyAsync(rr, r, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-            const double  minus1 = -1.0;
-            HEFF_CUDA(cudaMemcpyAsync(dscal + 2, &minus1, sizeof(double), cudaMemcpyHostToDevice, s));
-            HEFF_TRY(scale_dev<CPLX>(rr, n, dscal + 2, false, s));  // rr = -r (residual of the linear system at d = 0)
-            HEFF_CUDA(cudaMemsetAsync(d, 0, sizeof(T) * n, s));
-            HEFF_CUDA(cudaMemcpyAsync(p, rr, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-            double rho = r2, rho0 = r2;
-            for(int it = 0; it < cfg.inner_iters; it++) {
-                // q = P (H - theta) P p   (p stays in x^perp)
-                HEFF_TRY(apply(p, z, false));
-                HEFF_TRY(residual<CPLX>(z, p, theta, q, n, s));
-                HEFF_TRY(multi_dot<CPLX>(x, n, n, 1, q, dh, partials, s));
-                HEFF_TRY(multi_axpy<CPLX>(x, n, n, 1, dh, -1.0, q, s));
-                T pq;
-                HEFF_TRY(dot_device<CPLX>(p, q, n, reinterpret_cast<T *>(dscal), partials, s));
-                HEFF_CUDA(cudaMemcpyAsync(&pq, dscal, sizeof(T), cudaMemcpyDeviceToHost, s));
-                HEFF_CUDA(cudaStreamSynchronize(s));
-                double pqr;
-                if constexpr(CPLX)
-                    pqr = pq.x;
-                else
-                    pqr = pq;
-                if(!(std::fabs(pqr) > 0)) break;
-                const double alpha = rho / pqr;
-                double       a2[2] = {alpha, -alpha};
-                HEFF_CUDA(cudaMemcpyAsync(dscal + 3, a2, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
-                HEFF_TRY(axpy_dev(p, d, dscal + 3));   // d += alpha p
-                HEFF_TRY(axpy_dev(q, rr, dscal + 4));  // rr -= alpha q
-                double rho_new = 0;
-                HEFF_TRY(norm2(rr, rho_new));
-                if(rho_new <= cfg.inner_tol * cfg.inner_tol * rho0) break;
-                const double beta = rho_new / rho;
-                rho               = rho_new;
-                // p = rr + beta p
-                HEFF_CUDA(cudaMemcpyAsync(dscal + 5, &beta, sizeof(double), cudaMemcpyHostToDevice, s));
-                HEFF_TRY(scale_dev<CPLX>(p, n, dscal + 5, false, s));
-                const double one = 1.0;
-                HEFF_CUDA(cudaMemcpyAsync(dscal + 6, &one, sizeof(double), cudaMemcpyHostToDevice, s));
-                HEFF_TRY(axpy_dev(rr, p, dscal + 6));
-                HEFF_CUDA(cudaStreamSynchronize(s));
+            if(k == kmax) {
+                HEFF_TRY(restart(k, 4, w, vecs, ord, false));
+                k = 4;
             }
-            // x <- (x + d) / ||x + d||
-            const double one = 1.0;
-            HEFF_CUDA(cudaMemcpyAsync(dscal + 6, &one, sizeof(double), cudaMemcpyHostToDevice, s));
-            HEFF_TRY(axpy_dev(d, x, dscal + 6));
-            double xn = 0;
-            HEFF_TRY(norm2(x, xn));
-            const double inv = 1.0 / std::sqrt(xn);
-            HEFF_CUDA(cudaMemcpyAsync(dscal + 1, &inv, sizeof(double), cudaMemcpyHostToDevice, s));
-            HEFF_TRY(scale_dev<CPLX>(x, n, dscal + 1, false, s));
-            HEFF_CUDA(cudaStreamSynchronize(s));
+            HEFF_TRY(correction(x, r, theta, rnorm));
+            HEFF_CUDA(cudaMemcpyAsync(t, cg_d, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
         }
         return HEFF_OK;
-    }
-    // y += a * v  (a read on the device)
-    int axpy_dev(const T *v, T *y, const double *a) {
-        // multi_axpy with k = 1 and h = 1 scaled by alpha: y += alpha * v * h; use dh[0] = 1
-        const T one_t = one_value();
-        HEFF_CUDA(cudaMemcpyAsync(dh + MD_MAXK, &one_t, sizeof(T), cudaMemcpyHostToDevice, s));
-        double ah = 0;
-        HEFF_CUDA(cudaMemcpyAsync(&ah, a, sizeof(double), cudaMemcpyDeviceToHost, s));
-        HEFF_CUDA(cudaStreamSynchronize(s));
-        return multi_axpy<CPLX>(v, n, n, 1, dh + MD_MAXK, ah, y, s);
-    }
-    static T one_value() {
-        if constexpr(CPLX)
-            return make_double2(1.0, 0.0);
-        else
-            return 1.0;
     }
 };
 
 template<bool CPLX>
 static int eigs_impl(heff_op *op, const heff_eig_config &cfg, const void *x0, void *x_out, heff_eig_result &res) {
-    using T = typename Scalar<CPLX>::T;
-    auto                t0 = std::chrono::steady_clock::now();
-    Davidson<CPLX>      D(op, cfg, res);
-    HEFF_TRY(D.setup());
+    using T          = typename Scalar<CPLX>::T;
+    auto       t0    = std::chrono::steady_clock::now();
+    const bool mixed = cfg.mixed && op->precision == HEFF_PREC_MIXED && op->mixed_apply;
+    Davidson<CPLX> D(op, cfg, res);
+    HEFF_TRY(D.setup(mixed));
     double theta = 0, rnorm = INFINITY;
     bool   conv  = false;
-    const bool mixed = cfg.mixed && op->precision == HEFF_PREC_MIXED && op->mixed_apply;
     if(mixed) {
-        HEFF_TRY(D.run(x0, true, cfg.mixed_tol > 0 ? cfg.mixed_tol : 1e-6, cfg.max_matvecs, theta, rnorm, conv));
-        conv = false;
+        HEFF_TRY(D.run(x0, true, cfg.mixed_tol > 0 ? cfg.mixed_tol : 1e-5, cfg.max_matvecs, theta, rnorm, conv));
         res.num_mv_phase1 = res.num_mv;
         HEFF_TRY(D.refine(theta, rnorm, conv));
     } else {
@@ -420,13 +470,13 @@ extern "C" void heff_eig_config_default(heff_eig_config *cfg) {
     cfg->ritz        = HEFF_RITZ_SA;
     cfg->target      = 0.0;
     cfg->tol         = 1e-12;  // solver.cpp:378 default tolerance
-    cfg->max_basis   = 32;
+    cfg->max_basis   = 24;
     cfg->min_basis   = 8;
     cfg->max_matvecs = 20000;
     cfg->mixed       = 1;
-    cfg->mixed_tol   = 1e-6;
-    cfg->inner_iters = 40;
-    cfg->inner_tol   = 1e-4;
+    cfg->mixed_tol   = 1e-5;
+    cfg->inner_iters = 30;
+    cfg->inner_tol   = 1e-3;
     cfg->seed        = 0;
 }
 
