@@ -32,58 +32,80 @@ struct VOps<double2> {
     static __device__ __forceinline__ double2 addscaled(double2 y, double a, double2 x) { return make_double2(fma(a, x.x, y.x), fma(a, x.y, y.y)); }
 };
 
-// partials[(blk * k + j) * 2 + {0,1}]
+// Partial sums of h[j] = sum_i conj(V[i,j]) t[i], MD_G columns per pass: every thread streams rows
+// (coalesced across the warp, one load per column per row) into MD_G register accumulators, then the
+// block reduces them.  partials[(j * nb + blk) * 2 + {0,1}] (column-major over blocks for the final pass).
+constexpr int MD_G = 8;
 template<class T>
 __global__ void __launch_bounds__(256) multi_dot_partial(const T *__restrict__ V, int64_t ldv, int64_t n, int k, const T *__restrict__ t,
                                                         double *__restrict__ partials) {
-    __shared__ double sre[8][MD_MAXK], sim[8][MD_MAXK];
+    constexpr bool CPLX = sizeof(T) == 16;
+    __shared__ double sre[8][MD_G], sim[8][MD_G];
     const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for(int j0 = 0; j0 < k; j0 += 32) {
-        const int jn = min(32, k - j0);
-        double    re[32], im[32];
+    const int         nb   = gridDim.x;
+    for(int j0 = 0; j0 < k; j0 += MD_G) {
+        const int jn = min(MD_G, k - j0);
+        double    re[MD_G], im[MD_G];
 #pragma unroll
-        for(int q = 0; q < 32; q++) re[q] = im[q] = 0.0;
+        for(int q = 0; q < MD_G; q++) re[q] = im[q] = 0.0;
+        const T *Vj = V + ldv * j0;
         for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
             const T tv = t[i];
+            if(jn == MD_G) {
 #pragma unroll
-            for(int q = 0; q < 32; q++)
-                if(q < jn) VOps<T>::dot_acc(re[q], im[q], V[i + ldv * (j0 + q)], tv);
+                for(int q = 0; q < MD_G; q++) VOps<T>::dot_acc(re[q], im[q], Vj[i + ldv * q], tv);
+            } else {
+                for(int q = 0; q < jn; q++) VOps<T>::dot_acc(re[q], im[q], Vj[i + ldv * q], tv);
+            }
         }
 #pragma unroll
-        for(int q = 0; q < 32; q++) {
+        for(int q = 0; q < MD_G; q++) {
             double a = re[q], b = im[q];
             for(int o = 16; o > 0; o >>= 1) {
                 a += __shfl_xor_sync(0xffffffffu, a, o);
-                b += __shfl_xor_sync(0xffffffffu, b, o);
+                if(CPLX) b += __shfl_xor_sync(0xffffffffu, b, o);
             }
-            if(lane == 0 && q < jn) {
-                sre[warp][j0 + q] = a;
-                sim[warp][j0 + q] = b;
+            if(lane == 0) {
+                sre[warp][q] = a;
+                sim[warp][q] = b;
             }
         }
-    }
-    __syncthreads();
-    for(int j = threadIdx.x; j < k; j += blockDim.x) {
-        double a = 0, b = 0;
-        for(int w = 0; w < 8; w++) {
-            a += sre[w][j];
-            b += sim[w][j];
+        __syncthreads();
+        if(threadIdx.x < jn) {
+            double a = 0, b = 0;
+            for(int w = 0; w < 8; w++) {
+                a += sre[w][threadIdx.x];
+                b += sim[w][threadIdx.x];
+            }
+            const int64_t j = j0 + threadIdx.x;
+            partials[(j * nb + blockIdx.x) * 2 + 0] = a;
+            partials[(j * nb + blockIdx.x) * 2 + 1] = b;
         }
-        partials[((int64_t)blockIdx.x * k + j) * 2 + 0] = a;
-        partials[((int64_t)blockIdx.x * k + j) * 2 + 1] = b;
+        __syncthreads();
     }
 }
 
+// One block per column: fixed-order tree reduction of the nb partial sums.
 template<class T>
-__global__ void multi_dot_final(const double *__restrict__ partials, int nb, int k, T *__restrict__ h) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if(j >= k) return;
-    double a = 0, b = 0;
-    for(int blk = 0; blk < nb; blk++) {
-        a += partials[((int64_t)blk * k + j) * 2 + 0];
-        b += partials[((int64_t)blk * k + j) * 2 + 1];
+__global__ void __launch_bounds__(256) multi_dot_final(const double *__restrict__ partials, int nb, int k, T *__restrict__ h) {
+    __shared__ double sa[256], sb[256];
+    const int         j = blockIdx.x;
+    double            a = 0, b = 0;
+    for(int blk = threadIdx.x; blk < nb; blk += blockDim.x) {
+        a += partials[((int64_t)j * nb + blk) * 2 + 0];
+        b += partials[((int64_t)j * nb + blk) * 2 + 1];
     }
-    h[j] = VOps<T>::make(a, b);
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for(int w = 128; w > 0; w >>= 1) {
+        if(threadIdx.x < w) {
+            sa[threadIdx.x] += sa[threadIdx.x + w];
+            sb[threadIdx.x] += sb[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) h[j] = VOps<T>::make(sa[0], sb[0]);
 }
 
 template<class T>
@@ -135,10 +157,10 @@ int multi_dot(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, 
     using T = typename Scalar<CPLX>::T;
     if(k <= 0) return HEFF_OK;
     if(k > MD_MAXK) return HEFF_BAD_ARG;
-    const int nb = (int)std::min<int64_t>(MD_BLOCKS, std::max<int64_t>(1, (n + 255) / 256));
+    const int nb = (int)std::min<int64_t>(std::min<int64_t>(MD_BLOCKS, 4 * (int64_t)device_sm_count()), std::max<int64_t>(1, (n + 255) / 256));
     multi_dot_partial<T><<<nb, 256, 0, s>>>(V, ldv, n, k, t, partials);
     HEFF_LAUNCH_CHECK();
-    multi_dot_final<T><<<(k + 127) / 128, 128, 0, s>>>(partials, nb, k, h);
+    multi_dot_final<T><<<k, 256, 0, s>>>(partials, nb, k, h);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }

@@ -1,14 +1,15 @@
 // Device eigensolver for H_eff, driving the operator through the same apply path the reference's
 // PRIMME/ARPACK callback uses (MatVecMPOS::MultAx, solver_primme.cpp:122-128).
 //
-// Phase 1 -- thick-restart Davidson without preconditioner (a restarted Krylov method):
+// Phase 1 -- thick-restart Davidson without preconditioner, i.e. a restarted Krylov (Lanczos) method:
 //   * expansion with A v_last (for a Hermitian operator this spans the same Krylov space as expanding
-//     with the Ritz residual, also after a thick restart, and needs no extra pass over the basis),
+//     with the Ritz residual, also after a thick restart); the projection coefficients of A v_last on
+//     the basis are the new column of the Rayleigh-Ritz matrix, so one pass over the basis per iteration,
 //   * FP64 Gram-Schmidt with DGKS selective re-orthogonalisation (a second pass only when the first
-//     removed more than ~30% of the vector),
+//     removed more than half of the vector's norm squared),
 //   * Rayleigh-Ritz on the host in FP64; Ritz selection smallest / largest algebraic or closest to a target,
-//   * residual norm from ||r||^2 = s^H (AV^H AV) s - theta^2 while it is large, explicitly (x = V s,
-//     r = AV s - theta x) once it approaches the tolerance.
+//   * residual norm |beta s_last| from the Krylov relation, checked explicitly (x = V s, r = AV s - theta x)
+//     before convergence is declared.
 // With an FP64 operator this phase runs to the tolerance: ||H x - theta x|| <= tol * ||H||_est
 // (PRIMME eps, solver_primme.cpp:364; ||H||_est = largest |Ritz value| seen).
 //
@@ -105,36 +106,55 @@ struct Davidson {
     double              anorm = 0.0;
 
     Davidson(heff_op *o, const heff_eig_config &c, heff_eig_result &r_) : op(o), cfg(c), res(r_), s(o->stream), n(o->d.size_mps()) {
-        maxb = std::max(4, std::min(cfg.max_basis > 0 ? cfg.max_basis : 32, (int)MD_MAXK));
+        maxb = std::max(4, std::min(cfg.max_basis > 0 ? cfg.max_basis : 32, (int)MD_MAXK - 1));
         minb = std::max(1, std::min(cfg.min_basis > 0 ? cfg.min_basis : 8, maxb - 2));
         if((int64_t)maxb > n) maxb = (int)std::max<int64_t>(1, n);
         if(minb >= maxb) minb = std::max(1, maxb - 1);
     }
-    ~Davidson() {
-        for(void *p : allocs) cudaFree(p);
-    }
-    int alloc(void **p, size_t bytes) {
-        cudaError_t e = cudaMalloc(p, bytes);
-        if(e != cudaSuccess) {
-            set_last_cuda_error(e, "eigensolver workspace", __FILE__, __LINE__);
-            return HEFF_OOM;
-        }
-        allocs.push_back(*p);
+    // All device buffers are carved from the operator's eigensolver workspace, which persists across
+    // solves on the same operator (no allocation per solve once it has grown to size).
+    char  *carve_ptr = nullptr;
+    size_t carve_left = 0;
+    int    take(void **p, size_t bytes) {
+        bytes = (bytes + 255) / 256 * 256;
+        if(bytes > carve_left) return HEFF_OOM;
+        *p = carve_ptr;
+        carve_ptr += bytes;
+        carve_left -= bytes;
         return HEFF_OK;
     }
     int setup(bool mixed) {
-        const size_t es = sizeof(T);
-        HEFF_TRY(alloc((void **)&V, es * n * maxb));
-        HEFF_TRY(alloc((void **)&AV, es * n * maxb));
-        HEFF_TRY(alloc((void **)&V2, es * n * maxb));
-        HEFF_TRY(alloc((void **)&AV2, es * n * maxb));
-        for(T **p : {&t, &x, &ax, &r}) HEFF_TRY(alloc((void **)p, es * n));
+        const size_t es  = sizeof(T);
+        const size_t vec = (es * n + 255) / 256 * 256;
+        const size_t need = vec * (2 * (maxb + 1) + 2 * maxb + 4 + (mixed ? 5 : 0)) + es * MD_MAXK * 3 + es * MD_MAXK * MD_MAXK +
+                            sizeof(double) * MD_BLOCKS * MD_MAXK * 4 + 16 * sizeof(double) + 16 * 256;
+        if(op->eig_ws_bytes < need) {
+            if(op->eig_ws) {
+                HEFF_CUDA(cudaStreamSynchronize(s));
+                cudaFree(op->eig_ws);
+                op->eig_ws       = nullptr;
+                op->eig_ws_bytes = 0;
+            }
+            cudaError_t e = cudaMalloc(&op->eig_ws, need);
+            if(e != cudaSuccess) {
+                set_last_cuda_error(e, "eigensolver workspace", __FILE__, __LINE__);
+                return HEFF_OOM;
+            }
+            op->eig_ws_bytes = need;
+        }
+        carve_ptr  = reinterpret_cast<char *>(op->eig_ws);
+        carve_left = op->eig_ws_bytes;
+        HEFF_TRY(take((void **)&V, es * n * (maxb + 1)));  // column maxb holds the next Krylov vector
+        HEFF_TRY(take((void **)&AV, es * n * maxb));
+        HEFF_TRY(take((void **)&V2, es * n * (maxb + 1)));
+        HEFF_TRY(take((void **)&AV2, es * n * maxb));
+        for(T **p : {&t, &x, &ax, &r}) HEFF_TRY(take((void **)p, es * n));
         if(mixed)
-            for(T **p : {&cg_p, &cg_q, &cg_z, &cg_d, &cg_r}) HEFF_TRY(alloc((void **)p, es * n));
-        HEFF_TRY(alloc((void **)&dh, es * MD_MAXK * 3));
-        HEFF_TRY(alloc((void **)&dc, es * MD_MAXK * MD_MAXK));
-        HEFF_TRY(alloc((void **)&partials, sizeof(double) * MD_BLOCKS * MD_MAXK * 4));
-        HEFF_TRY(alloc((void **)&dscal, sizeof(double) * 16));
+            for(T **p : {&cg_p, &cg_q, &cg_z, &cg_d, &cg_r}) HEFF_TRY(take((void **)p, es * n));
+        HEFF_TRY(take((void **)&dh, es * MD_MAXK * 3));
+        HEFF_TRY(take((void **)&dc, es * MD_MAXK * MD_MAXK));
+        HEFF_TRY(take((void **)&partials, sizeof(double) * MD_BLOCKS * MD_MAXK * 4));
+        HEFF_TRY(take((void **)&dscal, sizeof(double) * 16));
         Hk.assign((size_t)maxb * maxb, HT(0));
         G2.assign((size_t)maxb * maxb, HT(0));
         return HEFF_OK;
@@ -285,77 +305,128 @@ struct Davidson {
         return sync();  // S must outlive its copy
     }
 
-    // Phase 1.  Returns with x = Ritz vector (normalised), theta, rnorm (explicit when conv).
+    double inv_beta_ = 1.0;  // host source of an async copy: must outlive it
+
+    // Phase 1 (thick-restart Krylov / Lanczos structure).  With w = A v_{k-1} projected out of V_k,
+    //   A V_k = V_k H_k + beta v_k e_k^H,
+    // so the projection coefficients ARE the last column of the Rayleigh-Ritz matrix H_k and the Ritz
+    // residual norm is |beta * s_{k-1}|: one pass over the basis per iteration (two when DGKS triggers).
+    // A thick restart keeps Y = V_k S_m (all residuals along v_k) and appends v_k, preserving the relation.
+    // Returns x = Ritz vector (normalised), theta, rnorm (explicit when converged).
     int run(const void *x0, bool use_mixed, double stop_tol, int64_t max_mv, double &theta, double &rnorm, bool &conv) {
-        int k = 0;
-        if(x0)
-            HEFF_CUDA(cudaMemcpyAsync(t, x0, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-        else
-            HEFF_TRY(random_vector(t, 0x5eedULL + (uint64_t)cfg.seed));
         conv  = false;
         theta = 0;
         rnorm = INFINITY;
+        if(x0)
+            HEFF_CUDA(cudaMemcpyAsync(V, x0, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+        else
+            HEFF_TRY(random_vector(V, 0x5eedULL + (uint64_t)cfg.seed));
+        {
+            double n2 = 0;
+            HEFF_TRY(norm2(V, n2));
+            if(!std::isfinite(n2)) {
+                set_last_error_msg("eigensolver: non-finite start vector");
+                return HEFF_NAN_INPUT;
+            }
+            if(!(n2 > 0)) {
+                HEFF_TRY(random_vector(V, 0x5eedULL + (uint64_t)cfg.seed));
+                HEFF_TRY(norm2(V, n2));
+            }
+            HEFF_TRY(scale(V, 1.0 / std::sqrt(n2)));
+        }
+        std::fill(Hk.begin(), Hk.end(), HT(0));
+        int                 k = 1;
         std::vector<double> w;
         std::vector<HT>     vecs;
+        std::vector<T>      hh(MD_MAXK + 1);
         int                 stagn = 0;
-        double              best  = INFINITY;
-        const bool          track = true;
-        std::vector<HT>     sbest;
+        double              best = INFINITY, verify = 1.0;
         while(true) {
-            double n0 = 0, nrm = 0;
-            HEFF_TRY(orthonormalize(V, k, n0, nrm));
-            if(!(nrm > 1e-10 * n0) || !(nrm > 0)) {
-                // breakdown (invariant subspace): continue with a fresh random direction
-                HEFF_TRY(random_vector(t, 0xabcdefULL + (uint64_t)res.num_mv));
-                HEFF_TRY(orthonormalize(V, k, n0, nrm));
-                if(!(nrm > 1e-10 * n0)) break;
+            T *vk = V + (int64_t)k * n;  // slot of the next basis vector
+            HEFF_TRY(apply(V + (int64_t)(k - 1) * n, AV + (int64_t)(k - 1) * n, !use_mixed));
+            HEFF_CUDA(cudaMemcpyAsync(vk, AV + (int64_t)(k - 1) * n, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+            // pass 1 (+ DGKS pass 2): h = V_k^H w and ||w||^2 from one multi_dot over k+1 columns
+            std::vector<HT> h(k, HT(0));
+            double          beta2 = 0, w2 = 0;
+            for(int pass = 0; pass < 2; pass++) {
+                HEFF_TRY(multi_dot<CPLX>(V, n, n, k + 1, vk, dh, partials, s));
+                HEFF_TRY(multi_axpy<CPLX>(V, n, n, k, dh, -1.0, vk, s));
+                HEFF_CUDA(cudaMemcpyAsync(hh.data(), dh, sizeof(T) * (k + 1), cudaMemcpyDeviceToHost, s));
+                HEFF_TRY(sync());
+                double hn2 = 0;
+                for(int i = 0; i < k; i++) {
+                    HT v;
+                    std::memcpy((void *)&v, (void *)&hh[i], sizeof(T));
+                    h[i] += v;
+                    hn2 += std::norm(std::complex<double>(v));
+                }
+                HT last;
+                std::memcpy((void *)&last, (void *)&hh[k], sizeof(T));
+                w2    = HostScalar<CPLX>::re(last);
+                beta2 = w2 - hn2;
+                if(!std::isfinite(w2)) {
+                    set_last_error_msg("eigensolver: non-finite vector (NaN/Inf in the operator or start vector)");
+                    return HEFF_NAN_INPUT;
+                }
+                if(beta2 > 0.5 * w2) break;  // no severe cancellation: the Pythagoras norm is accurate
+                if(pass == 1) {
+                    double n2 = 0;
+                    HEFF_TRY(norm2(vk, n2));
+                    beta2 = n2;
+                }
             }
-            HEFF_TRY(append(k, !use_mixed, track));
-            k++;
+            for(int i = 0; i < k; i++) {
+                Hk[i + (size_t)maxb * (k - 1)] = h[i];
+                Hk[(k - 1) + (size_t)maxb * i] = HostScalar<CPLX>::conj(h[i]);
+            }
+            const double beta = std::sqrt(std::max(0.0, beta2));
             HEFF_TRY(ritz<CPLX>(k, Hk, maxb, w, vecs));
             for(double wi : w) anorm = std::max(anorm, std::fabs(wi));
             const std::vector<int> ord = ritz_order(w, cfg.ritz, cfg.target);
-            const int              j0  = ord[0];
-            theta                      = w[j0];
-            const HT              *sv  = vecs.data() + (size_t)k * j0;
-            // residual estimate ||r||^2 = s^H G2 s - theta^2
-            double q = 0;
-            for(int jj = 0; jj < k; jj++)
-                for(int ii = 0; ii < k; ii++) q += HostScalar<CPLX>::re(HostScalar<CPLX>::conj(sv[ii]) * G2[ii + (size_t)maxb * jj] * sv[jj]);
-            double       rest   = std::sqrt(std::max(0.0, q - theta * theta));
-            const double floor_ = 3e-8 * std::max(anorm, std::fabs(theta));  // where the estimate loses accuracy
-            if(rest <= std::max(floor_, 4 * stop_tol * anorm) || res.num_mv >= max_mv) {
-                HEFF_TRY(explicit_residual(k, sv, theta, rest));
-            }
-            rnorm = rest;
+            theta                      = w[ord[0]];
+            const HT *sv               = vecs.data() + (size_t)k * ord[0];
+            const double est           = beta * std::abs(std::complex<double>(sv[k - 1]));
+            rnorm                      = est;
             res.iters++;
-            if(!std::isfinite(rnorm)) {
-                set_last_error_msg("eigensolver: non-finite residual");
-                return HEFF_NAN_INPUT;
-            }
-            if(rnorm <= stop_tol * std::max(anorm, 1e-300)) {
-                if(rnorm != rest) HEFF_TRY(explicit_residual(k, sv, theta, rnorm));
-                conv = true;
-                break;
+            if(est <= verify * stop_tol * std::max(anorm, 1e-300) || res.num_mv >= max_mv) {
+                HEFF_TRY(explicit_residual(k, sv, theta, rnorm));
+                if(!std::isfinite(rnorm)) {
+                    set_last_error_msg("eigensolver: non-finite residual");
+                    return HEFF_NAN_INPUT;
+                }
+                if(rnorm <= stop_tol * std::max(anorm, 1e-300)) {
+                    conv = true;
+                    break;
+                }
+                verify *= 0.1;  // the estimate was optimistic: ask it for more before the next check
+                if(res.num_mv >= max_mv) break;
             }
             if(use_mixed) {  // stop when the inexact operator floors the residual
-                if(rnorm < 0.5 * best) {
-                    best  = rnorm;
+                if(est < 0.5 * best) {
+                    best  = est;
                     stagn = 0;
                 } else if(++stagn >= 20) {
                     HEFF_TRY(explicit_residual(k, sv, theta, rnorm));
                     break;
                 }
             }
-            if(res.num_mv >= max_mv) break;
-            int kk = k;
-            if(k == maxb) {
-                HEFF_TRY(restart(k, minb, w, vecs, ord, track));
-                kk = minb;
+            if(!(beta > 1e-13 * std::sqrt(std::max(w2, 1e-300)))) {
+                // invariant subspace: the Ritz pair is exact for this operator
+                HEFF_TRY(explicit_residual(k, sv, theta, rnorm));
+                conv = rnorm <= stop_tol * std::max(anorm, 1e-300);
+                break;
             }
-            // expansion: A v_last (already computed)
-            HEFF_CUDA(cudaMemcpyAsync(t, AV + (int64_t)(kk - 1) * n, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-            k = kk;
+            inv_beta_ = 1.0 / beta;
+            HEFF_CUDA(cudaMemcpyAsync(dscal + 9, &inv_beta_, sizeof(double), cudaMemcpyHostToDevice, s));
+            HEFF_TRY(scale_dev<CPLX>(vk, n, dscal + 9, false, s));
+            if(k == maxb) {
+                // keep minb Ritz vectors, then append v_k
+                HEFF_TRY(restart(k, minb, w, vecs, ord, false));  // swaps V <-> V2: v_k is now V2[:, k]
+                HEFF_CUDA(cudaMemcpyAsync(V + (int64_t)minb * n, V2 + (int64_t)k * n, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+                k = minb + 1;
+            } else {
+                k++;
+            }
         }
         return HEFF_OK;
     }

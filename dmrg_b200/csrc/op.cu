@@ -190,6 +190,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->W) cudaFree(op->W);
     if(op->scratch) cudaFree(op->scratch);
     if(op->stage_x) cudaFree(op->stage_x);
+    if(op->eig_ws) cudaFree(op->eig_ws);
     delete op;
     return HEFF_OK;
 }

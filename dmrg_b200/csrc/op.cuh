@@ -15,6 +15,9 @@ struct heff_op {
     size_t             scratch_bytes = 0;
     void              *stage_x       = nullptr;  // device staging for MultAx with host buffers
     int64_t            num_mv        = 0;
+    // eigensolver workspace, kept across heff_eigs calls on this operator (grown on demand)
+    void              *eig_ws       = nullptr;
+    size_t             eig_ws_bytes = 0;
     // stage profiling (heff_op_set_profiling): ring of 5-event sets, summed on query
     bool               profiling     = false;
     std::vector<cudaEvent_t> prof_events;  // 5 * prof_cap
