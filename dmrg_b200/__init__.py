@@ -226,6 +226,100 @@ def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, preci
     return res.as_dict()
 
 
+def make_env(chi, D, cplx, seed, swap_base=0, stream=None):
+    """Seeded [chi, chi, D] environment on the device (heff_make_env): every slice Hermitian, or for
+    D = swap_base^2 the MPO-squared swap symmetry.  Returns a flat device tensor."""
+    torch = _torch()
+    out = torch.empty(chi * chi * D, dtype=torch.complex128 if cplx else torch.float64, device="cuda")
+    check(lib().heff_make_env(C128 if cplx else F64, chi, D, swap_base, seed & (2**64 - 1), ptr(out), _stream_handle(stream)), "heff_make_env")
+    return out
+
+
+def make_vector(n, cplx, seed, stream=None):
+    torch = _torch()
+    out = torch.empty(n, dtype=torch.complex128 if cplx else torch.float64, device="cuda")
+    check(lib().heff_make_vector(C128 if cplx else F64, n, seed & (2**64 - 1), ptr(out), _stream_handle(stream)), "heff_make_vector")
+    return out
+
+
+class EigServer:
+    """Continuous-batching eigensolve server (heff_server_*): submit requests, wait for answers, read stats."""
+
+    def __init__(self, hbm_budget_bytes=64 << 30, max_inflight=4, device=0, max_basis=24):
+        from ._sigs import ServerConfig
+
+        cfg = ServerConfig()
+        lib().heff_server_config_default(ctypes.byref(cfg))
+        cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+        cfg.max_inflight = int(max_inflight)
+        cfg.device = int(device)
+        cfg.max_basis = int(max_basis)
+        h = ctypes.c_void_p()
+        check(lib().heff_server_create(ctypes.byref(cfg), ctypes.byref(h)), "heff_server_create")
+        self.handle = h
+        self._keep = {}
+
+    @staticmethod
+    def request(mpo, envL, envR, spin, chiL, chiR, cplx, theta0=None, ritz="SA", target=0.0, tol=1e-10, precision=PREC_FP64, theta_out=None):
+        """Builds an heff_request; mpo: host numpy [mL,mR,spin,spin]; envs/theta0: device tensors; theta_out: host numpy or None."""
+        from ._sigs import Request
+
+        dt = np.complex128 if cplx else np.float64
+        W = np.asfortranarray(np.asarray(mpo, dtype=dt))
+        r = Request()
+        r.dtype = C128 if cplx else F64
+        r.spin, r.chiL, r.chiR, r.mpoL, r.mpoR = spin, chiL, chiR, W.shape[0], W.shape[1]
+        r.mpo = W.ctypes.data
+        r.envL = envL.data_ptr()
+        r.envR = envR.data_ptr()
+        r.env_where = MEM_DEVICE
+        r.theta0 = theta0.data_ptr() if theta0 is not None else None
+        r.ritz = {"SA": 0, "LA": 1, "TARGET": 2}[ritz]
+        r.target = float(target)
+        r.tol = float(tol)
+        r.precision = int(precision)
+        r.theta_out = theta_out.ctypes.data if theta_out is not None else None
+        return r, (W, envL, envR, theta0, theta_out)
+
+    @staticmethod
+    def request_bytes(req, max_basis=24):
+        """Admission estimate: device bytes the request holds while it runs."""
+        return int(lib().heff_request_bytes(ctypes.byref(req), max_basis))
+
+    def submit(self, req_and_keep):
+        req, keep = req_and_keep
+        rid = ctypes.c_int64(0)
+        check(lib().heff_server_submit(self.handle, ctypes.byref(req), ctypes.byref(rid)), "heff_server_submit")
+        self._keep[rid.value] = (req, keep)
+        return rid.value
+
+    def wait(self, rid, timeout=0.0):
+        from ._sigs import Response
+
+        resp = Response()
+        check(lib().heff_server_wait(self.handle, rid, float(timeout), ctypes.byref(resp)), "heff_server_wait")
+        self._keep.pop(rid, None)
+        return resp.as_dict()
+
+    def stats(self):
+        from ._sigs import ServerStats
+
+        st = ServerStats()
+        check(lib().heff_server_get_stats(self.handle, ctypes.byref(st)), "heff_server_get_stats")
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().heff_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class MatVecMPOS:
     """MatVecMPOS<T> (matvec_mpos.h:23-180): operator object handed to an eigensolver.
 

@@ -49,7 +49,44 @@ class DmrgResult(ctypes.Structure):
         return d
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_inflight", ctypes.c_int), ("device", ctypes.c_int), ("max_basis", ctypes.c_int)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int), ("spin", ctypes.c_int64), ("chiL", ctypes.c_int64), ("chiR", ctypes.c_int64), ("mpoL", ctypes.c_int64),
+                ("mpoR", ctypes.c_int64), ("mpo", _P), ("envL", _P), ("envR", _P), ("env_where", ctypes.c_int), ("theta0", _P),
+                ("ritz", ctypes.c_int), ("target", ctypes.c_double), ("tol", ctypes.c_double), ("precision", ctypes.c_int), ("theta_out", _P)]
+
+
+class Response(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int), ("converged", ctypes.c_int), ("eigval", ctypes.c_double),
+                ("resnorm", ctypes.c_double), ("num_mv", ctypes.c_int64), ("num_mv_mixed", ctypes.c_int64), ("t_submit", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("queued", ctypes.c_int64), ("inflight", ctypes.c_int),
+                ("peak_inflight", ctypes.c_int), ("peak_bytes", ctypes.c_size_t), ("p50_latency_s", ctypes.c_double),
+                ("p99_latency_s", ctypes.c_double), ("max_latency_s", ctypes.c_double), ("solves_per_s", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def declare(L, sig):
+    sig(L, "heff_server_config_default", None, [ctypes.POINTER(ServerConfig)])
+    sig(L, "heff_server_create", _I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)])
+    sig(L, "heff_request_bytes", ctypes.c_size_t, [ctypes.POINTER(Request), _I])
+    sig(L, "heff_server_submit", _I, [_P, ctypes.POINTER(Request), _I64P])
+    sig(L, "heff_server_wait", _I, [_P, _I64, ctypes.c_double, ctypes.POINTER(Response)])
+    sig(L, "heff_server_get_stats", _I, [_P, ctypes.POINTER(ServerStats)])
+    sig(L, "heff_server_destroy", _I, [_P])
+    sig(L, "heff_make_env", _I, [_I, _I64, _I64, _I64, ctypes.c_uint64, _P, _P])
+    sig(L, "heff_make_vector", _I, [_I, _I64, ctypes.c_uint64, _P, _P])
     sig(L, "heff_op_device_error", _I, [_P, ctypes.POINTER(ctypes.c_int)])
     sig(L, "heff_gemm_bf16_f32", _I, [_P, _P, _P, _I64, _I64, _I64, _P])
     sig(L, "heff_dmrg_config_default", None, [ctypes.POINTER(DmrgConfig)])

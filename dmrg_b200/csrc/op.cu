@@ -59,12 +59,9 @@ static int create_impl(heff_op **out, int nsites, const void *const *mpos, const
         if(di[0] <= 0 || di[1] <= 0 || di[2] <= 0 || di[3] <= 0 || di[2] != di[3]) return HEFF_BAD_SHAPE;
         size_t          n = (size_t)(di[0] * di[1] * di[2] * di[3]);
         std::vector<HT> Wi(n);
-        if(where == HEFF_MEM_HOST)
-            std::memcpy(Wi.data(), mpos[i], n * sizeof(HT));
-        else {
-            HEFF_CUDA(cudaMemcpyAsync(Wi.data(), mpos[i], n * sizeof(HT), cudaMemcpyDeviceToHost, stream));
-            HEFF_CUDA(cudaStreamSynchronize(stream));
-        }
+        // the MPO may live on the host even when the environments are on the device: let UVA decide
+        HEFF_CUDA(cudaMemcpyAsync(Wi.data(), mpos[i], n * sizeof(HT), cudaMemcpyDefault, stream));
+        HEFF_CUDA(cudaStreamSynchronize(stream));
         if(i == 0) {
             W = std::move(Wi);
             std::memcpy(wd, di, sizeof(wd));
@@ -103,7 +100,8 @@ static int create_impl(heff_op **out, int nsites, const void *const *mpos, const
     op->scratch_bytes = (size_t)nscr * es;
     void *Rtmp        = nullptr;
     if(cudaMalloc(&Rtmp, nR * es) != cudaSuccess) return fail(HEFF_OOM);
-    const cudaMemcpyKind kind = (where == HEFF_MEM_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    (void)where;  // source location of each buffer is inferred from its address (unified addressing)
+    const cudaMemcpyKind kind = cudaMemcpyDefault;
     cudaError_t          e    = cudaMemcpyAsync(op->L, envL, nL * es, kind, stream);
     if(e == cudaSuccess) e = cudaMemcpyAsync(Rtmp, envR, nR * es, kind, stream);
     if(e == cudaSuccess) e = cudaMemcpyAsync(op->W, W.data(), nW * es, cudaMemcpyHostToDevice, stream);

@@ -240,6 +240,76 @@ typedef struct {
 void heff_dmrg_config_default(heff_dmrg_config *cfg);
 int  heff_dmrg_run(const heff_dmrg_config *cfg, heff_dmrg_result *res, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Eigensolve server: continuous batching of site-optimisation eigensolves.
+ * No counterpart in the reference (it solves one site problem at a time on the
+ * calling thread, solver_primme.cpp:298-517).  max_inflight worker slots, each
+ * with its own stream, admit queued requests first-fit while the device memory
+ * the in-flight requests hold stays within hbm_budget_bytes; environments stay
+ * on the device for the whole solve; work of concurrent requests overlaps.
+ * Results do not depend on the mix (every reduction has a fixed order).
+ * ------------------------------------------------------------------------- */
+typedef struct heff_server heff_server;
+
+typedef struct {
+    size_t hbm_budget_bytes; /* admission limit on the device memory held by in-flight requests */
+    int    max_inflight;     /* concurrent slots */
+    int    device;           /* CUDA device of the worker threads */
+    int    max_basis;        /* eigensolver basis size per request, default 24 */
+} heff_server_config;
+
+typedef struct {
+    int           dtype;                       /* HEFF_F64 / HEFF_C128 */
+    int64_t       spin, chiL, chiR, mpoL, mpoR; /* mps [spin, chiL, chiR], mpo [mpoL, mpoR, spin, spin] */
+    const void   *mpo;                         /* HOST mpo (merged) */
+    const void   *envL, *envR;                 /* [chiL,chiL,mpoL], [chiR,chiR,mpoR] in env_where */
+    int           env_where;                   /* heff_mem */
+    const void   *theta0;                      /* start vector (host or device) or NULL */
+    int           ritz;                        /* heff_ritz */
+    double        target;                      /* for HEFF_RITZ_TARGET */
+    double        tol;                         /* eigensolver tolerance, default 1e-10 */
+    int           precision;                   /* heff_precision */
+    void         *theta_out;                   /* HOST output eigenvector (rows elements) or NULL */
+} heff_request; /* buffers must stay valid until the request is answered; device buffers must be
+                   complete (their producing work finished) when the request is submitted */
+
+typedef struct {
+    int64_t id;
+    int     status; /* HEFF_OK, HEFF_NOT_CONVERGED, HEFF_OOM (larger than the whole budget), ... */
+    int     converged;
+    double  eigval, resnorm;
+    int64_t num_mv, num_mv_mixed;
+    double  t_submit, t_start, t_done; /* seconds on the server clock */
+} heff_response;
+
+typedef struct {
+    int64_t completed, failed, queued;
+    int     inflight, peak_inflight;
+    size_t  peak_bytes;
+    double  p50_latency_s, p99_latency_s, max_latency_s, solves_per_s;
+} heff_server_stats;
+
+void   heff_server_config_default(heff_server_config *cfg);
+int    heff_server_create(const heff_server_config *cfg, heff_server **srv);
+/* Device bytes a request holds while it runs (the admission estimate). */
+size_t heff_request_bytes(const heff_request *req, int max_basis);
+int    heff_server_submit(heff_server *srv, const heff_request *req, int64_t *id);
+/* Blocks until request `id` is answered (or timeout_s passes: HEFF_TIMEOUT). */
+int    heff_server_wait(heff_server *srv, int64_t id, double timeout_s, heff_response *resp);
+int    heff_server_get_stats(heff_server *srv, heff_server_stats *stats);
+/* Finishes queued requests, joins the workers, frees the server. */
+int    heff_server_destroy(heff_server *srv);
+
+/* ---------------------------------------------------------------------------
+ * Seeded synthetic inputs on the device (workload generators, not on the hot path)
+ * ------------------------------------------------------------------------- */
+/* env[a,a',mu] = (g(a,a',mu) + conj(g(a',a,pair(mu))))/2, g counter-based Gaussian:
+ * pair = identity (swap_base <= 1: every slice Hermitian) or, for D = swap_base^2,
+ * the swap (m + b*m~) <-> (m~ + b*m) matching the uncompressed MPO squared. */
+int heff_make_env(int dtype, int64_t chi, int64_t D, int64_t swap_base, uint64_t seed, void *out, void *stream);
+/* n Gaussian entries (complex: N(0,1) + i N(0,1)). */
+int heff_make_vector(int dtype, int64_t n, uint64_t seed, void *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
