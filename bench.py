@@ -208,6 +208,70 @@ def measure_mixed_and_eigs(hb, torch, op64, mpos, L, R, x, y, flush, stream, F):
     }
 
 
+def two_site_mpo(D, cplx):
+    """Merged two-site Ising MPO (D=3) or merged uncompressed MPO squared (D=9), h = 0.8 / 1.2, J = 1."""
+    def site(h):
+        W = np.zeros((3, 3, 2, 2))
+        sx = np.array([[0.0, 1.0], [1.0, 0.0]])
+        sz = np.array([[1.0, 0.0], [0.0, -1.0]])
+        W[0, 0] = np.eye(2)
+        W[1, 0] = sz
+        W[2, 0] = -h * sx
+        W[2, 1] = -sz
+        W[2, 2] = np.eye(2)
+        return W
+
+    def square(W):
+        X = np.einsum("mnsp,MNpt->mMnNst", W, W)
+        return X.reshape(9, 9, 2, 2, order="F")
+
+    WA, WB = site(0.8), site(1.2)
+    if D == 9:
+        WA, WB = square(WA), square(WB)
+    X = np.einsum("mcst,cnuv->mnsutv", WA, WB)
+    W = X.reshape(WA.shape[0], WB.shape[1], 4, 4, order="F")
+    return np.asfortranarray(W.astype(np.complex128 if cplx else np.float64))
+
+
+def measure_serving(hb, torch, n_req, chi_lo, chi_hi, rate, precision, seed=2024):
+    """Bounded sample of the serving stream: Poisson arrivals at `rate`/s, chi log-uniform in [chi_lo, chi_hi],
+    70% float64 / 30% complex128, D=3 requests target the lowest eigenpair, D=9 requests (MPO squared) the
+    lowest eigenpair of the folded operator; envs Hermitian (seeded Gaussians, generated on the device),
+    resident on the device; tol 1e-10.  Returns p50/p99 latency, solves/s and the server's peak concurrency."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_req):
+        chi = int(round(np.exp(rng.uniform(np.log(chi_lo), np.log(chi_hi)))))
+        D = 3 if rng.uniform() < 0.5 else 9
+        cplx = rng.uniform() < 0.3
+        specs.append((chi, D, cplx))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    reqs = []
+    for i, (chi, D, cplx) in enumerate(specs):
+        envL = hb.make_env(chi, D, cplx, seed=seed * 1000 + 2 * i, swap_base=3 if D == 9 else 0)
+        envR = hb.make_env(chi, D, cplx, seed=seed * 1000 + 2 * i + 1, swap_base=3 if D == 9 else 0)
+        th0 = hb.make_vector(4 * chi * chi, cplx, seed=seed * 1000 + 7 * i)
+        reqs.append(hb.EigServer.request(two_site_mpo(D, cplx), envL, envR, 4, chi, chi, cplx, theta0=th0, tol=1e-10, precision=precision))
+    torch.cuda.synchronize()
+    free, total = torch.cuda.mem_get_info()
+    srv = hb.EigServer(hbm_budget_bytes=int(0.8 * free), max_inflight=8)
+    t0 = time.perf_counter()
+    ids = []
+    for a, r in zip(arrivals, reqs):
+        dt = a - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(srv.submit(r))
+    resp = [srv.wait(i, timeout=600) for i in ids]
+    st = srv.stats()
+    srv.close()
+    ok = sum(1 for r in resp if r["status"] == 0)
+    return {"requests": n_req, "answered_ok": ok, "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+            "max_latency_s": st["max_latency_s"], "solves_per_s": st["solves_per_s"], "peak_inflight": st["peak_inflight"],
+            "peak_device_bytes": st["peak_bytes"], "arrival_rate_per_s": rate, "chi_range": [chi_lo, chi_hi],
+            "eigvals_head": [r["eigval"] for r in resp[:4]]}
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -247,7 +311,11 @@ def main():
     ap.add_argument("--impl", default="heff_b200", choices=["heff_b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and eigensolve measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision, eigensolve and serving measurements")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--serving-requests", type=int, default=40)
+    ap.add_argument("--serving-chi-max", type=int, default=1024)
+    ap.add_argument("--serving-rate", type=float, default=6.0, help="Poisson arrival rate (requests/s)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -341,6 +409,18 @@ def main():
             t_e2e.append(time.perf_counter() - t0)
         clk = clocks.stop()
         extras = {} if args.no_extras else measure_mixed_and_eigs(hb, torch, op, mpos, L, R, x, y, flush, stream, F)
+    if not args.no_extras and not args.no_serving:
+        op.close()
+        del x, y, flush
+        torch.cuda.empty_cache()
+        sv = {}
+        for name, prec in (("mixed", hb.PREC_MIXED), ("fp64", hb.PREC_FP64)):
+            sv[name] = measure_serving(hb, torch, args.serving_requests, 64, args.serving_chi_max, args.serving_rate, prec)
+        sv["workload"] = ("bounded sample of the serving stream: Poisson arrivals, chi log-uniform, 70% f64 / 30% c128, D in {3, 9} "
+                          "(D=9: MPO squared, folded-spectrum target), Hermitian seeded envs resident on the device, tol 1e-10")
+        if sv["fp64"]["solves_per_s"] > 0:
+            sv["mixed_vs_fp64_solves_per_s"] = sv["mixed"]["solves_per_s"] / sv["fp64"]["solves_per_s"]
+        extras["serving"] = sv
 
     tot_ms = sum(step_ms)
     if dist:

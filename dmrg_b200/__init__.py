@@ -226,6 +226,35 @@ def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, preci
     return res.as_dict()
 
 
+def ensemble(realisations, nthreads=16, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, J=1.0, precision=PREC_FP64):
+    """Independent fDMRG realisations (heff_ensemble_run).  realisations: list of (h_fields, chi_max or None, seed).
+    Returns (list of result dicts, list of status codes, wall seconds)."""
+    from ._sigs import DmrgConfig, DmrgResult
+
+    n = len(realisations)
+    cfgs = (DmrgConfig * n)()
+    keep = []
+    for i, (h, chi, seed) in enumerate(realisations):
+        hs = np.ascontiguousarray(np.asarray(h, dtype=np.float64))
+        keep.append(hs)
+        c = cfgs[i]
+        lib().heff_dmrg_config_default(ctypes.byref(c))
+        c.L = len(hs)
+        c.J = J
+        c.h = hs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        c.chi_max = int(chi or chi_max)
+        c.sweeps = sweeps
+        c.trunc_lim = trunc_lim
+        c.eig_tol = eig_tol
+        c.precision = precision
+        c.seed = int(seed)
+    res = (DmrgResult * n)()
+    st = (ctypes.c_int * n)()
+    secs = ctypes.c_double(0)
+    check(lib().heff_ensemble_run(cfgs, n, int(nthreads), res, st, ctypes.byref(secs)), "heff_ensemble_run")
+    return [res[i].as_dict() for i in range(n)], list(st), float(secs.value)
+
+
 def make_env(chi, D, cplx, seed, swap_base=0, stream=None):
     """Seeded [chi, chi, D] environment on the device (heff_make_env): every slice Hermitian, or for
     D = swap_base^2 the MPO-squared swap symmetry.  Returns a flat device tensor."""

@@ -1,18 +1,24 @@
 // Minimal two-site finite-DMRG sweep driver over the device hot path, for the random-field Ising chain
-// H = -sum J sz_i sz_{i+1} - sum h_i sx_i (IsingRandomField, source/tensors/site/mpo/IsingRandomField.cpp:93-136).
+// H = -sum J sz_i sz_{i+1} - sum h_i sx_i (IsingRandomField, source/tensors/site/mpo/IsingRandomField.cpp:93-136),
+// and the ensemble runner that overlaps many independent realisations on one GPU.
 //
-// It exists to run whole ground-state (fDMRG, fdmrg.cpp:282-360) calculations on the hot path
+// The driver exists to run whole ground-state (fDMRG, fdmrg.cpp:282-360) calculations on the hot path
 // and compare energies / entropies with exact answers; it is not a port of the reference's algorithm
 // layer.  Per bond (i, i+1):
 //   theta = M_i M_{i+1}                                    (merge, one DMMA GEMM + layout kernels)
-//   (E, theta) = lowest eigenpair of H_eff                  (heff_op + device Davidson)
+//   (E, theta) = lowest eigenpair of H_eff                  (heff_op rebound to the bond + device Davidson)
 //   theta -> U S V with the svd.cpp:257-280 rank rule        (device Jacobi SVD, schmidt_multisite)
 //   right-moving: M_i = U, M_{i+1} = S V, L_{i+1} = build_block(L_i, M_i, W_i)
 //   left-moving:  M_{i+1} = V, M_i = U S, R_i = build_block(R_{i+1}, M_{i+1}, W_{i+1})
+// All device memory (MPS, environments, operator, eigensolver basis, SVD scratch) is allocated once per
+// workspace and reused for every bond and every realisation, so a sweep step never allocates or
+// synchronises the device -- realisations on different streams overlap.
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "dmrg.cuh"
@@ -30,7 +36,7 @@ static int env_update_d(int side, double *out, const double *E, const int64_t ed
     return env_update<false>(side, out, E, ed, M, md, W, wd, scratch, s);
 }
 
-// splitmix64 -> uniform [lo, hi): the generator shared with oracle/physics.py
+// splitmix64 -> uniform [0, 1): the generator shared with oracle/physics.py
 static uint64_t splitmix(uint64_t &st) {
     st += 0x9E3779B97F4A7C15ull;
     uint64_t z = st;
@@ -53,8 +59,8 @@ static void ising_site_mpo(std::vector<double> &W, int64_t wd[4], int i, int L, 
             at(2, 1, s, t) = -J * sz[s][t];
             at(2, 2, s, t) = id[s][t];
         }
-    const int m0 = (i == 0) ? 2 : 0, m1 = (i == 0) ? 3 : 3;  // left edge keeps row 2
-    const int n0 = 0, n1 = (i == L - 1) ? 1 : 3;             // right edge keeps column 0
+    const int m0 = (i == 0) ? 2 : 0, m1 = 3;       // left edge keeps row 2
+    const int n0 = 0, n1 = (i == L - 1) ? 1 : 3;   // right edge keeps column 0
     wd[0] = m1 - m0;
     wd[1] = n1 - n0;
     wd[2] = wd[3] = 2;
@@ -82,7 +88,7 @@ __global__ void perm_sc_kernel(const double *__restrict__ M, double *__restrict_
         P[e]            = M[s2 + d * (c + cc * b)];
     }
 }
-// X[s, a, k] *= S[k] (mid index) or X[s, k, b] *= S[k]
+// X[s, a, k] *= S[k] (which = 0) or X[s, k, b] *= S[k] (which = 1)
 __global__ void scale_bond_kernel(double *__restrict__ X, const double *__restrict__ S, int64_t d, int64_t n1, int64_t n2, int which) {
     const int64_t tot = d * n1 * n2;
     for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
@@ -96,9 +102,17 @@ static int g1(int64_t n) {
     return (int)(g < 1 ? 1 : (g < cap ? g : cap));
 }
 
-struct Dev {
-    std::vector<void *> ptrs;
-    ~Dev() {
+// Device memory of one DMRG run, sized for chains up to Lcap sites and bonds up to chicap.
+struct DmrgWorkspace {
+    std::vector<void *>   ptrs;
+    int                   Lcap   = 0;
+    int64_t               chicap = 0;
+    cudaStream_t          s      = nullptr;
+    std::vector<double *> M, Lenv, Renv, W;
+    double *theta = nullptr, *Cbuf = nullptr, *P2 = nullptr, *U = nullptr, *S = nullptr, *V = nullptr, *scr = nullptr;
+    heff_op *op = nullptr;
+    ~DmrgWorkspace() {
+        if(op) heff_op_destroy(op);
         for(void *p : ptrs) cudaFree(p);
     }
     int get(double **p, size_t n) {
@@ -110,66 +124,78 @@ struct Dev {
         ptrs.push_back(*p);
         return HEFF_OK;
     }
+    int init(int L, int64_t chi, heff_precision prec, cudaStream_t stream) {
+        const int64_t d = 2;
+        Lcap = L;
+        chicap = chi;
+        s = stream;
+        M.resize(L);
+        W.resize(L);
+        Lenv.resize(L + 1);
+        Renv.resize(L + 1);
+        const size_t msz = (size_t)(d * chi * chi), tsz = (size_t)(d * d * chi * chi);
+        for(int i = 0; i < L; i++) {
+            HEFF_TRY(get(&M[i], msz));
+            HEFF_TRY(get(&W[i], 36));
+        }
+        for(int i = 0; i <= L; i++) {
+            HEFF_TRY(get(&Lenv[i], (size_t)(chi * chi * 3)));
+            HEFF_TRY(get(&Renv[i], (size_t)(chi * chi * 3)));
+        }
+        HEFF_TRY(get(&theta, tsz));
+        HEFF_TRY(get(&Cbuf, tsz));
+        HEFF_TRY(get(&P2, msz));
+        HEFF_TRY(get(&U, tsz));
+        HEFF_TRY(get(&S, (size_t)(2 * chi + 64)));
+        HEFF_TRY(get(&V, tsz));
+        const int64_t md_max[3] = {d, chi, chi}, wd_max[4] = {3, 3, 2, 2};
+        const size_t  scr_elems = std::max<size_t>((size_t)env_scratch_elems(md_max, wd_max), (size_t)schmidt_scratch_bytes(d, d, chi, chi, chi) / 8 + 64);
+        HEFF_TRY(get(&scr, scr_elems));
+        HEFF_TRY(op_create_capacity(&op, false, d * d, chi, 3, prec, stream));
+        heff_eig_config ec;
+        heff_eig_config_default(&ec);
+        return eig_reserve(op, d * d * chi * chi, ec.max_basis, prec == HEFF_PREC_MIXED);
+    }
 };
 
-int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s) {
+static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgWorkspace &ws) {
     auto      t0 = std::chrono::steady_clock::now();
     const int L  = cfg.L;
-    if(L < 2 || L > 4096 || !cfg.h || cfg.chi_max < 1) return HEFF_BAD_ARG;
+    if(L < 2 || L > ws.Lcap || !cfg.h || cfg.chi_max < 1 || cfg.chi_max > ws.chicap) return HEFF_BAD_ARG;
     const int64_t d = 2, chi_max = cfg.chi_max;
+    cudaStream_t  s = ws.s;
     std::memset(&res, 0, sizeof(res));
-    // --- model
-    std::vector<std::vector<double>> Wh(L);
+    ws.op->precision = (heff_precision)cfg.precision;
+    // --- model (host copies stay alive until the stream has consumed them)
+    std::vector<std::vector<double>>    Wh(L);
     std::vector<std::array<int64_t, 4>> wd(L);
-    Dev                                 dev;
-    std::vector<double *>               W(L);
     for(int i = 0; i < L; i++) {
         int64_t dd[4];
         ising_site_mpo(Wh[i], dd, i, L, cfg.J, cfg.h[i], cfg.energy_shift_per_site);
         for(int k = 0; k < 4; k++) wd[i][k] = dd[k];
-        HEFF_TRY(dev.get(&W[i], Wh[i].size()));
-        HEFF_CUDA(cudaMemcpyAsync(W[i], Wh[i].data(), Wh[i].size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        HEFF_CUDA(cudaMemcpyAsync(ws.W[i], Wh[i].data(), Wh[i].size() * sizeof(double), cudaMemcpyHostToDevice, s));
     }
-    // --- bond dimensions and buffers (sized for chi_max)
     std::vector<int64_t> chi(L + 1, 1);
-    std::vector<double *> M(L), Lenv(L + 1), Renv(L + 1);
-    const size_t          msz = (size_t)(d * chi_max * chi_max);
-    for(int i = 0; i < L; i++) HEFF_TRY(dev.get(&M[i], msz));
-    for(int i = 0; i <= L; i++) {
-        HEFF_TRY(dev.get(&Lenv[i], (size_t)(chi_max * chi_max * 3)));
-        HEFF_TRY(dev.get(&Renv[i], (size_t)(chi_max * chi_max * 3)));
-    }
-    double *theta, *Cbuf, *P2, *U, *S, *V, *scr;
-    const size_t tsz = (size_t)(d * d * chi_max * chi_max);
-    HEFF_TRY(dev.get(&theta, tsz));
-    HEFF_TRY(dev.get(&Cbuf, tsz));
-    HEFF_TRY(dev.get(&P2, msz));
-    HEFF_TRY(dev.get(&U, tsz));
-    HEFF_TRY(dev.get(&S, (size_t)(2 * chi_max + 64)));
-    HEFF_TRY(dev.get(&V, tsz));
-    const int64_t md_max[3] = {d, chi_max, chi_max}, wd_max[4] = {3, 3, 2, 2};
-    const size_t  scr_elems = std::max<size_t>((size_t)env_scratch_elems(md_max, wd_max),
-                                               (size_t)schmidt_scratch_bytes(d, d, chi_max, chi_max, chi_max) / 8 + 64);
-    HEFF_TRY(dev.get(&scr, scr_elems));
     // --- random product state (real, normalised per site), seed via splitmix64
-    uint64_t st = (uint64_t)cfg.seed * 0x2545F4914F6CDD1Dull + 17;
+    std::vector<double> init(2 * L);
+    uint64_t            st = (uint64_t)cfg.seed * 0x2545F4914F6CDD1Dull + 17;
     for(int i = 0; i < L; i++) {
         double a = uniform01(st) - 0.5, b = uniform01(st) - 0.5, nn = std::sqrt(a * a + b * b);
-        double v[2] = {a / nn, b / nn};
-        HEFF_CUDA(cudaMemcpyAsync(M[i], v, sizeof(v), cudaMemcpyHostToDevice, s));
-        HEFF_CUDA(cudaStreamSynchronize(s));
+        init[2 * i]     = a / nn;
+        init[2 * i + 1] = b / nn;
+        HEFF_CUDA(cudaMemcpyAsync(ws.M[i], init.data() + 2 * i, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
     }
     const double one = 1.0;
-    HEFF_CUDA(cudaMemcpyAsync(Lenv[0], &one, sizeof(double), cudaMemcpyHostToDevice, s));
-    HEFF_CUDA(cudaMemcpyAsync(Renv[L - 1], &one, sizeof(double), cudaMemcpyHostToDevice, s));
+    HEFF_CUDA(cudaMemcpyAsync(ws.Lenv[0], &one, sizeof(double), cudaMemcpyHostToDevice, s));
+    HEFF_CUDA(cudaMemcpyAsync(ws.Renv[L - 1], &one, sizeof(double), cudaMemcpyHostToDevice, s));
     HEFF_CUDA(cudaStreamSynchronize(s));
-    auto t_env = 0.0, t_eig = 0.0, t_svd = 0.0;
-    auto now   = [] { return std::chrono::steady_clock::now(); };
-    auto secs  = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+    double t_env = 0.0, t_eig = 0.0, t_svd = 0.0;
+    auto   now  = [] { return std::chrono::steady_clock::now(); };
+    auto   secs = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
     // R environments: Renv[i] = env of sites > i, dims [chi_{i+1}, chi_{i+1}, wd[i][1]]
     for(int i = L - 2; i >= 0; i--) {
         const int64_t ed[3] = {chi[i + 2], chi[i + 2], wd[i + 1][1]}, mdd[3] = {d, chi[i + 1], chi[i + 2]};
-        HEFF_TRY(env_update_d(1, Renv[i], Renv[i + 1], ed, M[i + 1], mdd, W[i + 1], wd[i + 1].data(), scr, s));
+        HEFF_TRY(env_update_d(1, ws.Renv[i], ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), ws.scr, s));
     }
     heff_eig_config ecfg;
     heff_eig_config_default(&ecfg);
@@ -178,37 +204,34 @@ int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s)
     ecfg.target      = cfg.target;
     ecfg.mixed       = cfg.precision == HEFF_PREC_MIXED;
     ecfg.max_matvecs = 4000;
-    double energy = 0;
+    double energy    = 0;
     for(int sweep = 0; sweep < cfg.sweeps; sweep++) {
         for(int dir = 0; dir < 2; dir++) {
             for(int step = 0; step < L - 1; step++) {
                 const int     i  = dir == 0 ? step : (L - 2 - step);
                 const int64_t ca = chi[i], cc = chi[i + 1], cb = chi[i + 2];
                 // theta = M_i M_{i+1}
-                perm_sc_kernel<<<g1(d * cc * cb), 256, 0, s>>>(M[i + 1], P2, d, cc, cb);
+                perm_sc_kernel<<<g1(d * cc * cb), 256, 0, s>>>(ws.M[i + 1], ws.P2, d, cc, cb);
                 HEFF_LAUNCH_CHECK();
                 GemmArgs g{};
                 g.M = (int)(d * ca), g.N = (int)(d * cb), g.K = (int)cc, g.batch = 1;
-                g.A = M[i], g.lda = d * ca, g.B = P2, g.ldb = cc, g.C = Cbuf, g.ldc = d * ca;
+                g.A = ws.M[i], g.lda = d * ca, g.B = ws.P2, g.ldb = cc, g.C = ws.Cbuf, g.ldc = d * ca;
                 g.alpha = make_double2(1, 0), g.beta = make_double2(0, 0);
                 HEFF_TRY(gemm_f64<false>(false, false, false, g, s));
-                merge_layout_kernel<<<g1(d * d * ca * cb), 256, 0, s>>>(Cbuf, theta, d, ca, cb);
+                merge_layout_kernel<<<g1(d * d * ca * cb), 256, 0, s>>>(ws.Cbuf, ws.theta, d, ca, cb);
                 HEFF_LAUNCH_CHECK();
-                // eigensolve
-                auto           te0 = now();
-                heff_op       *op  = nullptr;
-                const void    *mp[2] = {W[i], W[i + 1]};
-                int64_t        mdims[8];
+                // eigensolve on the rebound operator
+                auto          te0   = now();
+                const void   *mp[2] = {Wh[i].data(), Wh[i + 1].data()};
+                int64_t       mdims[8];
                 for(int k = 0; k < 4; k++) {
                     mdims[k]     = wd[i][k];
                     mdims[4 + k] = wd[i + 1][k];
                 }
                 const int64_t ld[3] = {ca, ca, wd[i][0]}, rd[3] = {cb, cb, wd[i + 1][1]};
-                HEFF_TRY(heff_op_create(&op, HEFF_F64, 2, mp, mdims, Lenv[i], ld, Renv[i + 1], rd, HEFF_MEM_DEVICE,
-                                        (heff_precision)cfg.precision, s));
+                HEFF_TRY(op_rebind(ws.op, 2, mp, mdims, ws.Lenv[i], ld, ws.Renv[i + 1], rd));
                 heff_eig_result er;
-                int             rc = eigs(op, &ecfg, theta, theta, &er);
-                heff_op_destroy(op);
+                int             rc = eigs(ws.op, &ecfg, ws.theta, ws.theta, &er);
                 if(rc != HEFF_OK && rc != HEFF_NOT_CONVERGED) return rc;
                 res.num_mv += er.num_mv;
                 res.num_mv_mixed += er.num_mv_mixed;
@@ -219,11 +242,11 @@ int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s)
                 auto    ts0 = now();
                 int64_t k   = 0;
                 double  te  = 0;
-                HEFF_TRY(schmidt_split(theta, d, d, ca, cb, chi_max, cfg.trunc_lim, U, S, V, &k, &te, scr, s));
+                HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_max, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s));
                 res.trunc_err_max = std::max(res.trunc_err_max, te);
                 if(i + 1 == L / 2 && sweep == cfg.sweeps - 1) {
                     std::vector<double> hs(k);
-                    HEFF_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+                    HEFF_CUDA(cudaMemcpyAsync(hs.data(), ws.S, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
                     HEFF_CUDA(cudaStreamSynchronize(s));
                     double ent = 0;
                     for(double v : hs)
@@ -235,32 +258,82 @@ int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s)
                 chi[i + 1] = k;
                 auto tv0   = now();
                 if(dir == 0) {
-                    HEFF_CUDA(cudaMemcpyAsync(M[i], U, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
-                    scale_bond_kernel<<<g1(d * k * cb), 256, 0, s>>>(V, S, d, k, cb, 1);
+                    HEFF_CUDA(cudaMemcpyAsync(ws.M[i], ws.U, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
+                    scale_bond_kernel<<<g1(d * k * cb), 256, 0, s>>>(ws.V, ws.S, d, k, cb, 1);
                     HEFF_LAUNCH_CHECK();
-                    HEFF_CUDA(cudaMemcpyAsync(M[i + 1], V, sizeof(double) * d * k * cb, cudaMemcpyDeviceToDevice, s));
+                    HEFF_CUDA(cudaMemcpyAsync(ws.M[i + 1], ws.V, sizeof(double) * d * k * cb, cudaMemcpyDeviceToDevice, s));
                     const int64_t ed[3] = {ca, ca, wd[i][0]}, mdd[3] = {d, ca, k};
-                    HEFF_TRY(env_update_d(0, Lenv[i + 1], Lenv[i], ed, M[i], mdd, W[i], wd[i].data(), scr, s));
+                    HEFF_TRY(env_update_d(0, ws.Lenv[i + 1], ws.Lenv[i], ed, ws.M[i], mdd, ws.W[i], wd[i].data(), ws.scr, s));
                 } else {
-                    HEFF_CUDA(cudaMemcpyAsync(M[i + 1], V, sizeof(double) * d * k * cb, cudaMemcpyDeviceToDevice, s));
-                    scale_bond_kernel<<<g1(d * ca * k), 256, 0, s>>>(U, S, d, ca, k, 0);
+                    HEFF_CUDA(cudaMemcpyAsync(ws.M[i + 1], ws.V, sizeof(double) * d * k * cb, cudaMemcpyDeviceToDevice, s));
+                    scale_bond_kernel<<<g1(d * ca * k), 256, 0, s>>>(ws.U, ws.S, d, ca, k, 0);
                     HEFF_LAUNCH_CHECK();
-                    HEFF_CUDA(cudaMemcpyAsync(M[i], U, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
+                    HEFF_CUDA(cudaMemcpyAsync(ws.M[i], ws.U, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
                     const int64_t ed[3] = {cb, cb, wd[i + 1][1]}, mdd[3] = {d, k, cb};
-                    HEFF_TRY(env_update_d(1, Renv[i], Renv[i + 1], ed, M[i + 1], mdd, W[i + 1], wd[i + 1].data(), scr, s));
+                    HEFF_TRY(env_update_d(1, ws.Renv[i], ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), ws.scr, s));
                 }
-                HEFF_CUDA(cudaStreamSynchronize(s));
                 t_env += secs(tv0, now());
             }
         }
         if(sweep < 64) res.energy_per_sweep[sweep] = energy;
         res.sweeps_done = sweep + 1;
     }
-    res.energy   = energy;
-    res.t_eig    = t_eig;
-    res.t_svd    = t_svd;
-    res.t_env    = t_env;
-    res.seconds  = secs(t0, now());
+    HEFF_CUDA(cudaStreamSynchronize(s));
+    res.energy  = energy;
+    res.t_eig   = t_eig;
+    res.t_svd   = t_svd;
+    res.t_env   = t_env;
+    res.seconds = secs(t0, now());
+    return HEFF_OK;
+}
+
+int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s) {
+    if(cfg.L < 2 || cfg.L > 4096 || !cfg.h || cfg.chi_max < 1) return HEFF_BAD_ARG;
+    DmrgWorkspace ws;
+    HEFF_TRY(ws.init(cfg.L, cfg.chi_max, (heff_precision)cfg.precision, s));
+    return dmrg_run_ws(cfg, res, ws);
+}
+
+// Many independent realisations: nthreads workers, each with its own stream and workspace (sized for the
+// largest chain and bond dimension), take realisations from a shared counter.  Different streams overlap
+// on the device; nthreads = 1 runs them one at a time.
+int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_result *results, int *status, double *seconds) {
+    int     Lmax   = 2;
+    int64_t chimax = 1;
+    for(int i = 0; i < n; i++) {
+        Lmax   = std::max(Lmax, cfgs[i].L);
+        chimax = std::max(chimax, cfgs[i].chi_max);
+    }
+    int dev = 0;
+    HEFF_CUDA(cudaGetDevice(&dev));
+    std::atomic<int>         next{0};
+    std::vector<int>         rcs(nthreads, HEFF_OK);
+    std::vector<std::thread> pool;
+    HEFF_CUDA(cudaDeviceSynchronize());
+    // workspaces are built before the clock starts (one-time allocation)
+    std::vector<cudaStream_t>                   streams(nthreads);
+    std::vector<std::unique_ptr<DmrgWorkspace>> wss(nthreads);
+    for(int t = 0; t < nthreads; t++) {
+        HEFF_CUDA(cudaStreamCreateWithFlags(&streams[t], cudaStreamNonBlocking));
+        wss[t] = std::make_unique<DmrgWorkspace>();
+        int rc = wss[t]->init(Lmax, chimax, (heff_precision)cfgs[0].precision, streams[t]);
+        if(rc != HEFF_OK) return rc;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    for(int t = 0; t < nthreads; t++) {
+        pool.emplace_back([&, t] {
+            cudaSetDevice(dev);
+            while(true) {
+                const int i = next.fetch_add(1);
+                if(i >= n) break;
+                status[i] = dmrg_run_ws(cfgs[i], results[i], *wss[t]);
+            }
+        });
+    }
+    for(auto &th : pool) th.join();
+    if(seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    wss.clear();
+    for(auto st : streams) cudaStreamDestroy(st);
     return HEFF_OK;
 }
 
@@ -269,17 +342,22 @@ int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s)
 extern "C" void heff_dmrg_config_default(heff_dmrg_config *cfg) {
     if(!cfg) return;
     std::memset(cfg, 0, sizeof(*cfg));
-    cfg->L                     = 16;
-    cfg->J                     = 1.0;
-    cfg->chi_max               = 64;
-    cfg->sweeps                = 10;
-    cfg->trunc_lim             = 1e-12;
-    cfg->eig_tol               = 1e-12;
-    cfg->ritz                  = HEFF_RITZ_SA;
-    cfg->precision             = HEFF_PREC_FP64;
+    cfg->L         = 16;
+    cfg->J         = 1.0;
+    cfg->chi_max   = 64;
+    cfg->sweeps    = 10;
+    cfg->trunc_lim = 1e-12;
+    cfg->eig_tol   = 1e-12;
+    cfg->ritz      = HEFF_RITZ_SA;
+    cfg->precision = HEFF_PREC_FP64;
 }
 
 extern "C" int heff_dmrg_run(const heff_dmrg_config *cfg, heff_dmrg_result *res, void *stream) {
     if(!cfg || !res) return HEFF_BAD_ARG;
     return heff::dmrg_run(*cfg, *res, (cudaStream_t)stream);
+}
+
+extern "C" int heff_ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_result *results, int *status, double *seconds) {
+    if(!cfgs || n <= 0 || nthreads < 1 || nthreads > 64 || !results || !status) return HEFF_BAD_ARG;
+    return heff::ensemble_run(cfgs, n, nthreads, results, status, seconds);
 }

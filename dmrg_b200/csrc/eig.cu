@@ -123,11 +123,15 @@ struct Davidson {
         carve_left -= bytes;
         return HEFF_OK;
     }
-    int setup(bool mixed) {
+    static size_t workspace_bytes(int64_t n, int maxb, bool mixed) {
         const size_t es  = sizeof(T);
         const size_t vec = (es * n + 255) / 256 * 256;
-        const size_t need = vec * (2 * (maxb + 1) + 2 * maxb + 4 + (mixed ? 5 : 0)) + es * MD_MAXK * 3 + es * MD_MAXK * MD_MAXK +
-                            sizeof(double) * MD_BLOCKS * MD_MAXK * 4 + 16 * sizeof(double) + 16 * 256;
+        return vec * (2 * (maxb + 1) + 2 * maxb + 4 + (mixed ? 5 : 0)) + es * MD_MAXK * 3 + es * MD_MAXK * MD_MAXK +
+               sizeof(double) * MD_BLOCKS * MD_MAXK * 4 + 16 * sizeof(double) + 16 * 256;
+    }
+    int setup(bool mixed) {
+        const size_t es   = sizeof(T);
+        const size_t need = workspace_bytes(n, maxb, mixed);
         if(op->eig_ws_bytes < need) {
             if(op->eig_ws) {
                 HEFF_CUDA(cudaStreamSynchronize(s));
@@ -522,6 +526,28 @@ static int eigs_impl(heff_op *op, const heff_eig_config &cfg, const void *x0, vo
     res.converged = conv ? 1 : 0;
     res.seconds   = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return conv ? HEFF_OK : HEFF_NOT_CONVERGED;
+}
+
+// Pre-sizes the operator's eigensolver workspace for problems up to n_max elements (so that solves on a
+// rebound operator never allocate).
+int eig_reserve(heff_op *op, int64_t n_max, int max_basis, bool mixed) {
+    if(!op) return HEFF_BAD_ARG;
+    const int    maxb = std::max(4, std::min(max_basis > 0 ? max_basis : 32, (int)MD_MAXK - 1));
+    const size_t need = op->cplx ? Davidson<true>::workspace_bytes(n_max, maxb, mixed) : Davidson<false>::workspace_bytes(n_max, maxb, mixed);
+    if(op->eig_ws_bytes >= need) return HEFF_OK;
+    if(op->eig_ws) {
+        HEFF_CUDA(cudaStreamSynchronize(op->stream));
+        cudaFree(op->eig_ws);
+        op->eig_ws       = nullptr;
+        op->eig_ws_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&op->eig_ws, need);
+    if(e != cudaSuccess) {
+        set_last_cuda_error(e, "eigensolver workspace", __FILE__, __LINE__);
+        return HEFF_OOM;
+    }
+    op->eig_ws_bytes = need;
+    return HEFF_OK;
 }
 
 int eigs(heff_op *op, const heff_eig_config *cfg_in, const void *x0, void *x_out, heff_eig_result *res) {

@@ -122,6 +122,87 @@ static int create_impl(heff_op **out, int nsites, const void *const *mpos, const
     return HEFF_OK;
 }
 
+// Operator with fixed-capacity buffers (spin S, bond <= cmax, MPO bond <= Dmax) for a sweep: every bond is
+// bound with op_rebind, which reuses the buffers (no allocation, no device synchronisation per bond).
+int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_t Dmax, heff_precision prec, cudaStream_t stream) {
+    if(!out || S <= 0 || cmax <= 0 || Dmax <= 0) return HEFF_BAD_ARG;
+    heff_op *op     = new heff_op();
+    op->cplx        = cplx;
+    op->precision   = prec;
+    op->stream      = stream;
+    op->mixed_apply = mixed_apply;
+    const size_t es = cplx ? 16 : 8;
+    auto         fail = [&](int rc) {
+        heff_op_destroy(op);
+        return rc;
+    };
+    const MatvecDims dmax{S, cmax, cmax, Dmax, Dmax};
+    op->cap_env     = cmax * cmax * Dmax;
+    op->cap_W       = Dmax * Dmax * S * S;
+    op->cap_scratch = cplx ? MatvecScratch<true>::elems(dmax) : MatvecScratch<false>::elems(dmax);
+    if(cudaMalloc(&op->L, op->cap_env * es) != cudaSuccess) return fail(HEFF_OOM);
+    if(cudaMalloc(&op->Rp, op->cap_env * es) != cudaSuccess) return fail(HEFF_OOM);
+    if(cudaMalloc(&op->Rtmp, op->cap_env * es) != cudaSuccess) return fail(HEFF_OOM);
+    if(cudaMalloc(&op->W, op->cap_W * es) != cudaSuccess) return fail(HEFF_OOM);
+    if(cudaMalloc(&op->scratch, op->cap_scratch * es) != cudaSuccess) return fail(HEFF_OOM);
+    op->scratch_bytes = (size_t)op->cap_scratch * es;
+    *out              = op;
+    return HEFF_OK;
+}
+
+// Binds the operator to new site MPOs (host, merged like matvec_mpos.cpp:104-119) and environments
+// (device, stream-ordered before the next apply).  Requires the capacities of op_create_capacity.
+template<bool CPLX>
+static int rebind_impl(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3],
+                       const void *envR, const int64_t rd[3]) {
+    using T  = typename Scalar<CPLX>::T;
+    using HT = typename std::conditional<CPLX, HostC, double>::type;
+    if(op->mixed && op->destroy_hook) op->destroy_hook(op);  // split operands belong to the old environments
+    std::vector<HT> W;
+    int64_t         wd[4];
+    for(int i = 0; i < nsites; i++) {
+        const int64_t  *di = mdims + 4 * i;
+        const size_t    n  = (size_t)(di[0] * di[1] * di[2] * di[3]);
+        std::vector<HT> Wi(reinterpret_cast<const HT *>(mpos_host[i]), reinterpret_cast<const HT *>(mpos_host[i]) + n);
+        if(i == 0) {
+            W = std::move(Wi);
+            std::memcpy(wd, di, sizeof(wd));
+        } else {
+            if(wd[1] != di[0]) return HEFF_BAD_SHAPE;
+            std::vector<HT> M2;
+            int64_t         nd[4];
+            merge_two(M2, nd, W, wd, Wi, di);
+            W = std::move(M2);
+            std::memcpy(wd, nd, sizeof(wd));
+        }
+    }
+    const int64_t md[3] = {wd[2], ld[0], rd[0]};
+    MatvecDims    d;
+    HEFF_TRY(check_matvec_dims(md, wd, ld, rd, d));
+    const int64_t nL = d.cL * d.cL * d.DL, nR = d.size_Rp(), nW = wd[0] * wd[1] * wd[2] * wd[3];
+    if(nL > op->cap_env || nR > op->cap_env || nW > op->cap_W || MatvecScratch<CPLX>::elems(d) > op->cap_scratch) {
+        set_last_error_msg("operator rebind: dimensions exceed the operator's capacity");
+        return HEFF_BAD_SHAPE;
+    }
+    op->d = d;
+    std::memcpy(op->mpo_dims, wd, sizeof(wd));
+    op->w_host.resize(nW * sizeof(T));
+    std::memcpy(op->w_host.data(), W.data(), nW * sizeof(T));  // stays alive until the next rebind
+    const size_t es = sizeof(T);
+    HEFF_CUDA(cudaMemcpyAsync(op->W, op->w_host.data(), nW * es, cudaMemcpyHostToDevice, op->stream));
+    HEFF_CUDA(cudaMemcpyAsync(op->L, envL, nL * es, cudaMemcpyDefault, op->stream));
+    HEFF_CUDA(cudaMemcpyAsync(op->Rtmp, envR, nR * es, cudaMemcpyDefault, op->stream));
+    return permute_R<CPLX>(reinterpret_cast<const T *>(op->Rtmp), reinterpret_cast<T *>(op->Rp), d, op->stream);
+}
+
+int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3], const void *envR,
+              const int64_t rd[3]) {
+    if(!op || nsites < 1 || nsites > 5 || !mpos_host || !mdims || !envL || !envR) return HEFF_BAD_ARG;
+    if(op->cap_env == 0) return HEFF_BAD_ARG;
+    return op->cplx ? rebind_impl<true>(op, nsites, mpos_host, mdims, envL, ld, envR, rd)
+                    : rebind_impl<false>(op, nsites, mpos_host, mdims, envL, ld, envR, rd);
+}
+
 int op_prof_flush(heff_op *op) {
     if(op->prof_used == 0) return HEFF_OK;
     HEFF_CUDA(cudaStreamSynchronize(op->stream));
@@ -189,6 +270,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->scratch) cudaFree(op->scratch);
     if(op->stage_x) cudaFree(op->stage_x);
     if(op->eig_ws) cudaFree(op->eig_ws);
+    if(op->Rtmp) cudaFree(op->Rtmp);
     delete op;
     return HEFF_OK;
 }

@@ -15,6 +15,10 @@ struct heff_op {
     size_t             scratch_bytes = 0;
     void              *stage_x       = nullptr;  // device staging for MultAx with host buffers
     int64_t            num_mv        = 0;
+    // fixed-capacity operators (op_create_capacity / op_rebind): element capacities, R staging, host MPO copy
+    int64_t            cap_env = 0, cap_W = 0, cap_scratch = 0;
+    void              *Rtmp    = nullptr;
+    std::vector<unsigned char> w_host;
     // eigensolver workspace, kept across heff_eigs calls on this operator (grown on demand)
     void              *eig_ws       = nullptr;
     size_t             eig_ws_bytes = 0;
@@ -34,6 +38,9 @@ namespace heff {
 int op_apply(heff_op *op, const void *x, void *y);
 int mixed_apply(heff_op *op, const void *x, void *y);     // mixed.cu
 int mixed_error_flag(heff_op *op, int *flag);              // mixed.cu
+int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_t Dmax, heff_precision prec, cudaStream_t stream);
+int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3], const void *envR,
+              const int64_t rd[3]);
 int op_prof_flush(heff_op *op);  // synchronises the op's stream and folds recorded events into prof_ms
 cudaEvent_t *op_prof_slot(heff_op *op);  // next free 5-event set or nullptr (profiling off)
 }

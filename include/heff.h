@@ -239,6 +239,13 @@ typedef struct {
 
 void heff_dmrg_config_default(heff_dmrg_config *cfg);
 int  heff_dmrg_run(const heff_dmrg_config *cfg, heff_dmrg_result *res, void *stream);
+/* Ensemble of independent realisations (disorder average): n configurations run by nthreads
+ * workers, each with its own stream and a workspace allocated once for the largest chain and
+ * bond dimension, so sweeps never allocate and realisations overlap on the device; nthreads = 1
+ * runs them one at a time.  status[i] is realisation i's return code; *seconds the wall time of
+ * the runs (workspace set-up excluded).  The reference runs one realisation per OS process
+ * (slurm/submit_jobarray.py:49-95). */
+int  heff_ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_result *results, int *status, double *seconds);
 
 /* ---------------------------------------------------------------------------
  * Eigensolve server: continuous batching of site-optimisation eigensolves.
