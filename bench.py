@@ -272,6 +272,38 @@ def measure_serving(hb, torch, n_req, chi_lo, chi_hi, rate, precision, seed=2024
             "eigvals_head": [r["eigval"] for r in resp[:4]]}
 
 
+def splitmix_fields(seed, L, lo=0.5, hi=1.5):
+    """h_i ~ U[lo, hi) from splitmix64 (the generator the library's sweep driver and tests share)."""
+    m64 = (1 << 64) - 1
+    st, out = seed & m64, []
+    for _ in range(L):
+        st = (st + 0x9E3779B97F4A7C15) & m64
+        z = st
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m64
+        z ^= z >> 31
+        out.append(lo + (hi - lo) * ((z >> 11) * (1.0 / 9007199254740992.0)))
+    return out
+
+
+def measure_ensemble(hb, n, sweeps, nthreads, seed=77):
+    """Bounded sample of the disorder ensemble: L uniform in {12,16,20,24}, chi_max uniform in {32,64}, h_i ~ U[0.5,1.5]
+    per realisation seed, real FP64 two-site fDMRG; realisations/s one at a time vs overlapped workers, and the
+    largest energy difference between the two runs."""
+    rng = np.random.default_rng(seed)
+    reals = []
+    for i in range(n):
+        L = int(rng.choice([12, 16, 20, 24]))
+        chi = int(rng.choice([32, 64]))
+        reals.append((splitmix_fields(seed * 100003 + i, L), chi, i))
+    r1, s1, t1 = hb.ensemble(reals, nthreads=1, sweeps=sweeps)
+    rp, sp, tp = hb.ensemble(reals, nthreads=nthreads, sweeps=sweeps)
+    dE = max(abs(a["energy"] - b["energy"]) for a, b in zip(r1, rp))
+    return {"realisations": n, "sweeps": sweeps, "workers": nthreads, "one_at_a_time_per_s": n / t1, "overlapped_per_s": n / tp,
+            "speedup": t1 / tp, "max_abs_dE_between_runs": dE, "ok": int(all(s == 0 for s in s1 + sp)),
+            "workload": "L in {12,16,20,24}, chi_max in {32,64}, two-site fDMRG FP64, random-field Ising h~U[0.5,1.5]"}
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -316,6 +348,7 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=40)
     ap.add_argument("--serving-chi-max", type=int, default=1024)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--ensemble-n", type=int, default=16, help="realisations in the ensemble sample")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -421,6 +454,7 @@ def main():
         if sv["fp64"]["solves_per_s"] > 0:
             sv["mixed_vs_fp64_solves_per_s"] = sv["mixed"]["solves_per_s"] / sv["fp64"]["solves_per_s"]
         extras["serving"] = sv
+        extras["ensemble"] = measure_ensemble(hb, args.ensemble_n, 4, 16)
 
     tot_ms = sum(step_ms)
     if dist:

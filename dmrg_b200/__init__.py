@@ -201,8 +201,13 @@ def schmidt_multisite(theta, dL, dR, chiL, chiR, rank_max=0, trunc_lim=1e-12, st
     return U[: m * k], S[:k], V[: k * n], k, float(err.value)
 
 
+def xdmrg(h, energy_target, **kw):
+    """Excited-state DMRG (folded spectrum): the eigenstate closest to energy_target (heff_dmrg_run, algorithm 1)."""
+    return fdmrg(h, energy_shift_per_site=energy_target / len(h), algorithm=1, **kw)
+
+
 def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, precision=PREC_FP64, seed=0, ritz="SA", target=0.0,
-          energy_shift_per_site=0.0, stream=None):
+          energy_shift_per_site=0.0, algorithm=0, stream=None):
     """Two-site DMRG of the random-field Ising chain on the device (heff_dmrg_run); returns the result dict."""
     from ._sigs import DmrgConfig, DmrgResult
 
@@ -221,6 +226,7 @@ def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, preci
     cfg.ritz = {"SA": 0, "LA": 1, "TARGET": 2}[ritz]
     cfg.target = target
     cfg.energy_shift_per_site = energy_shift_per_site
+    cfg.algorithm = int(algorithm)
     res = DmrgResult()
     check(lib().heff_dmrg_run(ctypes.byref(cfg), ctypes.byref(res), _stream_handle(stream)), "heff_dmrg_run")
     return res.as_dict()

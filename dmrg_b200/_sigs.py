@@ -32,7 +32,7 @@ class DmrgConfig(ctypes.Structure):
 
     _fields_ = [("L", ctypes.c_int), ("J", ctypes.c_double), ("h", _DP), ("chi_max", ctypes.c_int64), ("sweeps", ctypes.c_int),
                 ("trunc_lim", ctypes.c_double), ("eig_tol", ctypes.c_double), ("ritz", ctypes.c_int), ("target", ctypes.c_double),
-                ("precision", ctypes.c_int), ("seed", ctypes.c_int64), ("energy_shift_per_site", ctypes.c_double)]
+                ("precision", ctypes.c_int), ("seed", ctypes.c_int64), ("energy_shift_per_site", ctypes.c_double), ("algorithm", ctypes.c_int)]
 
 
 class DmrgResult(ctypes.Structure):
@@ -41,7 +41,7 @@ class DmrgResult(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("entropy_mid", ctypes.c_double), ("trunc_err_max", ctypes.c_double), ("seconds", ctypes.c_double),
                 ("t_eig", ctypes.c_double), ("t_svd", ctypes.c_double), ("t_env", ctypes.c_double), ("chi_mid", ctypes.c_int64),
                 ("num_mv", ctypes.c_int64), ("num_mv_mixed", ctypes.c_int64), ("unconverged_solves", ctypes.c_int64), ("sweeps_done", ctypes.c_int),
-                ("energy_per_sweep", ctypes.c_double * 64)]
+                ("energy_per_sweep", ctypes.c_double * 64), ("variance", ctypes.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "energy_per_sweep"}

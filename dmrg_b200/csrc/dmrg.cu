@@ -71,6 +71,35 @@ static void ising_site_mpo(std::vector<double> &W, int64_t wd[4], int i, int L, 
                 for(int m = m0; m < m1; m++) W[(m - m0) + wd[0] * ((n - n0) + wd[1] * (s + 2 * t))] = at(m, n, s, t);
 }
 
+// Uncompressed square of the energy-shifted site MPO (MpoSite.cpp:57-70, real):
+//   W2[(m + 3 m~), (n + 3 n~), s, s''] = sum_s' W[m,n,s,s'] W[m~,n~,s',s'']
+// with the MPO^2 edges (MpoSite.cpp:609-640): the left edge keeps row 8 = (2, 2), the right edge column 0.
+static void ising_site_mpo2(std::vector<double> &W2, int64_t wd[4], int i, int L, double J, double h, double eshift) {
+    std::vector<double> W;
+    int64_t             w1[4];
+    ising_site_mpo(W, w1, 1, 3, J, h, eshift);  // bulk site: full 3x3
+    double full[81 * 4];
+    for(int t = 0; t < 2; t++)
+        for(int s = 0; s < 2; s++)
+            for(int nt = 0; nt < 3; nt++)
+                for(int n = 0; n < 3; n++)
+                    for(int mt = 0; mt < 3; mt++)
+                        for(int m = 0; m < 3; m++) {
+                            double acc = 0;
+                            for(int p = 0; p < 2; p++) acc += W[m + 3 * (n + 3 * (s + 2 * p))] * W[mt + 3 * (nt + 3 * (p + 2 * t))];
+                            full[(m + 3 * mt) + 9 * ((n + 3 * nt) + 9 * (s + 2 * t))] = acc;
+                        }
+    const int m0 = (i == 0) ? 8 : 0, m1 = 9, n0 = 0, n1 = (i == L - 1) ? 1 : 9;
+    wd[0] = m1 - m0;
+    wd[1] = n1 - n0;
+    wd[2] = wd[3] = 2;
+    W2.assign((size_t)(wd[0] * wd[1] * 4), 0.0);
+    for(int t = 0; t < 2; t++)
+        for(int s = 0; s < 2; s++)
+            for(int n = n0; n < n1; n++)
+                for(int m = m0; m < m1; m++) W2[(m - m0) + wd[0] * ((n - n0) + wd[1] * (s + 2 * t))] = full[m + 9 * (n + 9 * (s + 2 * t))];
+}
+
 // C[(s1 + d a) + d ca (s2 + d b)] -> theta[(s1 + d s2) + d^2 (a + ca b)]
 __global__ void merge_layout_kernel(const double *__restrict__ C, double *__restrict__ th, int64_t d, int64_t ca, int64_t cb) {
     const int64_t tot = d * d * ca * cb;
@@ -106,10 +135,10 @@ static int g1(int64_t n) {
 struct DmrgWorkspace {
     std::vector<void *>   ptrs;
     int                   Lcap   = 0;
-    int64_t               chicap = 0;
+    int64_t               chicap = 0, Dcap = 3;
     cudaStream_t          s      = nullptr;
     std::vector<double *> M, Lenv, Renv, W;
-    double *theta = nullptr, *Cbuf = nullptr, *P2 = nullptr, *U = nullptr, *S = nullptr, *V = nullptr, *scr = nullptr;
+    double *theta = nullptr, *Cbuf = nullptr, *P2 = nullptr, *U = nullptr, *S = nullptr, *V = nullptr, *scr = nullptr, *red = nullptr;
     heff_op *op = nullptr;
     ~DmrgWorkspace() {
         if(op) heff_op_destroy(op);
@@ -124,10 +153,11 @@ struct DmrgWorkspace {
         ptrs.push_back(*p);
         return HEFF_OK;
     }
-    int init(int L, int64_t chi, heff_precision prec, cudaStream_t stream) {
+    int init(int L, int64_t chi, heff_precision prec, cudaStream_t stream, int64_t Dmax = 3) {
         const int64_t d = 2;
         Lcap = L;
         chicap = chi;
+        Dcap   = Dmax;
         s = stream;
         M.resize(L);
         W.resize(L);
@@ -136,22 +166,23 @@ struct DmrgWorkspace {
         const size_t msz = (size_t)(d * chi * chi), tsz = (size_t)(d * d * chi * chi);
         for(int i = 0; i < L; i++) {
             HEFF_TRY(get(&M[i], msz));
-            HEFF_TRY(get(&W[i], 36));
+            HEFF_TRY(get(&W[i], 9 * 9 * 4));
         }
         for(int i = 0; i <= L; i++) {
-            HEFF_TRY(get(&Lenv[i], (size_t)(chi * chi * 3)));
-            HEFF_TRY(get(&Renv[i], (size_t)(chi * chi * 3)));
+            HEFF_TRY(get(&Lenv[i], (size_t)(chi * chi * Dmax)));
+            HEFF_TRY(get(&Renv[i], (size_t)(chi * chi * Dmax)));
         }
+        HEFF_TRY(get(&red, 4096));
         HEFF_TRY(get(&theta, tsz));
         HEFF_TRY(get(&Cbuf, tsz));
         HEFF_TRY(get(&P2, msz));
         HEFF_TRY(get(&U, tsz));
         HEFF_TRY(get(&S, (size_t)(2 * chi + 64)));
         HEFF_TRY(get(&V, tsz));
-        const int64_t md_max[3] = {d, chi, chi}, wd_max[4] = {3, 3, 2, 2};
+        const int64_t md_max[3] = {d, chi, chi}, wd_max[4] = {Dmax, Dmax, 2, 2};
         const size_t  scr_elems = std::max<size_t>((size_t)env_scratch_elems(md_max, wd_max), (size_t)schmidt_scratch_bytes(d, d, chi, chi, chi) / 8 + 64);
         HEFF_TRY(get(&scr, scr_elems));
-        HEFF_TRY(op_create_capacity(&op, false, d * d, chi, 3, prec, stream));
+        HEFF_TRY(op_create_capacity(&op, false, d * d, chi, Dmax, prec, stream));
         heff_eig_config ec;
         heff_eig_config_default(&ec);
         return eig_reserve(op, d * d * chi * chi, ec.max_basis, prec == HEFF_PREC_MIXED);
@@ -162,16 +193,21 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     auto      t0 = std::chrono::steady_clock::now();
     const int L  = cfg.L;
     if(L < 2 || L > ws.Lcap || !cfg.h || cfg.chi_max < 1 || cfg.chi_max > ws.chicap) return HEFF_BAD_ARG;
+    const bool folded = cfg.algorithm == 1;
+    if(folded && ws.Dcap < 9) return HEFF_BAD_ARG;
     const int64_t d = 2, chi_max = cfg.chi_max;
     cudaStream_t  s = ws.s;
     std::memset(&res, 0, sizeof(res));
     ws.op->precision = (heff_precision)cfg.precision;
-    // --- model (host copies stay alive until the stream has consumed them)
+    // --- model (host copies stay alive until the stream has consumed them): H, or (H - E_t)^2 for xDMRG
     std::vector<std::vector<double>>    Wh(L);
     std::vector<std::array<int64_t, 4>> wd(L);
     for(int i = 0; i < L; i++) {
         int64_t dd[4];
-        ising_site_mpo(Wh[i], dd, i, L, cfg.J, cfg.h[i], cfg.energy_shift_per_site);
+        if(folded)
+            ising_site_mpo2(Wh[i], dd, i, L, cfg.J, cfg.h[i], cfg.energy_shift_per_site);
+        else
+            ising_site_mpo(Wh[i], dd, i, L, cfg.J, cfg.h[i], cfg.energy_shift_per_site);
         for(int k = 0; k < 4; k++) wd[i][k] = dd[k];
         HEFF_CUDA(cudaMemcpyAsync(ws.W[i], Wh[i].data(), Wh[i].size() * sizeof(double), cudaMemcpyHostToDevice, s));
     }
@@ -278,6 +314,55 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
         if(sweep < 64) res.energy_per_sweep[sweep] = energy;
         res.sweeps_done = sweep + 1;
     }
+    if(folded) {
+        // <H> at the final centre, bond (0, 1): right environments of the unshifted H (D = 3) built from the
+        // converged MPS into the (now unused) left-environment storage, then one FP64 matvec and a dot.
+        const double E_t = cfg.energy_shift_per_site * L;
+        const double lam = energy;  // <(H - E_t)^2> of the last local eigensolve (normalised theta)
+        std::vector<std::vector<double>>    W3h(L);
+        std::vector<std::array<int64_t, 4>> w3(L);
+        for(int i = 0; i < L; i++) {
+            int64_t dd[4];
+            ising_site_mpo(W3h[i], dd, i, L, cfg.J, cfg.h[i], 0.0);
+            for(int k = 0; k < 4; k++) w3[i][k] = dd[k];
+            HEFF_CUDA(cudaMemcpyAsync(ws.W[i], W3h[i].data(), W3h[i].size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
+        HEFF_CUDA(cudaMemcpyAsync(ws.Lenv[L - 1], &one, sizeof(double), cudaMemcpyHostToDevice, s));
+        for(int i = L - 2; i >= 1; i--) {
+            const int64_t ed[3] = {chi[i + 2], chi[i + 2], w3[i + 1][1]}, mdd[3] = {d, chi[i + 1], chi[i + 2]};
+            HEFF_TRY(env_update_d(1, ws.Lenv[i], ws.Lenv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], w3[i + 1].data(), ws.scr, s));
+        }
+        const int64_t ca = chi[0], cc = chi[1], cb = chi[2];
+        perm_sc_kernel<<<g1(d * cc * cb), 256, 0, s>>>(ws.M[1], ws.P2, d, cc, cb);
+        HEFF_LAUNCH_CHECK();
+        GemmArgs g{};
+        g.M = (int)(d * ca), g.N = (int)(d * cb), g.K = (int)cc, g.batch = 1;
+        g.A = ws.M[0], g.lda = d * ca, g.B = ws.P2, g.ldb = cc, g.C = ws.Cbuf, g.ldc = d * ca;
+        g.alpha = make_double2(1, 0), g.beta = make_double2(0, 0);
+        HEFF_TRY(gemm_f64<false>(false, false, false, g, s));
+        merge_layout_kernel<<<g1(d * d * ca * cb), 256, 0, s>>>(ws.Cbuf, ws.theta, d, ca, cb);
+        HEFF_LAUNCH_CHECK();
+        // Lenv[0] still holds the trivial left edge (1)
+        const void   *mp[2] = {W3h[0].data(), W3h[1].data()};
+        int64_t       mdims[8];
+        for(int k = 0; k < 4; k++) {
+            mdims[k]     = w3[0][k];
+            mdims[4 + k] = w3[1][k];
+        }
+        const int64_t ld[3] = {ca, ca, w3[0][0]}, rd[3] = {cb, cb, w3[1][1]};
+        HEFF_TRY(op_rebind(ws.op, 2, mp, mdims, ws.Lenv[0], ld, ws.Lenv[1], rd));
+        ws.op->precision = HEFF_PREC_FP64;
+        HEFF_TRY(op_apply(ws.op, ws.theta, ws.Cbuf));
+        const int64_t n = d * d * ca * cb;
+        double        hv[2];
+        HEFF_TRY(dot_device<false>(ws.theta, ws.Cbuf, n, ws.red, ws.red + 8, s));
+        HEFF_TRY(dot_device<false>(ws.theta, ws.theta, n, ws.red + 1, ws.red + 8, s));
+        HEFF_CUDA(cudaMemcpyAsync(hv, ws.red, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        HEFF_CUDA(cudaStreamSynchronize(s));
+        const double Eh = hv[0] / hv[1];
+        res.variance    = lam - (Eh - E_t) * (Eh - E_t);
+        energy          = Eh;
+    }
     HEFF_CUDA(cudaStreamSynchronize(s));
     res.energy  = energy;
     res.t_eig   = t_eig;
@@ -290,7 +375,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
 int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s) {
     if(cfg.L < 2 || cfg.L > 4096 || !cfg.h || cfg.chi_max < 1) return HEFF_BAD_ARG;
     DmrgWorkspace ws;
-    HEFF_TRY(ws.init(cfg.L, cfg.chi_max, (heff_precision)cfg.precision, s));
+    HEFF_TRY(ws.init(cfg.L, cfg.chi_max, (heff_precision)cfg.precision, s, cfg.algorithm == 1 ? 9 : 3));
     return dmrg_run_ws(cfg, res, ws);
 }
 
@@ -316,7 +401,10 @@ int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_re
     for(int t = 0; t < nthreads; t++) {
         HEFF_CUDA(cudaStreamCreateWithFlags(&streams[t], cudaStreamNonBlocking));
         wss[t] = std::make_unique<DmrgWorkspace>();
-        int rc = wss[t]->init(Lmax, chimax, (heff_precision)cfgs[0].precision, streams[t]);
+        int64_t Dmax = 3;
+        for(int i = 0; i < n; i++)
+            if(cfgs[i].algorithm == 1) Dmax = 9;
+        int rc = wss[t]->init(Lmax, chimax, (heff_precision)cfgs[0].precision, streams[t], Dmax);
         if(rc != HEFF_OK) return rc;
     }
     auto t0 = std::chrono::steady_clock::now();

@@ -2,6 +2,7 @@
 // and the stateless C entry points heff_matvec_{d,z} / heff_expval_{d,z}.
 #include "matvec.cuh"
 #include "runtime.cuh"
+#include "wlist.cuh"
 
 namespace heff {
 
@@ -57,8 +58,8 @@ __device__ __forceinline__ void zero(double &v) { v = 0.0; }
 __device__ __forceinline__ void zero(double2 &v) { v = make_double2(0.0, 0.0); }
 
 // T2[(s' + S a') + S cL (b + cR n)] = sum_{m,s} W[m + DL(n + DR(s + S s'))] T1[(a' + cL m) + cL DL (s + S b)]
-// One CTA: 128 consecutive a' at one b.  W and the CTA's T1 column block are staged in shared memory;
-// zero MPO entries (most of them for Ising-type MPOs) are skipped with a warp-uniform branch.
+// One CTA: 128 consecutive a' at one b.  W, its nonzero list (wlist.cuh) and the CTA's T1 column block are
+// staged in shared memory; each output runs only over the nonzero MPO entries.
 constexpr int MIX_THREADS = 128;
 template<class T>
 __global__ void __launch_bounds__(MIX_THREADS) mix_kernel(const T *__restrict__ T1, T *__restrict__ T2, const T *__restrict__ W, int S, int cL,
@@ -67,6 +68,7 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_kernel(const T *__restrict__ 
     T        *sW  = reinterpret_cast<T *>(mix_smem);
     const int nW  = DL * DR * S * S;
     T        *sIn = sW + nW;
+    unsigned char *lmem = reinterpret_cast<unsigned char *>(sIn + (size_t)DL * S * MIX_THREADS);
     for(int i = threadIdx.x; i < nW; i += blockDim.x) sW[i] = W[i];
     const int     b   = blockIdx.y;
     const int     ap  = blockIdx.x * MIX_THREADS + threadIdx.x;
@@ -80,22 +82,19 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_kernel(const T *__restrict__ 
             sIn[(m * S + s) * MIX_THREADS + threadIdx.x] = v;
         }
     __syncthreads();
+    int   *off;
+    short *idx;
+    T     *wv;
+    build_wlist(sW, DL, DR, S, lmem, off, idx, wv);
     if(!act) return;
-    T acc[16];
     for(int n = 0; n < DR; n++) {
-        for(int sp0 = 0; sp0 < S; sp0 += 16) {
-            const int ns = min(16, S - sp0);
-            for(int q = 0; q < ns; q++) zero(acc[q]);
-            for(int q = 0; q < ns; q++) {
-                const int sp = sp0 + q;
-                for(int s = 0; s < S; s++)
-                    for(int m = 0; m < DL; m++) {
-                        const T w = sW[m + DL * (n + DR * (s + S * sp))];
-                        if(!is_zero(w)) acc[q] = fma_s(w, sIn[(m * S + s) * MIX_THREADS + threadIdx.x], acc[q]);
-                    }
-            }
-            T *out = T2 + (sp0 + (int64_t)S * ap) + (int64_t)S * cL * (b + (int64_t)cR * n);
-            for(int q = 0; q < ns; q++) out[q] = acc[q];
+        T *out = T2 + ((int64_t)S * ap) + (int64_t)S * cL * (b + (int64_t)cR * n);
+        for(int sp = 0; sp < S; sp++) {
+            const int o = n * S + sp;
+            T         acc;
+            zero(acc);
+            for(int e = off[o]; e < off[o + 1]; e++) acc = fma_s(wv[e], sIn[idx[e] * MIX_THREADS + threadIdx.x], acc);
+            out[sp] = acc;
         }
     }
 }
@@ -118,7 +117,8 @@ template<bool CPLX>
 static int launch_mix(const MatvecDims &d, const typename Scalar<CPLX>::T *T1, typename Scalar<CPLX>::T *T2, const typename Scalar<CPLX>::T *W,
                       cudaStream_t s) {
     using T           = typename Scalar<CPLX>::T;
-    const size_t smem = sizeof(T) * ((size_t)d.DL * d.DR * d.S * d.S + (size_t)d.DL * d.S * MIX_THREADS);
+    const size_t smem = sizeof(T) * ((size_t)d.DL * d.DR * d.S * d.S + (size_t)d.DL * d.S * MIX_THREADS) +
+                        wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
     if(smem > 200 * 1024) return HEFF_BAD_SHAPE;
     static int attr_done[64] = {0};
     int        dev           = 0;

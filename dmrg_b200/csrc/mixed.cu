@@ -19,6 +19,7 @@
 #include "matvec.cuh"
 #include "op.cuh"
 #include "runtime.cuh"
+#include "wlist.cuh"
 
 namespace heff {
 
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__re
     float *sRe = reinterpret_cast<float *>(sW + nW);
     const int NP = DL * S;
     float *sIm = sRe + NP * MX_THREADS;
+    unsigned char *lmem = reinterpret_cast<unsigned char *>(sIm + (CPLX ? NP * MX_THREADS : 0));
     for(int i = threadIdx.x; i < nW; i += blockDim.x) sW[i] = W[i];
     const int a0 = blockIdx.x * MX_TA, b0 = blockIdx.y * MX_TB;
     {
@@ -168,25 +170,30 @@ __global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__re
         }
     }
     __syncthreads();
+    int   *off;
+    short *idx;
+    T     *wv;
+    build_wlist(sW, DL, DR, S, lmem, off, idx, wv);
     const int bl = threadIdx.x % MX_TB, al = threadIdx.x / MX_TB;
     const int ap = a0 + al, b = b0 + bl;
     if(ap >= cL || b >= cR) return;
+    const int me = al * MX_TB + bl;
     for(int n = 0; n < DR; n++)
         for(int sp = 0; sp < S; sp++) {
-            double re = 0, im = 0;
-            for(int s = 0; s < S; s++)
-                for(int m = 0; m < DL; m++) {
-                    const T w = sW[m + DL * (n + DR * (s + S * sp))];
-                    const int   slot = (m * S + s) * MX_THREADS + al * MX_TB + bl;
-                    const double xr  = sRe[slot];
-                    if constexpr(CPLX) {
-                        const double xi = sIm[slot];
-                        re += w.x * xr - w.y * xi;
-                        im += w.x * xi + w.y * xr;
-                    } else {
-                        re += w * xr;
-                    }
+            const int o  = n * S + sp;
+            double    re = 0, im = 0;
+            for(int e = off[o]; e < off[o + 1]; e++) {
+                const T      w    = wv[e];
+                const int    slot = idx[e] * MX_THREADS + me;
+                const double xr   = sRe[slot];
+                if constexpr(CPLX) {
+                    const double xi = sIm[slot];
+                    re += w.x * xr - w.y * xi;
+                    im += w.x * xi + w.y * xr;
+                } else {
+                    re += w * xr;
                 }
+            }
             const int64_t row = sp + (int64_t)S * ap, k = b + (int64_t)cR * n;
             put_A<CPLX>(A2 + row * Kx2, Kp2, k, re, im);
         }
@@ -263,7 +270,8 @@ static int mixed_setup(heff_op *op) {
     HEFF_TRY(make_tmap_bf16(&m->tB1, m->B1, cf * m->N1, m->Kx1, m->Kx1, X_BN));
     HEFF_TRY(make_tmap_bf16(&m->tA2, m->A2, m->M2, m->Kx2, m->Kx2, X_BM));
     HEFF_TRY(make_tmap_bf16(&m->tB2, m->B2, cf * m->N2, m->Kx2, m->Kx2, X_BN));
-    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS;
+    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS +
+                            wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
     if(mix_smem > 200 * 1024) return HEFF_BAD_SHAPE;
     HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     HEFF_CUDA(cudaStreamSynchronize(s));
@@ -283,7 +291,8 @@ static int mixed_apply_impl(heff_op *op, const void *x, void *y) {
     XGemmArgs g1a{};
     g1a.M = (int)m->M1, g1a.N = (int)(cf * m->N1), g1a.K = (int)m->Kx1, g1a.C = m->T1, g1a.ldc = m->M1, g1a.mode = X_OUT_F32, g1a.err = m->err;
     HEFF_TRY(gemm_bf16x(m->tA1, m->tB1, g1a, s));
-    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS;
+    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS +
+                            wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
     if(d.cR / MX_TB + 1 > 65535) return HEFF_BAD_SHAPE;
     dim3 grid((unsigned)cdiv(d.cL, MX_TA), (unsigned)cdiv(d.cR, MX_TB));
     mix_mixed_kernel<CPLX><<<grid, MX_THREADS, mix_smem, s>>>(m->T1, reinterpret_cast<const T *>(op->W), m->A2, (int)d.S, (int)d.cL, (int)d.cR,

@@ -228,13 +228,18 @@ typedef struct {
     int           precision;             /* heff_precision of the matvecs */
     int64_t       seed;                  /* random product-state initialisation */
     double        energy_shift_per_site; /* MPO energy shift (IsingRandomField.cpp:127) */
+    int           algorithm;             /* 0: ground state (fDMRG, H);  1: excited state (xDMRG): lowest
+                                            eigenpair of (H - E_t)^2 with E_t = L * energy_shift_per_site,
+                                            MPO^2 uncompressed (MpoSite.cpp:57-70, D = 9), as in
+                                            optimize_folded_spectrum.cpp:236-370 */
 } heff_dmrg_config;
 
 typedef struct {
     double  energy, entropy_mid, trunc_err_max, seconds, t_eig, t_svd, t_env;
     int64_t chi_mid, num_mv, num_mv_mixed, unconverged_solves;
     int     sweeps_done;
-    double  energy_per_sweep[64];
+    double  energy_per_sweep[64]; /* last eigenvalue of each sweep (energy, or <(H-E_t)^2> for xDMRG) */
+    double  variance;             /* xDMRG: <(H-E_t)^2> - (<H> - E_t)^2 (measure.cpp:575-640); energy = <H> */
 } heff_dmrg_result;
 
 void heff_dmrg_config_default(heff_dmrg_config *cfg);
