@@ -16,6 +16,7 @@ two-site random-field Ising MPO (D=3); chi = 1024.  Synthetic, seeded inputs.
 
 Multi-GPU: a single eigensolve does not shard ("replicas only"): under torchrun
 every rank runs its own replica on its own GPU; value = total FLOPs / max time.
+The extras (mixed precision, eigensolves, serving, ensemble) run at N=1 only.
 """
 import argparse
 import json
@@ -132,7 +133,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_sample(chi, D, cplx, budget_s, seed=5):
+def cpu_reference_sample(chi, D, cplx, budget_s, seed=5, one_thread_s=0.0):
     """Time the reference's contraction sequence (BLAS restatement, oracle/ref_numpy.py) on the host."""
     from oracle import ref_numpy as rn
 
@@ -148,14 +149,26 @@ def cpu_reference_sample(chi, D, cplx, budget_s, seed=5):
         if el >= budget_s:
             break
     F = matvec_flops(SPIN, chi, chi, D, D, cplx)
+    one = None
     try:
-        from threadpoolctl import threadpool_info
+        from threadpoolctl import threadpool_info, threadpool_limits
 
         threads = max((p.get("num_threads", 1) for p in threadpool_info() if p.get("internal_api") in ("openblas", "mkl", "blis")), default=1)
-    except Exception:
+        if one_thread_s > 0:
+            with threadpool_limits(limits=1):
+                n1, t1 = 0, time.perf_counter()
+                while True:
+                    rn.matvec_blas(theta, W, L, R)
+                    n1 += 1
+                    e1 = time.perf_counter() - t1
+                    if e1 >= one_thread_s:
+                        break
+            one = {"value": F * n1 / e1 / 1e12, "cores": 1, "matvecs": n1, "seconds": e1}
+    except ImportError:
         threads = os.cpu_count()
     return {"value": F * n / el / 1e12, "unit": UNIT, "cores": int(threads), "kind": "port", "matvecs": n, "seconds": el,
-            "sample": f"{n} complex128 matvecs at chi={chi}, D={D} (full workload size), BLAS restatement of contraction_tblis.cpp:277-290"}
+            "sample": f"{n} complex128 matvecs at chi={chi}, D={D} (full workload size), BLAS restatement of contraction_tblis.cpp:277-290",
+            "one_thread": one}
 
 
 def measure_mixed_and_eigs(hb, torch, op64, mpos, L, R, x, y, flush, stream, F):
@@ -311,6 +324,23 @@ def dist_env():
     return ws, rank, local
 
 
+def reduce_max_over_ranks(values, dist=None):
+    """Element-wise max of a list of floats over all ranks (NCCL reduces device tensors, gloo host ones)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu().tolist()]
+
+
+def job_tflops(flops_per_step, steps_per_rank, world, max_ms):
+    """Whole-job throughput: the work of all ranks divided by the slowest rank's time."""
+    return world * flops_per_step * steps_per_rank / (max_ms / 1e3) / 1e12
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -359,6 +389,10 @@ def main():
     import dmrg_b200 as hb
 
     ws, rank, local = dist_env()
+    if ws > 1:
+        # the extras (mixed precision, eigensolves, serving, ensemble) are single-GPU measurements; replicas run
+        # only the headline matvec so every rank takes the same collective steps in the same order
+        args.no_extras = True
     torch.cuda.set_device(local)
     dist = None
     if ws > 1:
@@ -371,7 +405,7 @@ def main():
     # CPU baseline first (rank 0, N=1 only), before any GPU work is timed
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_reference_sample(CHI, D, True, args.cpu_budget)
+        cpu = cpu_reference_sample(CHI, D, True, args.cpu_budget, one_thread_s=5.0)
 
     # FP64 peak reference: cuBLAS ZGEMM measured live (MEASURED_PEAKS.json has no FP64 entry)
     def zgemm_peak():
@@ -456,18 +490,9 @@ def main():
         extras["serving"] = sv
         extras["ensemble"] = measure_ensemble(hb, args.ensemble_n, 4, 16)
 
-    tot_ms = sum(step_ms)
-    if dist:
-        tt = torch.tensor([tot_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot_ms = float(tt.item())
-        te = torch.tensor([statistics.median(t_e2e)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_t = float(te.item())
-    else:
-        e2e_t = statistics.median(t_e2e)
+    tot_ms, e2e_t = reduce_max_over_ranks([sum(step_ms), statistics.median(t_e2e)], dist)
     ms_per_step = tot_ms / args.steps
-    value = ws * F * args.steps / (tot_ms / 1e3) / 1e12
+    value = job_tflops(F, args.steps, ws, tot_ms)
     gemm_ms = (stage_ms[1] + stage_ms[3]) / max(cnt, 1)
     achieved = FG / (gemm_ms / 1e3) / 1e12
     traffic = None
