@@ -168,35 +168,41 @@ def env_update(side, out, env, env_dims, mps, mps_dims, mpo, mpo_dims, stream=No
 
 
 def svd(A, rows, cols, rank_max=0, trunc_lim=1e-12, stream=None):
-    """svd::solver::do_svd_ptr + truncation (svd.cpp:113-206, 257-280) on a device matrix.
+    """svd::solver::do_svd_ptr + truncation (svd.cpp:113-206, 257-280) on a device matrix (float64 or complex128).
 
-    Returns (U [rows x k], S [k], VT [k x cols]) as flat device tensors plus (k, truncation_error)."""
+    Returns (U [rows x k], S [k], VT [k x cols]) as flat device tensors plus (k, truncation_error); VT = V^H."""
     torch = _torch()
+    cplx = A.dtype == torch.complex128
+    dt = torch.complex128 if cplx else torch.float64
     kmax = min(rows, cols, rank_max if rank_max > 0 else rows * cols)
-    U = torch.empty(rows * kmax, dtype=torch.float64, device=A.device)
+    U = torch.empty(rows * kmax, dtype=dt, device=A.device)
     S = torch.empty(kmax, dtype=torch.float64, device=A.device)
-    VT = torch.empty(kmax * cols, dtype=torch.float64, device=A.device)
+    VT = torch.empty(kmax * cols, dtype=dt, device=A.device)
     k = ctypes.c_int64(0)
     err = ctypes.c_double(0)
-    check(lib().heff_svd_d(ptr(A), rows, cols, rank_max, trunc_lim, ptr(U), ptr(S), ptr(VT), ctypes.byref(k), ctypes.byref(err),
-                           _stream_handle(stream)), "heff_svd_d")
+    name = "heff_svd_z" if cplx else "heff_svd_d"
+    check(getattr(lib(), name)(ptr(A), rows, cols, rank_max, trunc_lim, ptr(U), ptr(S), ptr(VT), ctypes.byref(k), ctypes.byref(err),
+                               _stream_handle(stream)), name)
     k = int(k.value)
     return U[: rows * k], S[:k], VT[: k * cols], k, float(err.value)
 
 
 def schmidt_multisite(theta, dL, dR, chiL, chiR, rank_max=0, trunc_lim=1e-12, stream=None):
     """svd::solver::schmidt_multisite (svd.h:189-220): returns U [dL,chiL,k], S [k] (unit norm), V [dR,k,chiR]
-    as flat device tensors, and (k, truncation_error)."""
+    as flat device tensors, and (k, truncation_error).  theta float64 or complex128."""
     torch = _torch()
+    cplx = theta.dtype == torch.complex128
+    dt = torch.complex128 if cplx else torch.float64
     m, n = dL * chiL, dR * chiR
     kmax = min(m, n, rank_max if rank_max > 0 else m * n)
-    U = torch.empty(m * kmax, dtype=torch.float64, device=theta.device)
+    U = torch.empty(m * kmax, dtype=dt, device=theta.device)
     S = torch.empty(kmax, dtype=torch.float64, device=theta.device)
-    V = torch.empty(kmax * n, dtype=torch.float64, device=theta.device)
+    V = torch.empty(kmax * n, dtype=dt, device=theta.device)
     k = ctypes.c_int64(0)
     err = ctypes.c_double(0)
-    check(lib().heff_schmidt_d(ptr(theta), dL, dR, chiL, chiR, rank_max, trunc_lim, ptr(U), ptr(S), ptr(V), ctypes.byref(k), ctypes.byref(err),
-                               _stream_handle(stream)), "heff_schmidt_d")
+    name = "heff_schmidt_z" if cplx else "heff_schmidt_d"
+    check(getattr(lib(), name)(ptr(theta), dL, dR, chiL, chiR, rank_max, trunc_lim, ptr(U), ptr(S), ptr(V), ctypes.byref(k), ctypes.byref(err),
+                               _stream_handle(stream)), name)
     k = int(k.value)
     return U[: m * k], S[:k], V[: k * n], k, float(err.value)
 
@@ -207,7 +213,7 @@ def xdmrg(h, energy_target, **kw):
 
 
 def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, precision=PREC_FP64, seed=0, ritz="SA", target=0.0,
-          energy_shift_per_site=0.0, algorithm=0, stream=None):
+          energy_shift_per_site=0.0, algorithm=0, precond=-1, stream=None):
     """Two-site DMRG of the random-field Ising chain on the device (heff_dmrg_run); returns the result dict."""
     from ._sigs import DmrgConfig, DmrgResult
 
@@ -227,6 +233,7 @@ def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, preci
     cfg.target = target
     cfg.energy_shift_per_site = energy_shift_per_site
     cfg.algorithm = int(algorithm)
+    cfg.precond = int(precond)
     res = DmrgResult()
     check(lib().heff_dmrg_run(ctypes.byref(cfg), ctypes.byref(res), _stream_handle(stream)), "heff_dmrg_run")
     return res.as_dict()
@@ -434,6 +441,17 @@ class MatVecMPOS:
         if rc not in (HEFF_OK, 5):
             check(rc, "heff_eigs")
         return res.eigval, res.as_dict()
+
+    def diagonal(self):
+        """Diagonal of H_eff (get_diagonal_new, matvec_mpos.cpp:300-407) as a device tensor of rows() elements."""
+        torch = _torch()
+        out = torch.empty(self.rows(), dtype=torch.complex128 if self.cplx else torch.float64, device="cuda")
+        check(lib().heff_op_diagonal(self.handle, ptr(out)), "heff_op_diagonal")
+        return out
+
+    def MultPc(self, x, y, shift):
+        """Jacobi preconditioner y = x / (diag - shift) (MultPc, matvec_mpos.cpp:1349-1364); device tensors."""
+        check(lib().heff_op_multpc(self.handle, ptr(x), ptr(y), float(shift)), "heff_op_multpc")
 
     @property
     def num_mv(self):

@@ -13,7 +13,7 @@ class EigConfig(ctypes.Structure):
 
     _fields_ = [("ritz", ctypes.c_int), ("target", ctypes.c_double), ("tol", ctypes.c_double), ("max_basis", ctypes.c_int),
                 ("min_basis", ctypes.c_int), ("max_matvecs", ctypes.c_int64), ("mixed", ctypes.c_int), ("mixed_tol", ctypes.c_double),
-                ("inner_iters", ctypes.c_int), ("inner_tol", ctypes.c_double), ("seed", ctypes.c_int64)]
+                ("inner_iters", ctypes.c_int), ("inner_tol", ctypes.c_double), ("seed", ctypes.c_int64), ("precond", ctypes.c_int)]
 
 
 class EigResult(ctypes.Structure):
@@ -32,7 +32,8 @@ class DmrgConfig(ctypes.Structure):
 
     _fields_ = [("L", ctypes.c_int), ("J", ctypes.c_double), ("h", _DP), ("chi_max", ctypes.c_int64), ("sweeps", ctypes.c_int),
                 ("trunc_lim", ctypes.c_double), ("eig_tol", ctypes.c_double), ("ritz", ctypes.c_int), ("target", ctypes.c_double),
-                ("precision", ctypes.c_int), ("seed", ctypes.c_int64), ("energy_shift_per_site", ctypes.c_double), ("algorithm", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("seed", ctypes.c_int64), ("energy_shift_per_site", ctypes.c_double), ("algorithm", ctypes.c_int),
+                ("precond", ctypes.c_int)]
 
 
 class DmrgResult(ctypes.Structure):
@@ -88,6 +89,8 @@ def declare(L, sig):
     sig(L, "heff_make_env", _I, [_I, _I64, _I64, _I64, ctypes.c_uint64, _P, _P])
     sig(L, "heff_make_vector", _I, [_I, _I64, ctypes.c_uint64, _P, _P])
     sig(L, "heff_op_device_error", _I, [_P, ctypes.POINTER(ctypes.c_int)])
+    sig(L, "heff_op_diagonal", _I, [_P, _P])
+    sig(L, "heff_op_multpc", _I, [_P, _P, _P, ctypes.c_double])
     sig(L, "heff_gemm_bf16_f32", _I, [_P, _P, _P, _I64, _I64, _I64, _P])
     sig(L, "heff_ensemble_run", _I, [ctypes.POINTER(DmrgConfig), _I, _I, ctypes.POINTER(DmrgResult), ctypes.POINTER(ctypes.c_int), _DP])
     sig(L, "heff_dmrg_config_default", None, [ctypes.POINTER(DmrgConfig)])
@@ -96,5 +99,7 @@ def declare(L, sig):
     sig(L, "heff_eigs", _I, [_P, ctypes.POINTER(EigConfig), _P, _P, ctypes.POINTER(EigResult)])
     for n in ("heff_env_update_d", "heff_env_update_z"):
         sig(L, n, _I, [_I, _P, _P, _I64P, _P, _I64P, _P, _I64P, _P])
-    sig(L, "heff_svd_d", _I, [_P, _I64, _I64, _I64, ctypes.c_double, _P, _P, _P, _I64P, _DP, _P])
-    sig(L, "heff_schmidt_d", _I, [_P, _I64, _I64, _I64, _I64, _I64, ctypes.c_double, _P, _P, _P, _I64P, _DP, _P])
+    for n in ("heff_svd_d", "heff_svd_z"):
+        sig(L, n, _I, [_P, _I64, _I64, _I64, ctypes.c_double, _P, _P, _P, _I64P, _DP, _P])
+    for n in ("heff_schmidt_d", "heff_schmidt_z"):
+        sig(L, n, _I, [_P, _I64, _I64, _I64, _I64, _I64, ctypes.c_double, _P, _P, _P, _I64P, _DP, _P])

@@ -239,6 +239,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     ecfg.ritz        = cfg.ritz;
     ecfg.target      = cfg.target;
     ecfg.mixed       = cfg.precision == HEFF_PREC_MIXED;
+    ecfg.precond     = cfg.precond >= 0 ? cfg.precond : (cfg.algorithm == 1 ? 1 : 0);  // H^2: Jacobi (optimize_folded_spectrum.cpp:303-304)
     ecfg.max_matvecs = 4000;
     double energy    = 0;
     for(int sweep = 0; sweep < cfg.sweeps; sweep++) {
@@ -435,6 +436,7 @@ extern "C" void heff_dmrg_config_default(heff_dmrg_config *cfg) {
     cfg->chi_max   = 64;
     cfg->sweeps    = 10;
     cfg->trunc_lim = 1e-12;
+    cfg->precond   = -1;
     cfg->eig_tol   = 1e-12;
     cfg->ritz      = HEFF_RITZ_SA;
     cfg->precision = HEFF_PREC_FP64;

@@ -317,27 +317,30 @@ struct Davidson {
     // residual norm is |beta * s_{k-1}|: one pass over the basis per iteration (two when DGKS triggers).
     // A thick restart keeps Y = V_k S_m (all residuals along v_k) and appends v_k, preserving the relation.
     // Returns x = Ritz vector (normalised), theta, rnorm (explicit when converged).
-    int run(const void *x0, bool use_mixed, double stop_tol, int64_t max_mv, double &theta, double &rnorm, bool &conv) {
-        conv  = false;
-        theta = 0;
-        rnorm = INFINITY;
+    // V[:, 0] = x0 / ||x0|| (a seeded random vector when x0 is NULL or zero)
+    int init_start(const void *x0) {
         if(x0)
             HEFF_CUDA(cudaMemcpyAsync(V, x0, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
         else
             HEFF_TRY(random_vector(V, 0x5eedULL + (uint64_t)cfg.seed));
-        {
-            double n2 = 0;
-            HEFF_TRY(norm2(V, n2));
-            if(!std::isfinite(n2)) {
-                set_last_error_msg("eigensolver: non-finite start vector");
-                return HEFF_NAN_INPUT;
-            }
-            if(!(n2 > 0)) {
-                HEFF_TRY(random_vector(V, 0x5eedULL + (uint64_t)cfg.seed));
-                HEFF_TRY(norm2(V, n2));
-            }
-            HEFF_TRY(scale(V, 1.0 / std::sqrt(n2)));
+        double n2 = 0;
+        HEFF_TRY(norm2(V, n2));
+        if(!std::isfinite(n2)) {
+            set_last_error_msg("eigensolver: non-finite start vector");
+            return HEFF_NAN_INPUT;
         }
+        if(!(n2 > 0)) {
+            HEFF_TRY(random_vector(V, 0x5eedULL + (uint64_t)cfg.seed));
+            HEFF_TRY(norm2(V, n2));
+        }
+        return scale(V, 1.0 / std::sqrt(n2));
+    }
+
+    int run(const void *x0, bool use_mixed, double stop_tol, int64_t max_mv, double &theta, double &rnorm, bool &conv) {
+        conv  = false;
+        theta = 0;
+        rnorm = INFINITY;
+        HEFF_TRY(init_start(x0));
         std::fill(Hk.begin(), Hk.end(), HT(0));
         int                 k = 1;
         std::vector<double> w;
@@ -435,6 +438,56 @@ struct Davidson {
         return HEFF_OK;
     }
 
+    // Jacobi-preconditioned Davidson (FP64): the expansion vector is t = (diag - theta)^-1 r for the current
+    // Ritz pair (MultPc with the Ritz value as shift, matvec_mpos.cpp:1349-1364), orthonormalised against V
+    // (DGKS), with its Rayleigh-Ritz column from a pass over the basis; thick restart to min_basis vectors.
+    // Falls back to t = r when the preconditioned vector lies in the basis.
+    int run_pc(const void *x0, double stop_tol, int64_t max_mv, double &theta, double &rnorm, bool &conv) {
+        conv  = false;
+        theta = 0;
+        rnorm = INFINITY;
+        HEFF_TRY(init_start(x0));
+        HEFF_TRY(op_diagonal_ready(op));
+        std::fill(Hk.begin(), Hk.end(), HT(0));
+        HEFF_CUDA(cudaMemcpyAsync(t, V, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+        HEFF_TRY(append(0, true, false));
+        int                 k = 1;
+        std::vector<double> w;
+        std::vector<HT>     vecs;
+        while(true) {
+            HEFF_TRY(ritz<CPLX>(k, Hk, maxb, w, vecs));
+            for(double wi : w) anorm = std::max(anorm, std::fabs(wi));
+            const std::vector<int> ord = ritz_order(w, cfg.ritz, cfg.target);
+            theta                      = w[ord[0]];
+            HEFF_TRY(explicit_residual(k, vecs.data() + (size_t)k * ord[0], theta, rnorm));
+            res.iters++;
+            if(!std::isfinite(rnorm)) {
+                set_last_error_msg("eigensolver: non-finite residual");
+                return HEFF_NAN_INPUT;
+            }
+            if(rnorm <= stop_tol * std::max(anorm, 1e-300)) {
+                conv = true;
+                break;
+            }
+            if(res.num_mv >= max_mv) break;
+            HEFF_TRY(op_multpc(op, r, t, theta));
+            if(k == maxb) {
+                HEFF_TRY(restart(k, minb, w, vecs, ord, false));
+                k = minb;
+            }
+            double n0 = 0, nrm = 0;
+            HEFF_TRY(orthonormalize(V, k, n0, nrm));
+            if(!(nrm > 1e-10 * n0)) {  // the preconditioned direction is already in the basis: use the residual
+                HEFF_CUDA(cudaMemcpyAsync(t, r, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+                HEFF_TRY(orthonormalize(V, k, n0, nrm));
+                if(!(nrm > 1e-10 * n0)) break;  // invariant subspace
+            }
+            HEFF_TRY(append(k, true, false));
+            k++;
+        }
+        return HEFF_OK;
+    }
+
     // CG on (I - u u^H)(H_mixed - theta)(I - u u^H) d = -r0 restricted to u^perp; d -> cg_d
     int correction(const T *u, const T *r0, double theta, double r0n) {
         HEFF_CUDA(cudaMemsetAsync(cg_d, 0, sizeof(T) * n, s));
@@ -515,6 +568,8 @@ static int eigs_impl(heff_op *op, const heff_eig_config &cfg, const void *x0, vo
         HEFF_TRY(D.run(x0, true, cfg.mixed_tol > 0 ? cfg.mixed_tol : 1e-5, cfg.max_matvecs, theta, rnorm, conv));
         res.num_mv_phase1 = res.num_mv;
         HEFF_TRY(D.refine(theta, rnorm, conv));
+    } else if(cfg.precond == 1) {
+        HEFF_TRY(D.run_pc(x0, cfg.tol, cfg.max_matvecs, theta, rnorm, conv));
     } else {
         HEFF_TRY(D.run(x0, false, cfg.tol, cfg.max_matvecs, theta, rnorm, conv));
     }

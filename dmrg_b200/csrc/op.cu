@@ -146,6 +146,8 @@ int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_
     if(cudaMalloc(&op->W, op->cap_W * es) != cudaSuccess) return fail(HEFF_OOM);
     if(cudaMalloc(&op->scratch, op->cap_scratch * es) != cudaSuccess) return fail(HEFF_OOM);
     op->scratch_bytes = (size_t)op->cap_scratch * es;
+    op->diag_cap      = S * cmax * cmax;
+    if(cudaMalloc(&op->diag, op->diag_cap * es) != cudaSuccess) return fail(HEFF_OOM);
     *out              = op;
     return HEFF_OK;
 }
@@ -158,6 +160,7 @@ static int rebind_impl(heff_op *op, int nsites, const void *const *mpos_host, co
     using T  = typename Scalar<CPLX>::T;
     using HT = typename std::conditional<CPLX, HostC, double>::type;
     if(op->mixed && op->destroy_hook) op->destroy_hook(op);  // split operands belong to the old environments
+    op->diag_ready = false;
     std::vector<HT> W;
     int64_t         wd[4];
     for(int i = 0; i < nsites; i++) {
@@ -271,6 +274,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->stage_x) cudaFree(op->stage_x);
     if(op->eig_ws) cudaFree(op->eig_ws);
     if(op->Rtmp) cudaFree(op->Rtmp);
+    if(op->diag) cudaFree(op->diag);
     delete op;
     return HEFF_OK;
 }

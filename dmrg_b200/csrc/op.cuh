@@ -22,6 +22,10 @@ struct heff_op {
     // eigensolver workspace, kept across heff_eigs calls on this operator (grown on demand)
     void              *eig_ws       = nullptr;
     size_t             eig_ws_bytes = 0;
+    // diagonal of H_eff for the Jacobi preconditioner (computed on first use after create / rebind)
+    void              *diag         = nullptr;
+    int64_t            diag_cap     = 0;
+    bool               diag_ready   = false;
     // stage profiling (heff_op_set_profiling): ring of 5-event sets, summed on query
     bool               profiling     = false;
     std::vector<cudaEvent_t> prof_events;  // 5 * prof_cap
@@ -41,6 +45,8 @@ int mixed_error_flag(heff_op *op, int *flag);              // mixed.cu
 int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_t Dmax, heff_precision prec, cudaStream_t stream);
 int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3], const void *envR,
               const int64_t rd[3]);
+int op_diagonal_ready(heff_op *op);  // precond.cu: op->diag holds the diagonal of H_eff (stream-ordered)
+int op_multpc(heff_op *op, const void *x, void *y, double shift);  // precond.cu: y = x / (diag - shift)
 int op_prof_flush(heff_op *op);  // synchronises the op's stream and folds recorded events into prof_ms
 cudaEvent_t *op_prof_slot(heff_op *op);  // next free 5-event set or nullptr (profiling off)
 }

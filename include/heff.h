@@ -121,6 +121,13 @@ int heff_svd_d(const double *A, int64_t rows, int64_t cols, int64_t rank_max, do
  * (svd.h:172), V [dR, k, chiR] (svd.h:173).  Synchronises the stream. */
 int heff_schmidt_d(const double *theta, int64_t dL, int64_t dR, int64_t chiL, int64_t chiR, int64_t rank_max, double trunc_lim, double *U,
                    double *S, double *V, int64_t *rank, double *trunc_err, void *stream);
+/* Complex128 forms of the two above (the reference instantiates svd::solver for
+ * cx64 = std::complex<double>, svd.cpp:208-217): A = U S VT with VT = V^H, the
+ * LAPACK zgesdd convention; same rank rule, layouts and synchronisation. */
+int heff_svd_z(const heff_z *A, int64_t rows, int64_t cols, int64_t rank_max, double trunc_lim, heff_z *U, double *S, heff_z *VT, int64_t *rank,
+               double *trunc_err, void *stream);
+int heff_schmidt_z(const heff_z *theta, int64_t dL, int64_t dR, int64_t chiL, int64_t chiR, int64_t rank_max, double trunc_lim, heff_z *U,
+                   double *S, heff_z *V, int64_t *rank, double *trunc_err, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Operator object: MatVecMPOS<T> / MatVecMPO<T>
@@ -166,6 +173,17 @@ int heff_op_stage_times(heff_op *op, double ms[4], int64_t *count, int reset);
  * bounded wait in the mixed-precision kernels completed, nonzero when one timed out
  * (the kernel then skipped its work and returned).  Synchronises the stream. */
 int heff_op_device_error(heff_op *op, int *code);
+/* Diagonal of H_eff, replacing MatVecMPOS::get_diagonal_new(0, ...)
+ * (source/math/eig/matvec/matvec_mpos.cpp:300-407): diag[s + S(a + chiL b)] =
+ * sum_{m,n} envL[a,a,m] W[m,n,s,s] envR[b,b,n] into a device buffer of rows()
+ * elements of the operator's dtype (stream-ordered).  Computed once per operator
+ * (and per rebind) like CalcPc's readyCalcPc flag. */
+int heff_op_diagonal(heff_op *op, void *diag_out);
+/* Jacobi preconditioner, replacing MatVecMPOS::MultPc(T*, T*, T shift) with
+ * jcbMaxBlockSize == 1 (matvec_mpos.cpp:1349-1364): y = x / (diag - shift), the
+ * denominator kept >= 1e-10 max(|shift|, 1) in magnitude.  Device buffers,
+ * stream-ordered. */
+int heff_op_multpc(heff_op *op, const void *x, void *y, double shift);
 
 /* ---------------------------------------------------------------------------
  * BF16 tensor-core GEMM used by the mixed-precision path (tcgen05 + TMA)
@@ -186,14 +204,17 @@ typedef struct {
     int     ritz;        /* heff_ritz: smallest / largest algebraic, or closest to `target` */
     double  target;      /* target eigenvalue for HEFF_RITZ_TARGET */
     double  tol;         /* ||H x - theta x|| <= tol * ||H||_est (PRIMME eps, solver_primme.cpp:364); default 1e-12 */
-    int     max_basis;   /* Davidson basis size (<= 128), default 32 */
+    int     max_basis;   /* Davidson basis size (<= 128), default 24 */
     int     min_basis;   /* vectors kept at a thick restart, default 8 */
     int64_t max_matvecs; /* default 20000 */
     int     mixed;       /* 1: when the operator is HEFF_PREC_MIXED, split-BF16 phase then FP64 refinement */
-    double  mixed_tol;   /* relative residual at which the mixed phase hands over, default 1e-6 */
-    int     inner_iters; /* CG iterations of one refinement correction (mixed operator), default 40 */
-    double  inner_tol;   /* relative CG residual that ends a correction, default 1e-4 */
+    double  mixed_tol;   /* relative residual at which the mixed phase hands over, default 1e-5 */
+    int     inner_iters; /* CG iterations of one refinement correction (mixed operator), default 30 */
+    double  inner_tol;   /* relative CG residual that ends a correction, default 1e-3 */
     int64_t seed;        /* start vector seed when x0 is NULL */
+    int     precond;     /* 0 (default): Krylov expansion A v_last;  1: Jacobi-preconditioned
+                            Davidson, expansion (diag - theta)^-1 r (PRIMME with MultPc,
+                            optimize_folded_spectrum.cpp:303-304); FP64 operators */
 } heff_eig_config;
 
 typedef struct {
@@ -232,6 +253,9 @@ typedef struct {
                                             eigenpair of (H - E_t)^2 with E_t = L * energy_shift_per_site,
                                             MPO^2 uncompressed (MpoSite.cpp:57-70, D = 9), as in
                                             optimize_folded_spectrum.cpp:236-370 */
+    int           precond;               /* eigensolver expansion (heff_eig_config.precond); default -1:
+                                            Jacobi for xDMRG (as the reference's PRIMME set-up for H^2,
+                                            optimize_folded_spectrum.cpp:303-304), Krylov for fDMRG */
 } heff_dmrg_config;
 
 typedef struct {

@@ -16,6 +16,21 @@ def matvec_einsum(mps, mpo, envL, envR):
     return np.einsum("axm,sab,mnst,byn->txy", envL, mps, mpo, envR, optimize=True)
 
 
+def diagonal_einsum(mps_shape, mpo, envL, envR):
+    """MatVecMPOS::get_diagonal_new(0, ...) / get_matrix_element(I, I) (matvec_mpos.cpp:300-407):
+    diag[s,a,b] = sum_{m,n} envL[a,a,m] W[m,n,s,s] envR[b,b,n], flattened column-major like the mps."""
+    S, cL, cR = mps_shape
+    lD = np.einsum("aam->am", envL)
+    rD = np.einsum("bbn->bn", envR)
+    wD = np.einsum("mnss->mns", mpo)
+    return np.einsum("am,mns,bn->sab", lD, wD, rD).ravel(order="F")
+
+
+def multpc(x, diag, shift):
+    """MatVecMPOS::MultPc with jcbMaxBlockSize == 1 (matvec_mpos.cpp:1349-1364): x / (diag - shift)."""
+    return x / (np.real(diag) - shift)
+
+
 def expval_einsum(mps, mpo, envL, envR):
     y = matvec_einsum(mps, mpo, envL, envR)
     return np.vdot(mps.ravel(order="F"), y.ravel(order="F"))

@@ -122,3 +122,15 @@ def test_env_update_blas_baseline_golden(golden, i, side):
     g = lambda k: golden[f"env{i}_{k}"]
     env = g("L") if side == "L" else g("R")
     assert relerr(rn.env_update_blas(side, env, g("M"), g("W")), g("out" + side)) < 1e-13
+
+
+@pytest.mark.parametrize("c", [False, True])
+def test_diagonal_restatement_matches_dense_heff(c):
+    """The preconditioner diagonal (get_matrix_element at I == J) equals the diagonal of the dense H_eff."""
+    th, W, L, R = ph.heff_inputs(5, D=3, cplx=c, seed=31, chiR=4)
+    H = np.einsum("axm,mnst,byn->txysab", L, W, R).reshape(th.size, th.size, order="F")
+    d = rn.diagonal_einsum(th.shape, W, L, R)
+    assert np.linalg.norm(d - np.diag(H)) < 1e-13 * np.linalg.norm(d)
+    if not c:
+        Hc = oracle.dense_heff(th.shape, W, L, R)
+        assert np.linalg.norm(d - np.diag(Hc)) < 1e-13 * np.linalg.norm(d)

@@ -117,3 +117,106 @@ def test_svd_full_size_properties(cuda):
     assert np.max(np.abs(S - Sr[:1024])) < 1e-12 * Sr[0]
     assert np.linalg.norm(U.T @ U - np.eye(k)) < 1e-13 * n
     assert err == pytest.approx(np.linalg.norm(Sr[1024:]), rel=1e-10)
+
+
+# ---- complex128 (svd::solver instantiated for cx64, svd.cpp:208-217; zgesdd convention VT = V^H)
+
+def cgauss(rng, *shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def cgraded(m, n, sig, seed):
+    rng = np.random.default_rng(seed)
+    Q1, _ = np.linalg.qr(cgauss(rng, m, m))
+    Q2, _ = np.linalg.qr(cgauss(rng, n, n))
+    k = len(sig)
+    return (Q1[:, :k] * sig) @ Q2[:, :k].conj().T
+
+
+def run_svd_z(A, rank_max=0, lim=1e-12):
+    m, n = A.shape
+    U, S, VT, k, err = hb.svd(hb.to_device(np.asfortranarray(A.astype(np.complex128))), m, n, rank_max, lim)
+    torch.cuda.synchronize()
+    assert U.dtype == torch.complex128 and S.dtype == torch.float64
+    return hb.to_host(U, (m, k)), S.cpu().numpy(), hb.to_host(VT, (k, n)), k, err
+
+
+def check_z_against_gesdd(A, rank_max=0, lim=1e-12):
+    U, S, VT, k, err = run_svd_z(A, rank_max, lim)
+    Ur, Sr, VTr, kr, errr = rn.svd_truncated(A, rank_max, lim)
+    assert k == kr
+    smax = Sr[0]
+    assert np.max(np.abs(S - Sr)) <= 1e-13 * smax
+    assert abs(err - errr) <= 1e-13 * smax
+    m, n = A.shape
+    assert np.linalg.norm(U.conj().T @ U - np.eye(k)) < 1e-13 * max(m, n)
+    assert np.linalg.norm(VT @ VT.conj().T - np.eye(k)) < 1e-13 * max(m, n)
+    assert np.linalg.norm(U * S @ VT - (Ur * Sr) @ VTr) <= 1e-12 * np.linalg.norm(A)
+    return S, k
+
+
+@pytest.mark.parametrize("m,n", [(8, 8), (33, 47), (47, 33), (128, 128), (200, 64)])
+def test_svd_complex_random_vs_zgesdd(cuda, m, n):
+    A = cgauss(np.random.default_rng(7 * m + n), m, n)
+    check_z_against_gesdd(A)
+
+
+def test_svd_complex_real_input_matches_real_path(cuda):
+    """A real matrix given as complex128 has the real path's singular values."""
+    A = np.random.default_rng(21).standard_normal((96, 80))
+    Sz = run_svd_z(A.astype(np.complex128))[1]
+    Sd = run_svd(A)[1]
+    assert np.max(np.abs(Sz - Sd)) < 1e-13 * Sd[0]
+
+
+def test_svd_complex_rank_deficient_and_graded(cuda):
+    S, k = check_z_against_gesdd(cgraded(128, 128, np.array([0.9, 0.4, 0.2, 0.05]), 3) + 1e-17 * cgauss(np.random.default_rng(4), 128, 128))
+    assert k == 4
+    sig = np.logspace(0, -13, 40)
+    A = cgraded(96, 96, sig, 5)
+    U, S, VT, k, err = run_svd_z(A, 0, 1e-14)
+    Ur, Sr, VTr, kr, errr = rn.svd_truncated(A, 0, 1e-14)
+    assert k == kr
+    assert np.max(np.abs(S - Sr)) < 1e-14
+    # a complex rotation is ~4 real multiply-adds per entry update: a few ulps of sigma_max (real path: 1e-15)
+    assert np.max(np.abs(S[:30] - sig[:30])) < 2e-15
+
+
+def test_svd_complex_rank_max(cuda):
+    S, k = check_z_against_gesdd(cgauss(np.random.default_rng(6), 160, 160), rank_max=48)
+    assert k == 48
+
+
+@pytest.mark.parametrize("chiL,chiR,rank_max", [(16, 16, 0), (32, 24, 20), (100, 80, 64)])
+def test_schmidt_two_site_split_complex(cuda, chiL, chiR, rank_max):
+    rng = np.random.default_rng(3 * chiL + chiR)
+    theta = np.asfortranarray(cgauss(rng, 4, chiL, chiR))
+    theta /= np.linalg.norm(theta)
+    U, S, V, k, err = hb.schmidt_multisite(hb.to_device(theta), 2, 2, chiL, chiR, rank_max, 1e-12)
+    torch.cuda.synchronize()
+    Ur, Sr, Vr, kr, errr = rn.schmidt_multisite(theta, 2, 2, rank_max, 1e-12)
+    assert k == kr
+    Sg = S.cpu().numpy()
+    assert np.max(np.abs(Sg - Sr)) < 1e-13
+    assert abs(err - errr) < 1e-13
+    assert oracle.entropy(Sg) == pytest.approx(oracle.entropy(Sr), abs=1e-12)
+    Ug = hb.to_host(U, (2, chiL, k))
+    Vg = hb.to_host(V, (2, k, chiR))
+    th_g = np.einsum("sak,k,tkb->stab", Ug, Sg, Vg).reshape(4, chiL, chiR, order="F")
+    th_r = np.einsum("sak,k,tkb->stab", Ur, Sr, Vr).reshape(4, chiL, chiR, order="F")
+    assert np.linalg.norm(th_g - th_r) < 1e-12
+    # left-canonical U: sum_{s,a} conj(U[s,a,k]) U[s,a,l] = delta_kl
+    Um = Ug.reshape(2 * chiL, k, order="F")
+    assert np.linalg.norm(Um.conj().T @ Um - np.eye(k)) < 1e-13 * k
+
+
+def test_svd_complex_large_properties(cuda):
+    """1024 x 1024 complex (two-site split at chi=512): singular values, unitarity, tail norm."""
+    n = 1024
+    A = cgauss(np.random.default_rng(12), n, n) / np.sqrt(2 * n)
+    U, S, VT, k, err = run_svd_z(A, 512, 1e-12)
+    assert k == 512
+    Sr = np.linalg.svd(A, compute_uv=False)
+    assert np.max(np.abs(S - Sr[:512])) < 1e-12 * Sr[0]
+    assert np.linalg.norm(U.conj().T @ U - np.eye(k)) < 1e-13 * n
+    assert err == pytest.approx(np.linalg.norm(Sr[512:]), rel=1e-10)
