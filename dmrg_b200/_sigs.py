@@ -42,7 +42,7 @@ class DmrgResult(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("entropy_mid", ctypes.c_double), ("trunc_err_max", ctypes.c_double), ("seconds", ctypes.c_double),
                 ("t_eig", ctypes.c_double), ("t_svd", ctypes.c_double), ("t_env", ctypes.c_double), ("chi_mid", ctypes.c_int64),
                 ("num_mv", ctypes.c_int64), ("num_mv_mixed", ctypes.c_int64), ("unconverged_solves", ctypes.c_int64), ("sweeps_done", ctypes.c_int),
-                ("energy_per_sweep", ctypes.c_double * 64), ("variance", ctypes.c_double)]
+                ("energy_per_sweep", ctypes.c_double * 64), ("variance", ctypes.c_double), ("svd_sweeps_max", ctypes.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "energy_per_sweep"}

@@ -281,6 +281,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
                 double  te  = 0;
                 HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_max, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s));
                 res.trunc_err_max = std::max(res.trunc_err_max, te);
+                res.svd_sweeps_max = std::max(res.svd_sweeps_max, last_svd_sweeps());
                 if(i + 1 == L / 2 && sweep == cfg.sweeps - 1) {
                     std::vector<double> hs(k);
                     HEFF_CUDA(cudaMemcpyAsync(hs.data(), ws.S, sizeof(double) * k, cudaMemcpyDeviceToHost, s));

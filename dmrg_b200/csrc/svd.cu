@@ -10,11 +10,14 @@
 //   2. diagonalises it with a cyclic two-sided Jacobi eigensolver in shared memory (16 disjoint
 //      rotations per step), accumulating the unitary Q,
 //   3. applies P <- P Q and V[:, pair] <- V[:, pair] Q.
-// A pair whose Gram is already diagonal to |g_ij| <= tol*sqrt(g_ii g_jj) is skipped; the sweep loop
-// stops when every pair was skipped.  The relative criterion, evaluated on freshly computed Gram
-// entries, is what lets one-sided Jacobi resolve small singular values to high relative accuracy
-// (Demmel & Veselic 1992), which the truncation rule at 1e-12 needs.  Then sigma_j = ||G_j||,
-// U_j = G_j / sigma_j, sorted descending, VT = V^H.
+// A pair whose Gram is already diagonal to |g_ij| <= max(tol*sqrt(g_ii g_jj), floor) is skipped; the
+// sweep loop stops when every pair was skipped.  The relative criterion, evaluated on freshly computed
+// Gram entries, is what lets one-sided Jacobi resolve small singular values to high relative accuracy
+// (Demmel & Veselic 1992), which the truncation rule at 1e-12 needs.  The absolute floor
+// m eps^2 max_j ||G_j||^2 (from the previous sweep) stops the sweeps on columns that are rounding
+// noise (singular values below ~eps sigma_max, which no rotation can make relatively orthogonal); an
+// off-diagonal below it moves a singular value sigma by at most ~floor / sigma, the eps ||A|| level
+// of LAPACK's gesdd.  Then sigma_j = ||G_j||, U_j = G_j / sigma_j, sorted descending, VT = V^H.
 //
 // Complex rotation: for the Hermitian 2x2 block [[a, h], [conj(h), b]] with h = |h| e (|e| = 1) the
 // unitary J = diag(1, conj(e)) R diag(1, e), R the real Jacobi rotation of [[a, |h|], [|h|, b]], acts as
@@ -104,7 +107,8 @@ __device__ __forceinline__ T rot_lo(T x, T y, T e, double sn, double tau) {
 // One round of the block Jacobi sweep: blockIdx.x = pair index.
 template<class T>
 __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, int64_t ldg, int m, T *__restrict__ V, int64_t ldv, int nv, int B,
-                                                           int round, double tol, double *__restrict__ offmax, int *__restrict__ rotated) {
+                                                           int round, double tol, double floor_abs, double *__restrict__ offmax,
+                                                           int *__restrict__ rotated) {
     using S                = JS<T>;
     constexpr int JROWS    = S::ROWS;
     __shared__ T      sG[JP][JP + 1];
@@ -142,14 +146,17 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
     for(int u = 0; u < 4; u++) sG[gi][gj0 + u] = acc[u];
     __syncthreads();
 
-    // ---- off-diagonal measure of the fresh Gram (relative to the diagonal)
-    double mx = 0;
+    // ---- off-diagonal measure of the fresh Gram (relative to the diagonal; entries under the floor ignored)
+    //      and the largest squared column norm of the pair (offmax[1], the next sweep's floor)
+    double mx = 0, gmx = 0;
     for(int e = tid; e < JP * JP; e += JTHR) {
         const int i = e / JP, j = e % JP;
         if(i < j) {
             const double d = sqrt(fabs(S::re(sG[i][i])) * fabs(S::re(sG[j][j])));
             const double o = S::absv(sG[i][j]);
-            if(o > 0) mx = fmax(mx, d > 0 ? o / d : 1.0);
+            if(o > floor_abs) mx = fmax(mx, d > 0 ? o / d : 1.0);
+        } else if(i == j) {
+            gmx = fmax(gmx, fabs(S::re(sG[i][i])));
         }
     }
     s_red[tid] = mx;
@@ -159,7 +166,17 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
         __syncthreads();
     }
     const double off0 = s_red[0];
-    if(tid == 0) atomic_max_pos(offmax, off0);
+    __syncthreads();
+    s_red[tid] = gmx;
+    __syncthreads();
+    for(int w = JTHR / 2; w > 0; w >>= 1) {
+        if(tid < w) s_red[tid] = fmax(s_red[tid], s_red[tid + w]);
+        __syncthreads();
+    }
+    if(tid == 0) {
+        atomic_max_pos(offmax, off0);
+        atomic_max_pos(offmax + 1, s_red[0]);
+    }
     if(off0 <= tol) return;  // uniform across the CTA
     if(tid == 0) atomicAdd(rotated, 1);
 
@@ -181,7 +198,7 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
                 const T      apq = sG[a][b];
                 const double h   = S::absv(apq);
                 double       sn = 0.0, tau = 0.0;
-                if(h > 1e-300 && h > tol * sqrt(fabs(app) * fabs(aqq))) {
+                if(h > 1e-300 && h > floor_abs && h > tol * sqrt(fabs(app) * fabs(aqq))) {
                     const double th = (aqq - app) / (2.0 * h);
                     const double t  = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(1.0 + th * th));
                     const double c  = 1.0 / sqrt(1.0 + t * t);
@@ -302,6 +319,11 @@ __global__ void eye_kernel(T *__restrict__ V, int64_t ldv, int npad) {
         V[e] = (e % ldv == e / ldv) ? JS<T>::one() : JS<T>::zero();
 }
 
+int &last_svd_sweeps() {
+    static thread_local int n = 0;
+    return n;
+}
+
 static int g1(int64_t n) {
     int64_t g = (n + 255) / 256, cap = (int64_t)device_sm_count() * 8;
     return (int)(g < 1 ? 1 : (g < cap ? g : cap));
@@ -346,7 +368,7 @@ static int svd_truncated_t(const T *A, int64_t lda, int64_t m, int64_t n, int64_
     T            *G    = reinterpret_cast<T *>(scratch);
     T            *V    = G + ldg * npad;
     double       *sig  = reinterpret_cast<double *>(V + (int64_t)npad * npad);
-    double       *dmax = sig + npad;  // [0] offmax, [1..] spare
+    double       *dmax = sig + npad;  // [0] largest relative off-diagonal, [1] largest squared column norm
     int          *drot = reinterpret_cast<int *>(dmax + 8);
     int          *perm = reinterpret_cast<int *>(dmax + 64);
     copy_pad_kernel<T><<<g1(ldg * npad), 256, 0, s>>>(A, lda, (int)m, (int)n, G, ldg, npad);
@@ -356,18 +378,26 @@ static int svd_truncated_t(const T *A, int64_t lda, int64_t m, int64_t n, int64_
     const int B = npad / JB;  // even
     // off-diagonal tolerance just above the rounding noise of a length-m dot product
     const double tol   = std::max(1e-14, 8.0 * 2.2e-16 * std::sqrt((double)m));
-    int          sweep = 0;
+    const double eps   = 2.220446049250313e-16;
+    double       floor_abs = 0.0;  // first sweep: relative criterion only
+    int          sweep     = 0;
     for(; sweep < 40; sweep++) {
         HEFF_CUDA(cudaMemsetAsync(dmax, 0, 8 * 8 + sizeof(int), s));
         for(int r = 0; r < B - 1; r++) {
-            jacobi_round_kernel<T><<<B / 2, JTHR, 0, s>>>(G, ldg, (int)m, V, npad, npad, B, r, tol, dmax, drot);
+            jacobi_round_kernel<T><<<B / 2, JTHR, 0, s>>>(G, ldg, (int)m, V, npad, npad, B, r, tol, floor_abs, dmax, drot);
             HEFF_LAUNCH_CHECK();
         }
-        int rot = 0;
-        HEFF_CUDA(cudaMemcpyAsync(&rot, drot, sizeof(int), cudaMemcpyDeviceToHost, s));
+        struct {
+            double gmax;
+            int    rot;
+        } st{};
+        HEFF_CUDA(cudaMemcpyAsync(&st.rot, drot, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HEFF_CUDA(cudaMemcpyAsync(&st.gmax, dmax + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
         HEFF_CUDA(cudaStreamSynchronize(s));
-        if(rot == 0) break;
+        if(st.rot == 0) break;
+        floor_abs = (double)m * eps * eps * st.gmax;
     }
+    last_svd_sweeps() = sweep + 1;
     if(sweeps_out) *sweeps_out = sweep + 1;
     col_norms_kernel<T><<<(npad * 32 + 255) / 256, 256, 0, s>>>(G, ldg, (int)m, npad, sig);
     HEFF_LAUNCH_CHECK();

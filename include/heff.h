@@ -264,6 +264,7 @@ typedef struct {
     int     sweeps_done;
     double  energy_per_sweep[64]; /* last eigenvalue of each sweep (energy, or <(H-E_t)^2> for xDMRG) */
     double  variance;             /* xDMRG: <(H-E_t)^2> - (<H> - E_t)^2 (measure.cpp:575-640); energy = <H> */
+    int     svd_sweeps_max;       /* most Jacobi sweeps one two-site split needed */
 } heff_dmrg_result;
 
 void heff_dmrg_config_default(heff_dmrg_config *cfg);
