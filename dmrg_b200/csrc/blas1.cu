@@ -199,12 +199,173 @@ int residual(const typename Scalar<CPLX>::T *ax, const typename Scalar<CPLX>::T 
     return HEFF_OK;
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// Device-side classical Gram-Schmidt with a conditional second pass (DGKS) and normalisation, for the
+// Krylov expansion of the eigensolver: no host decision between the passes, so the next matvec can be
+// enqueued before the host reads the coefficients.
+//
+// State st[] (doubles): [0] ||w||^2, [1] second pass needed (0/1), [2] ||w'||^2 after pass 1, [3] beta^2,
+// h1 at st + ORTH_H1 (re, im pairs), h2 at st + ORTH_H2.  Host-visible result hres (T): hres[j] = h1 + h2
+// (j < k), hres[k] = beta, hres[k+1] = (||w||^2, second pass flag).
+constexpr int ORTH_H1 = 8;
+constexpr int ORTH_H2 = 8 + 2 * (MD_MAXK + 2);
+
+template<class T>
+__device__ __forceinline__ T orth_make(double re, double im) {
+    return VOps<T>::make(re, im);
+}
+
+// pass 0: h1[j] = <V_j, w>, ||w||^2;  pass 1 (only when st[1] != 0): h2[j] = <V_j, v>, ||v||^2.
+// Partial sums per block, then the last block to finish reduces them in block order (deterministic).
+template<class T>
+__global__ void __launch_bounds__(256) orth_dot_kernel(const T *__restrict__ V, int64_t ldv, int64_t n, int k, const T *__restrict__ t,
+                                                      double *__restrict__ partials, unsigned *__restrict__ counter, double *__restrict__ st,
+                                                      T *__restrict__ hres, int pass) {
+    constexpr bool CPLX = sizeof(T) == 16;
+    if(pass == 1 && st[1] == 0.0) return;  // uniform over the grid
+    __shared__ double sre[8][MD_G], sim[8][MD_G];
+    __shared__ bool   s_last;
+    const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int         nb = gridDim.x, kk = k + 1;  // column k is t itself
+    for(int j0 = 0; j0 < kk; j0 += MD_G) {
+        const int jn = min(MD_G, kk - j0);
+        double    re[MD_G], im[MD_G];
+#pragma unroll
+        for(int q = 0; q < MD_G; q++) re[q] = im[q] = 0.0;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            const T tv = t[i];
+#pragma unroll
+            for(int q = 0; q < MD_G; q++) {
+                const int j = j0 + q;
+                if(q < jn) VOps<T>::dot_acc(re[q], im[q], j < k ? V[i + ldv * j] : tv, tv);
+            }
+        }
+#pragma unroll
+        for(int q = 0; q < MD_G; q++) {
+            double a = re[q], b = im[q];
+            for(int o = 16; o > 0; o >>= 1) {
+                a += __shfl_xor_sync(0xffffffffu, a, o);
+                if(CPLX) b += __shfl_xor_sync(0xffffffffu, b, o);
+            }
+            if(lane == 0) {
+                sre[warp][q] = a;
+                sim[warp][q] = b;
+            }
+        }
+        __syncthreads();
+        if(threadIdx.x < jn) {
+            double a = 0, b = 0;
+            for(int w = 0; w < 8; w++) {
+                a += sre[w][threadIdx.x];
+                b += sim[w][threadIdx.x];
+            }
+            const int64_t j = j0 + threadIdx.x;
+            partials[(j * nb + blockIdx.x) * 2 + 0] = a;
+            partials[(j * nb + blockIdx.x) * 2 + 1] = b;
+        }
+        __syncthreads();
+    }
+    __threadfence();
+    if(threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == (unsigned)(nb - 1);
+    __syncthreads();
+    if(!s_last) return;
+    __threadfence();
+    double *h = st + (pass == 0 ? ORTH_H1 : ORTH_H2);
+    // one warp per column: lanes take blocks lane, lane+32, ... in order, then a fixed shuffle tree
+    for(int j = warp; j < kk; j += 8) {
+        double a = 0, b = 0;
+        for(int blk = lane; blk < nb; blk += 32) {
+            a += __ldcg(&partials[((int64_t)j * nb + blk) * 2 + 0]);
+            b += __ldcg(&partials[((int64_t)j * nb + blk) * 2 + 1]);
+        }
+        for(int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if(lane == 0) {
+            h[2 * j]     = a;
+            h[2 * j + 1] = CPLX ? b : 0.0;
+        }
+    }
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        double hn2 = 0;
+        for(int j = 0; j < k; j++) hn2 += h[2 * j] * h[2 * j] + h[2 * j + 1] * h[2 * j + 1];
+        const double nrm2 = h[2 * k];
+        if(pass == 0) {
+            st[0] = nrm2;
+            st[3] = nrm2 - hn2;
+            st[1] = (nrm2 - hn2 > 0.5 * nrm2) ? 0.0 : 1.0;  // severe cancellation: orthogonalise again
+        } else {
+            st[2] = nrm2;
+            st[3] = nrm2 - hn2;
+        }
+        *counter = 0u;  // ready for the next launch
+    }
+    __syncthreads();
+    // host-visible coefficients and beta (block 0 of the last pass that ran writes them)
+    const double beta2 = st[3];
+    for(int j = threadIdx.x; j < k; j += blockDim.x) {
+        double re = st[ORTH_H1 + 2 * j], im = st[ORTH_H1 + 2 * j + 1];
+        if(pass == 1) {
+            re += st[ORTH_H2 + 2 * j];
+            im += st[ORTH_H2 + 2 * j + 1];
+        }
+        hres[j] = orth_make<T>(re, im);
+    }
+    if(threadIdx.x == 0) {
+        hres[k]     = orth_make<T>(sqrt(fmax(beta2, 0.0)), 0.0);
+        hres[k + 1] = orth_make<T>(st[0], st[1]);
+    }
+}
+
+// out = (in - V h) * s, with h = h1 (pass 0) or h2 (pass 1, skipped unless st[1] != 0) and s = 1 / beta when
+// this is the last pass (no second pass needed, or pass 1), else 1.  A vanishing beta (invariant subspace)
+// writes zeros (the host stops before using the vector).
+template<class T>
+__global__ void orth_axpy_kernel(const T *__restrict__ V, int64_t ldv, int64_t n, int k, const T *in, T *out, const double *__restrict__ st,
+                                 int pass) {
+    if(pass == 1 && st[1] == 0.0) return;
+    extern __shared__ __align__(16) unsigned char osm[];
+    T            *sh   = reinterpret_cast<T *>(osm);
+    const double *h    = st + (pass == 0 ? ORTH_H1 : ORTH_H2);
+    for(int j = threadIdx.x; j < k; j += blockDim.x) sh[j] = orth_make<T>(h[2 * j], h[2 * j + 1]);
+    const bool   last  = pass == 1 || st[1] == 0.0;
+    const double beta2 = st[3];
+    const double s     = !last ? 1.0 : (beta2 > 1e-300 ? 1.0 / sqrt(beta2) : 0.0);
+    __syncthreads();
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T acc = VOps<T>::zero();
+        for(int j = 0; j < k; j++) acc = VOps<T>::axpy(acc, V[i + ldv * j], sh[j]);
+        out[i] = VOps<T>::scale(VOps<T>::addscaled(in[i], -1.0, acc), s);
+    }
+}
+
+template<bool CPLX>
+int orth_cgs2(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *w, typename Scalar<CPLX>::T *v,
+              double *partials, unsigned *counter, double *st, typename Scalar<CPLX>::T *hres, cudaStream_t s) {
+    using T = typename Scalar<CPLX>::T;
+    if(k <= 0 || k + 1 > 2 * MD_MAXK || k > MD_MAXK) return HEFF_BAD_ARG;
+    const int nb = (int)std::min<int64_t>(std::min<int64_t>(MD_BLOCKS, 4 * (int64_t)device_sm_count()), std::max<int64_t>(1, (n + 255) / 256));
+    orth_dot_kernel<T><<<nb, 256, 0, s>>>(V, ldv, n, k, w, partials, counter, st, hres, 0);
+    HEFF_LAUNCH_CHECK();
+    orth_axpy_kernel<T><<<grid_for(n), 256, sizeof(T) * k, s>>>(V, ldv, n, k, w, v, st, 0);
+    HEFF_LAUNCH_CHECK();
+    orth_dot_kernel<T><<<nb, 256, 0, s>>>(V, ldv, n, k, v, partials, counter, st, hres, 1);
+    HEFF_LAUNCH_CHECK();
+    orth_axpy_kernel<T><<<grid_for(n), 256, sizeof(T) * k, s>>>(V, ldv, n, k, v, v, st, 1);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
 #define INST(C)                                                                                                                              \
     template int multi_dot<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, double *, cudaStream_t);   \
     template int multi_axpy<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, double, Scalar<C>::T *, cudaStream_t);   \
     template int combine<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, cudaStream_t);              \
     template int scale_dev<C>(Scalar<C>::T *, int64_t, const double *, bool, cudaStream_t);                                             \
-    template int residual<C>(const Scalar<C>::T *, const Scalar<C>::T *, double, Scalar<C>::T *, int64_t, cudaStream_t);
+    template int residual<C>(const Scalar<C>::T *, const Scalar<C>::T *, double, Scalar<C>::T *, int64_t, cudaStream_t);                  \
+    template int orth_cgs2<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, double *, unsigned *,     \
+                              double *, Scalar<C>::T *, cudaStream_t);
 INST(false)
 INST(true)
 #undef INST

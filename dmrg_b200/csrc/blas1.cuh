@@ -27,4 +27,12 @@ template<bool CPLX>
 int residual(const typename Scalar<CPLX>::T *ax, const typename Scalar<CPLX>::T *x, double theta, typename Scalar<CPLX>::T *r, int64_t n,
              cudaStream_t s);
 
+// Krylov expansion step on the device: v = (w - V h) / beta with h = V^H w, a second classical Gram-Schmidt
+// pass when ||w - V h||^2 <= 0.5 ||w||^2 (decided on the device), beta = ||v|| before normalisation.
+// st: >= 8 + 4 (MD_MAXK + 2) doubles of state; counter: one zeroed unsigned (left zeroed); hres (device, k+2):
+// hres[j] = h_j (j < k), hres[k] = beta, hres[k+1] = (||w||^2, 1 if the second pass ran).  w and v must differ.
+template<bool CPLX>
+int orth_cgs2(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *w, typename Scalar<CPLX>::T *v,
+              double *partials, unsigned *counter, double *st, typename Scalar<CPLX>::T *hres, cudaStream_t s);
+
 }  // namespace heff

@@ -6,7 +6,8 @@
 //     with the Ritz residual, also after a thick restart); the projection coefficients of A v_last on
 //     the basis are the new column of the Rayleigh-Ritz matrix, so one pass over the basis per iteration,
 //   * FP64 Gram-Schmidt with DGKS selective re-orthogonalisation (a second pass only when the first
-//     removed more than half of the vector's norm squared),
+//     removed more than half of the vector's norm squared), decided and normalised on the device so the
+//     next matvec is enqueued before the host reads the coefficients,
 //   * Rayleigh-Ritz on the host in FP64; Ritz selection smallest / largest algebraic or closest to a target,
 //   * residual norm |beta s_last| from the Krylov relation, checked explicitly (x = V s, r = AV s - theta x)
 //     before convergence is declared.
@@ -87,6 +88,21 @@ static std::vector<int> ritz_order(const std::vector<double> &w, int rule, doubl
     return o;
 }
 
+// Pinned host buffer and event through which the Krylov loop reads each iteration's coefficients while
+// the next matvec runs (created once per operator).
+int eig_host_ready(heff_op *op) {
+    if(!op->eig_host) {
+        cudaError_t e = cudaMallocHost(&op->eig_host, sizeof(double2) * (MD_MAXK + 2));
+        if(e != cudaSuccess) {
+            op->eig_host = nullptr;
+            set_last_cuda_error(e, "eigensolver host buffer", __FILE__, __LINE__);
+            return HEFF_OOM;
+        }
+    }
+    if(!op->eig_event) HEFF_CUDA(cudaEventCreateWithFlags(&op->eig_event, cudaEventDisableTiming));
+    return HEFF_OK;
+}
+
 template<bool CPLX>
 struct Davidson {
     using T  = typename Scalar<CPLX>::T;
@@ -99,8 +115,9 @@ struct Davidson {
     int                    maxb, minb;
     T *V = nullptr, *AV = nullptr, *V2 = nullptr, *AV2 = nullptr, *t = nullptr, *x = nullptr, *ax = nullptr, *r = nullptr;
     T *cg_p = nullptr, *cg_q = nullptr, *cg_z = nullptr, *cg_d = nullptr, *cg_r = nullptr;
-    T *dh = nullptr, *dc = nullptr;
-    double             *partials = nullptr, *dscal = nullptr;
+    T *dh = nullptr, *dc = nullptr, *hres = nullptr;
+    double             *partials = nullptr, *dscal = nullptr, *orth_st = nullptr;
+    unsigned           *orth_counter = nullptr;
     std::vector<HT>     Hk, G2;
     std::vector<void *> allocs;
     double              anorm = 0.0;
@@ -126,8 +143,9 @@ struct Davidson {
     static size_t workspace_bytes(int64_t n, int maxb, bool mixed) {
         const size_t es  = sizeof(T);
         const size_t vec = (es * n + 255) / 256 * 256;
-        return vec * (2 * (maxb + 1) + 2 * maxb + 4 + (mixed ? 5 : 0)) + es * MD_MAXK * 3 + es * MD_MAXK * MD_MAXK +
-               sizeof(double) * MD_BLOCKS * MD_MAXK * 4 + 16 * sizeof(double) + 16 * 256;
+        return vec * (4 * (maxb + 1) + 4 + (mixed ? 5 : 0)) + es * MD_MAXK * 3 + es * MD_MAXK * MD_MAXK +
+               sizeof(double) * MD_BLOCKS * MD_MAXK * 4 + 16 * sizeof(double) + es * (MD_MAXK + 2) +
+               sizeof(double) * (8 + 4 * (MD_MAXK + 2)) + 20 * 256;
     }
     int setup(bool mixed) {
         const size_t es   = sizeof(T);
@@ -149,9 +167,9 @@ struct Davidson {
         carve_ptr  = reinterpret_cast<char *>(op->eig_ws);
         carve_left = op->eig_ws_bytes;
         HEFF_TRY(take((void **)&V, es * n * (maxb + 1)));  // column maxb holds the next Krylov vector
-        HEFF_TRY(take((void **)&AV, es * n * maxb));
+        HEFF_TRY(take((void **)&AV, es * n * (maxb + 1)));  // column maxb holds the product of the next Krylov vector
         HEFF_TRY(take((void **)&V2, es * n * (maxb + 1)));
-        HEFF_TRY(take((void **)&AV2, es * n * maxb));
+        HEFF_TRY(take((void **)&AV2, es * n * (maxb + 1)));
         for(T **p : {&t, &x, &ax, &r}) HEFF_TRY(take((void **)p, es * n));
         if(mixed)
             for(T **p : {&cg_p, &cg_q, &cg_z, &cg_d, &cg_r}) HEFF_TRY(take((void **)p, es * n));
@@ -159,6 +177,11 @@ struct Davidson {
         HEFF_TRY(take((void **)&dc, es * MD_MAXK * MD_MAXK));
         HEFF_TRY(take((void **)&partials, sizeof(double) * MD_BLOCKS * MD_MAXK * 4));
         HEFF_TRY(take((void **)&dscal, sizeof(double) * 16));
+        HEFF_TRY(take((void **)&hres, es * (MD_MAXK + 2)));
+        HEFF_TRY(take((void **)&orth_st, sizeof(double) * (8 + 4 * (MD_MAXK + 2))));
+        HEFF_TRY(take((void **)&orth_counter, 256));
+        HEFF_CUDA(cudaMemsetAsync(orth_counter, 0, sizeof(unsigned), s));
+        HEFF_TRY(eig_host_ready(op));
         Hk.assign((size_t)maxb * maxb, HT(0));
         G2.assign((size_t)maxb * maxb, HT(0));
         return HEFF_OK;
@@ -309,14 +332,6 @@ struct Davidson {
         return sync();  // S must outlive its copy
     }
 
-    double inv_beta_ = 1.0;  // host source of an async copy: must outlive it
-
-    // Phase 1 (thick-restart Krylov / Lanczos structure).  With w = A v_{k-1} projected out of V_k,
-    //   A V_k = V_k H_k + beta v_k e_k^H,
-    // so the projection coefficients ARE the last column of the Rayleigh-Ritz matrix H_k and the Ritz
-    // residual norm is |beta * s_{k-1}|: one pass over the basis per iteration (two when DGKS triggers).
-    // A thick restart keeps Y = V_k S_m (all residuals along v_k) and appends v_k, preserving the relation.
-    // Returns x = Ritz vector (normalised), theta, rnorm (explicit when converged).
     // V[:, 0] = x0 / ||x0|| (a seeded random vector when x0 is NULL or zero)
     int init_start(const void *x0) {
         if(x0)
@@ -336,57 +351,49 @@ struct Davidson {
         return scale(V, 1.0 / std::sqrt(n2));
     }
 
+    // Phase 1 (thick-restart Krylov / Lanczos structure).  With w = A v_{k-1} projected out of V_k,
+    //   A V_k = V_k H_k + beta v_k e_k^H,
+    // so the projection coefficients ARE the last column of the Rayleigh-Ritz matrix H_k and the Ritz
+    // residual norm is |beta * s_{k-1}|.  The projection (with its DGKS second pass) and the normalisation of
+    // v_k run on the device (orth_cgs2), so the product A v_k is enqueued before the host reads the
+    // coefficients: the host's Rayleigh-Ritz step overlaps the GPU's matvec.  A thick restart keeps
+    // Y = V_k S_m (all residuals along v_k) and appends v_k with its product, preserving the relation.
+    // Returns x = Ritz vector (normalised), theta, rnorm (explicit when converged).
     int run(const void *x0, bool use_mixed, double stop_tol, int64_t max_mv, double &theta, double &rnorm, bool &conv) {
         conv  = false;
         theta = 0;
         rnorm = INFINITY;
         HEFF_TRY(init_start(x0));
         std::fill(Hk.begin(), Hk.end(), HT(0));
+        HEFF_TRY(apply(V, AV, !use_mixed));
         int                 k = 1;
         std::vector<double> w;
         std::vector<HT>     vecs;
-        std::vector<T>      hh(MD_MAXK + 1);
+        T                  *hh    = reinterpret_cast<T *>(op->eig_host);
         int                 stagn = 0;
         double              best = INFINITY, verify = 1.0;
         while(true) {
             T *vk = V + (int64_t)k * n;  // slot of the next basis vector
-            HEFF_TRY(apply(V + (int64_t)(k - 1) * n, AV + (int64_t)(k - 1) * n, !use_mixed));
-            HEFF_CUDA(cudaMemcpyAsync(vk, AV + (int64_t)(k - 1) * n, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-            // pass 1 (+ DGKS pass 2): h = V_k^H w and ||w||^2 from one multi_dot over k+1 columns
+            HEFF_TRY(orth_cgs2<CPLX>(V, n, n, k, AV + (int64_t)(k - 1) * n, vk, partials, orth_counter, orth_st, hres, s));
+            HEFF_CUDA(cudaMemcpyAsync(hh, hres, sizeof(T) * (k + 2), cudaMemcpyDeviceToHost, s));
+            HEFF_CUDA(cudaEventRecord(op->eig_event, s));
+            // the product of v_k, needed by the next iteration unless the solve stops here
+            HEFF_TRY(apply(vk, AV + (int64_t)k * n, !use_mixed));
+            HEFF_CUDA(cudaEventSynchronize(op->eig_event));
             std::vector<HT> h(k, HT(0));
-            double          beta2 = 0, w2 = 0;
-            for(int pass = 0; pass < 2; pass++) {
-                HEFF_TRY(multi_dot<CPLX>(V, n, n, k + 1, vk, dh, partials, s));
-                HEFF_TRY(multi_axpy<CPLX>(V, n, n, k, dh, -1.0, vk, s));
-                HEFF_CUDA(cudaMemcpyAsync(hh.data(), dh, sizeof(T) * (k + 1), cudaMemcpyDeviceToHost, s));
-                HEFF_TRY(sync());
-                double hn2 = 0;
-                for(int i = 0; i < k; i++) {
-                    HT v;
-                    std::memcpy((void *)&v, (void *)&hh[i], sizeof(T));
-                    h[i] += v;
-                    hn2 += std::norm(std::complex<double>(v));
-                }
-                HT last;
-                std::memcpy((void *)&last, (void *)&hh[k], sizeof(T));
-                w2    = HostScalar<CPLX>::re(last);
-                beta2 = w2 - hn2;
-                if(!std::isfinite(w2)) {
-                    set_last_error_msg("eigensolver: non-finite vector (NaN/Inf in the operator or start vector)");
-                    return HEFF_NAN_INPUT;
-                }
-                if(beta2 > 0.5 * w2) break;  // no severe cancellation: the Pythagoras norm is accurate
-                if(pass == 1) {
-                    double n2 = 0;
-                    HEFF_TRY(norm2(vk, n2));
-                    beta2 = n2;
-                }
+            for(int i = 0; i < k; i++) std::memcpy((void *)&h[i], (void *)&hh[i], sizeof(T));
+            HT bt, wf;
+            std::memcpy((void *)&bt, (void *)&hh[k], sizeof(T));
+            std::memcpy((void *)&wf, (void *)&hh[k + 1], sizeof(T));
+            const double beta = HostScalar<CPLX>::re(bt), w2 = HostScalar<CPLX>::re(wf);
+            if(!std::isfinite(w2) || !std::isfinite(beta)) {
+                set_last_error_msg("eigensolver: non-finite vector (NaN/Inf in the operator or start vector)");
+                return HEFF_NAN_INPUT;
             }
             for(int i = 0; i < k; i++) {
                 Hk[i + (size_t)maxb * (k - 1)] = h[i];
                 Hk[(k - 1) + (size_t)maxb * i] = HostScalar<CPLX>::conj(h[i]);
             }
-            const double beta = std::sqrt(std::max(0.0, beta2));
             HEFF_TRY(ritz<CPLX>(k, Hk, maxb, w, vecs));
             for(double wi : w) anorm = std::max(anorm, std::fabs(wi));
             const std::vector<int> ord = ritz_order(w, cfg.ritz, cfg.target);
@@ -423,13 +430,11 @@ struct Davidson {
                 conv = rnorm <= stop_tol * std::max(anorm, 1e-300);
                 break;
             }
-            inv_beta_ = 1.0 / beta;
-            HEFF_CUDA(cudaMemcpyAsync(dscal + 9, &inv_beta_, sizeof(double), cudaMemcpyHostToDevice, s));
-            HEFF_TRY(scale_dev<CPLX>(vk, n, dscal + 9, false, s));
             if(k == maxb) {
-                // keep minb Ritz vectors, then append v_k
-                HEFF_TRY(restart(k, minb, w, vecs, ord, false));  // swaps V <-> V2: v_k is now V2[:, k]
+                // keep minb Ritz vectors, then append v_k and its product
+                HEFF_TRY(restart(k, minb, w, vecs, ord, false));  // swaps V <-> V2, AV <-> AV2: v_k is now V2[:, k]
                 HEFF_CUDA(cudaMemcpyAsync(V + (int64_t)minb * n, V2 + (int64_t)k * n, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+                HEFF_CUDA(cudaMemcpyAsync(AV + (int64_t)minb * n, AV2 + (int64_t)k * n, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
                 k = minb + 1;
             } else {
                 k++;
@@ -587,6 +592,7 @@ static int eigs_impl(heff_op *op, const heff_eig_config &cfg, const void *x0, vo
 // rebound operator never allocate).
 int eig_reserve(heff_op *op, int64_t n_max, int max_basis, bool mixed) {
     if(!op) return HEFF_BAD_ARG;
+    HEFF_TRY(eig_host_ready(op));
     const int    maxb = std::max(4, std::min(max_basis > 0 ? max_basis : 32, (int)MD_MAXK - 1));
     const size_t need = op->cplx ? Davidson<true>::workspace_bytes(n_max, maxb, mixed) : Davidson<false>::workspace_bytes(n_max, maxb, mixed);
     if(op->eig_ws_bytes >= need) return HEFF_OK;

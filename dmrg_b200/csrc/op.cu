@@ -275,6 +275,8 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->eig_ws) cudaFree(op->eig_ws);
     if(op->Rtmp) cudaFree(op->Rtmp);
     if(op->diag) cudaFree(op->diag);
+    if(op->eig_host) cudaFreeHost(op->eig_host);
+    if(op->eig_event) cudaEventDestroy(op->eig_event);
     delete op;
     return HEFF_OK;
 }

@@ -22,6 +22,8 @@ struct heff_op {
     // eigensolver workspace, kept across heff_eigs calls on this operator (grown on demand)
     void              *eig_ws       = nullptr;
     size_t             eig_ws_bytes = 0;
+    void              *eig_host     = nullptr;  // pinned: per-iteration coefficients (Krylov loop)
+    cudaEvent_t        eig_event    = nullptr;
     // diagonal of H_eff for the Jacobi preconditioner (computed on first use after create / rebind)
     void              *diag         = nullptr;
     int64_t            diag_cap     = 0;
@@ -45,6 +47,7 @@ int mixed_error_flag(heff_op *op, int *flag);              // mixed.cu
 int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_t Dmax, heff_precision prec, cudaStream_t stream);
 int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3], const void *envR,
               const int64_t rd[3]);
+int eig_host_ready(heff_op *op);     // eig.cu: pinned coefficient buffer + event of the Krylov loop
 int op_diagonal_ready(heff_op *op);  // precond.cu: op->diag holds the diagonal of H_eff (stream-ordered)
 int op_multpc(heff_op *op, const void *x, void *y, double shift);  // precond.cu: y = x / (diag - shift)
 int op_prof_flush(heff_op *op);  // synchronises the op's stream and folds recorded events into prof_ms

@@ -2,6 +2,7 @@
 
     python -m dmrg_b200.profile_cases matvec --chi 1024 --dtype c128 --precision mixed --reps 3
     python -m dmrg_b200.profile_cases eigs --chi 1024 --dtype f64 --precision fp64
+    python -m dmrg_b200.profile_cases fdmrg --L 16 --chi 32 --sweeps 1
 
 The matvec case builds the standalone two-site workload (theta[4,chi,chi], Hermitian-slice environments
 generated on the device, merged two-site Ising MPO) and applies H_eff `reps` times after one warm-up
@@ -41,13 +42,20 @@ def main(argv=None):
     import dmrg_b200 as hb
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["matvec", "eigs"])
+    ap.add_argument("case", choices=["matvec", "eigs", "fdmrg"])
+    ap.add_argument("--L", type=int, default=16)
+    ap.add_argument("--sweeps", type=int, default=1)
     ap.add_argument("--chi", type=int, default=1024)
     ap.add_argument("--D", type=int, default=3)
     ap.add_argument("--dtype", choices=["f64", "c128"], default="c128")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args(argv)
+    if a.case == "fdmrg":  # two-site ground-state sweeps of the random-field Ising chain, fixed fields in [0.5, 1.5)
+        h = 0.5 + np.array([(((i * 0x9E3779B97F4A7C15) >> 11) % 1000003) / 1000003.0 for i in range(1, a.L + 1)])
+        r = hb.fdmrg(h, chi_max=a.chi, sweeps=a.sweeps, seed=2)
+        print("fdmrg", r["energy"], r["num_mv"], r["t_eig"], r["t_svd"], r["t_env"])
+        return 0
     cplx = a.dtype == "c128"
     prec = hb.PREC_MIXED if a.precision == "mixed" else hb.PREC_FP64
     chi, D = a.chi, a.D
