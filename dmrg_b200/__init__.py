@@ -167,6 +167,17 @@ def env_update(side, out, env, env_dims, mps, mps_dims, mpo, mpo_dims, stream=No
     return out
 
 
+def get_expansion_term(side, P, env, env_dims, mps, mps_dims, mpo, mpo_dims, alpha, stream=None):
+    """EnvBase::get_expansion_term (EnvBase.cpp:303-364) on device tensors; side 'L' or 'R'.  P holds
+    spin*chiL*chiR*D elements ([spin, chiL, chiR*DR] for L, the reference's [spin, chiL*DL, chiR] order for R)."""
+    cplx = mps.is_complex()
+    fn = lib().heff_expansion_term_z if cplx else lib().heff_expansion_term_d
+    sd = 0 if side in ("L", 0) else 1
+    rc = fn(sd, ptr(P), ptr(env), dims(env_dims), ptr(mps), dims(mps_dims), ptr(mpo), dims(mpo_dims), float(alpha), _stream_handle(stream))
+    check(rc, "heff_expansion_term")
+    return P
+
+
 def svd(A, rows, cols, rank_max=0, trunc_lim=1e-12, stream=None):
     """svd::solver::do_svd_ptr + truncation (svd.cpp:113-206, 257-280) on a device matrix (float64 or complex128).
 

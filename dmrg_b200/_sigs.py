@@ -99,6 +99,8 @@ def declare(L, sig):
     sig(L, "heff_eigs", _I, [_P, ctypes.POINTER(EigConfig), _P, _P, ctypes.POINTER(EigResult)])
     for n in ("heff_env_update_d", "heff_env_update_z"):
         sig(L, n, _I, [_I, _P, _P, _I64P, _P, _I64P, _P, _I64P, _P])
+    for n in ("heff_expansion_term_d", "heff_expansion_term_z"):
+        sig(L, n, _I, [_I, _P, _P, _I64P, _P, _I64P, _P, _I64P, ctypes.c_double, _P])
     for n in ("heff_svd_d", "heff_svd_z"):
         sig(L, n, _I, [_P, _I64, _I64, _I64, ctypes.c_double, _P, _P, _P, _I64P, _DP, _P])
     for n in ("heff_schmidt_d", "heff_schmidt_z"):

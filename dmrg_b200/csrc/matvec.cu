@@ -178,6 +178,32 @@ int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename
     return HEFF_OK;
 }
 
+// First two stages of the matvec with alpha folded into GEMM 1 and the mix written to `out`:
+//   out[s' + S (a' + cL (b + cR n))] = alpha * sum_{a,m,s} L[a,a',m] x[s,a,b] W[m,n,s,s']
+// which is the L-side subspace-expansion term P of EnvBase::get_expansion_term (EnvBase.cpp:303-333).
+template<bool CPLX>
+int matvec_left_stages(const MatvecDims &d, const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T *L, const typename Scalar<CPLX>::T *W,
+                       typename Scalar<CPLX>::T *out, typename Scalar<CPLX>::T *xp, typename Scalar<CPLX>::T *T1, double alpha, cudaStream_t s) {
+    const int64_t n = d.size_mps();
+    permute_mps_kernel<<<grid_1d(n), 256, 0, s>>>(x, xp, d.S, d.cL, n);
+    HEFF_LAUNCH_CHECK();
+    GemmArgs g1{};
+    g1.M     = (int)(d.cL * d.DL);
+    g1.N     = (int)(d.S * d.cR);
+    g1.K     = (int)d.cL;
+    g1.batch = 1;
+    g1.A     = L;
+    g1.lda   = d.cL;
+    g1.B     = xp;
+    g1.ldb   = d.cL;
+    g1.C     = T1;
+    g1.ldc   = d.cL * d.DL;
+    g1.alpha = make_double2(alpha, 0.0);
+    g1.beta  = make_double2(0.0, 0.0);
+    HEFF_TRY(gemm_f64<CPLX>(/*ta=*/true, /*tb=*/false, false, g1, s));
+    return launch_mix<CPLX>(d, T1, out, W, s);
+}
+
 // ---- deterministic dot product ----
 constexpr int DOT_BLOCKS = 1024;
 template<bool CPLX>
@@ -252,6 +278,10 @@ template int matvec_fp64<false>(const MatvecDims &, const double *, double *, co
                                 const MatvecScratch<false> &, cudaStream_t, cudaEvent_t *);
 template int matvec_fp64<true>(const MatvecDims &, const double2 *, double2 *, const double2 *, const double2 *, const double2 *,
                                const MatvecScratch<true> &, cudaStream_t, cudaEvent_t *);
+template int matvec_left_stages<false>(const MatvecDims &, const double *, const double *, const double *, double *, double *, double *, double,
+                                       cudaStream_t);
+template int matvec_left_stages<true>(const MatvecDims &, const double2 *, const double2 *, const double2 *, double2 *, double2 *, double2 *, double,
+                                      cudaStream_t);
 template int dot_device<false>(const double *, const double *, int64_t, double *, double *, cudaStream_t);
 template int dot_device<true>(const double2 *, const double2 *, int64_t, double2 *, double *, cudaStream_t);
 

@@ -55,4 +55,9 @@ template<bool CPLX>
 int dot_device(const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T *y, int64_t n, typename Scalar<CPLX>::T *out,
                double *partials /* >= 1024 * (CPLX ? 2 : 1) doubles */, cudaStream_t s);
 
+// Stages 1-2 of the matvec (permute, GEMM 1 scaled by alpha, MPO mix into `out`): the L-side expansion term.
+template<bool CPLX>
+int matvec_left_stages(const MatvecDims &d, const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T *L, const typename Scalar<CPLX>::T *W,
+                       typename Scalar<CPLX>::T *out, typename Scalar<CPLX>::T *xp, typename Scalar<CPLX>::T *T1, double alpha, cudaStream_t s);
+
 }  // namespace heff

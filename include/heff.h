@@ -99,6 +99,20 @@ int heff_env_update_d(int side, double *out, const double *env, const int64_t en
 int heff_env_update_z(int side, heff_z *out, const heff_z *env, const int64_t env_dims[3], const heff_z *mps, const int64_t mps_dims[3],
                       const heff_z *mpo, const int64_t mpo_dims[4], void *stream);
 
+/* Subspace-expansion term of one-site DMRG, replacing EnvBase::get_expansion_term(mps,
+ * mpo, alpha) (source/tensors/site/env/EnvBase.cpp:303-364), no conjugation:
+ *   side 0 ('L'): P[s',a',b + chiR*n] = alpha sum env[a,a',m] mps[s,a,b] mpo[m,n,s,s'],
+ *                 P [spin, chiL, chiR*DR], env [chiL,chiL,DL]
+ *   side 1 ('R'): P_flat[s' + spin*(b' + chiR*(a + chiL*m))] = alpha sum env[b,b',n] mps[s,a,b] mpo[m,n,s,s'],
+ *                 P [spin, chiL*DL, chiR] in the reference's memory order (its shuffle
+ *                 {3,0,1,2} of [b',a,m,s'] then a reshape), env [chiR,chiR,DR]
+ * alpha == 0 writes zeros; a NaN alpha returns HEFF_NAN_INPUT (the reference throws).
+ * Device pointers, stream-ordered. */
+int heff_expansion_term_d(int side, double *P, const double *env, const int64_t env_dims[3], const double *mps, const int64_t mps_dims[3],
+                          const double *mpo, const int64_t mpo_dims[4], double alpha, void *stream);
+int heff_expansion_term_z(int side, heff_z *P, const heff_z *env, const int64_t env_dims[3], const heff_z *mps, const int64_t mps_dims[3],
+                          const heff_z *mpo, const int64_t mpo_dims[4], double alpha, void *stream);
+
 /* ---------------------------------------------------------------------------
  * SVD truncation
  * ------------------------------------------------------------------------- */

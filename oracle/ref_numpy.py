@@ -16,6 +16,27 @@ def matvec_einsum(mps, mpo, envL, envR):
     return np.einsum("axm,sab,mnst,byn->txy", envL, mps, mpo, envR, optimize=True)
 
 
+def expansion_term_einsum(side, env, mps, mpo, alpha):
+    """EnvBase::get_expansion_term(mps, mpo, alpha) (EnvBase.cpp:303-364), Eigen semantics restated:
+    a contraction's result lists the free dims of the left operand, then of the right one.
+      L (:311-333): B[a,a',m] . M[s,a,b] over (0,1) -> [a',m,s,b];  . W[m,n,s,s'] over ({1,2},{0,2}) -> [a',b,n,s'];
+                    shuffle {3,0,1,2} -> [s',a',b,n];  reshape [spin, chiL, chiR*DR]
+      R (:335-357): B[b,b',n] . M[s,a,b] over (0,2) -> [b',n,s,a];  . W over ({1,2},{1,2}) -> [b',a,m,s'];
+                    shuffle {3,0,1,2} -> [s',b',a,m];  reshape [spin, chiL*DL, chiR] (memory order kept)
+    alpha == 0 returns zeros (:319-322, :343-346)."""
+    S, cL, cR = mps.shape
+    DL, DR = mpo.shape[0], mpo.shape[1]
+    if side == "L":
+        Q = np.einsum("axm,sab,mnst->txbn", env, mps, mpo)
+        shape = (S, cL, cR * DR)
+    else:
+        Q = np.einsum("byn,sab,mnst->tyam", env, mps, mpo)
+        shape = (S, cL * DL, cR)
+    if alpha == 0:
+        return np.zeros(shape, dtype=Q.dtype, order="F")
+    return np.asfortranarray(alpha * Q.reshape(shape, order="F"))
+
+
 def diagonal_einsum(mps_shape, mpo, envL, envR):
     """MatVecMPOS::get_diagonal_new(0, ...) / get_matrix_element(I, I) (matvec_mpos.cpp:300-407):
     diag[s,a,b] = sum_{m,n} envL[a,a,m] W[m,n,s,s] envR[b,b,n], flattened column-major like the mps."""

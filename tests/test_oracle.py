@@ -134,3 +134,32 @@ def test_diagonal_restatement_matches_dense_heff(c):
     if not c:
         Hc = oracle.dense_heff(th.shape, W, L, R)
         assert np.linalg.norm(d - np.diag(Hc)) < 1e-13 * np.linalg.norm(d)
+
+
+def _expansion_literal(side, B, M, W, alpha):
+    """The Eigen expression of EnvBase.cpp:326-330 / :351-355 written with tensordot (same result-dim order
+    as Eigen's contract: free dims of the left operand, then of the right) and transpose for shuffle."""
+    S, cL, cR = M.shape
+    if side == "L":
+        X = np.tensordot(B, M, axes=([0], [1]))
+        Y = np.tensordot(X, W, axes=([1, 2], [0, 2]))
+        shape = (S, cL, cR * W.shape[1])
+    else:
+        X = np.tensordot(B, M, axes=([0], [2]))
+        Y = np.tensordot(X, W, axes=([1, 2], [1, 2]))
+        shape = (S, cL * W.shape[0], cR)
+    return alpha * Y.transpose(3, 0, 1, 2).reshape(shape, order="F")
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("c", [False, True])
+def test_expansion_term_restatement(side, c):
+    rng = np.random.default_rng(5 if side == "L" else 6)
+    S, cL, cR, D = 2, 5, 4, 3
+    g = (lambda *s: rng.standard_normal(s) + 1j * rng.standard_normal(s)) if c else (lambda *s: rng.standard_normal(s))
+    M = np.asfortranarray(g(S, cL, cR))
+    W = np.asfortranarray(g(D, D, S, S))
+    B = np.asfortranarray(g(cL, cL, D) if side == "L" else g(cR, cR, D))
+    P = rn.expansion_term_einsum(side, B, M, W, 0.7)
+    assert np.linalg.norm(P - _expansion_literal(side, B, M, W, 0.7)) < 1e-13 * np.linalg.norm(P)
+    assert not np.any(rn.expansion_term_einsum(side, B, M, W, 0.0))
