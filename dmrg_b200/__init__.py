@@ -178,6 +178,17 @@ def get_expansion_term(side, P, env, env_dims, mps, mps_dims, mpo, mpo_dims, alp
     return P
 
 
+def dense_eig(A, n, stream=None):
+    """All eigenpairs of a Hermitian n x n device matrix (flat, column-major): heff_dense_eig.  Returns
+    (evals ascending [n] float64, evecs flat column-major [n x n]) as device tensors."""
+    torch = _torch()
+    cplx = A.dtype == torch.complex128
+    ev = torch.empty(n, dtype=torch.float64, device=A.device)
+    V = torch.empty(n * n, dtype=A.dtype, device=A.device)
+    check(lib().heff_dense_eig(C128 if cplx else F64, n, ptr(A), n, ptr(ev), ptr(V), _stream_handle(stream)), "heff_dense_eig")
+    return ev, V
+
+
 def svd(A, rows, cols, rank_max=0, trunc_lim=1e-12, stream=None):
     """svd::solver::do_svd_ptr + truncation (svd.cpp:113-206, 257-280) on a device matrix (float64 or complex128).
 
@@ -452,6 +463,15 @@ class MatVecMPOS:
         if rc not in (HEFF_OK, 5):
             check(rc, "heff_eigs")
         return res.eigval, res.as_dict()
+
+    def get_matrix(self):
+        """Dense H_eff as the reference's get_matrix (matvec_mpo.cpp:313-332): device [rows x rows] column-major
+        tensor (a flat tensor viewed as its transpose in torch's row-major view), M[(s,a,b),(s',a',b')]."""
+        torch = _torch()
+        n = self.rows()
+        M = torch.empty(n * n, dtype=torch.complex128 if self.cplx else torch.float64, device="cuda")
+        check(lib().heff_op_get_matrix(self.handle, ptr(M)), "heff_op_get_matrix")
+        return M
 
     def diagonal(self):
         """Diagonal of H_eff (get_diagonal_new, matvec_mpos.cpp:300-407) as a device tensor of rows() elements."""

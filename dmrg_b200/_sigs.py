@@ -90,6 +90,8 @@ def declare(L, sig):
     sig(L, "heff_make_vector", _I, [_I, _I64, ctypes.c_uint64, _P, _P])
     sig(L, "heff_op_device_error", _I, [_P, ctypes.POINTER(ctypes.c_int)])
     sig(L, "heff_op_diagonal", _I, [_P, _P])
+    sig(L, "heff_op_get_matrix", _I, [_P, _P])
+    sig(L, "heff_dense_eig", _I, [_I, _I64, _P, _I64, _P, _P, _P])
     sig(L, "heff_op_multpc", _I, [_P, _P, _P, ctypes.c_double])
     sig(L, "heff_gemm_bf16_f32", _I, [_P, _P, _P, _I64, _I64, _I64, _P])
     sig(L, "heff_ensemble_run", _I, [ctypes.POINTER(DmrgConfig), _I, _I, ctypes.POINTER(DmrgResult), ctypes.POINTER(ctypes.c_int), _DP])

@@ -193,6 +193,20 @@ int heff_op_device_error(heff_op *op, int *code);
  * elements of the operator's dtype (stream-ordered).  Computed once per operator
  * (and per rebind) like CalcPc's readyCalcPc flag. */
 int heff_op_diagonal(heff_op *op, void *diag_out);
+/* Dense effective Hamiltonian, replacing MatVecMPO(S)::get_matrix (source/math/eig/
+ * matvec/matvec_mpo.cpp:313-332, matvec_mpos.cpp:1570-1588): M[(s,a,b), (s',a',b')] =
+ * sum_{m,n} envL[a,a',m] W[m,n,s,s'] envR[b,b',n], rows() x rows() column-major in
+ * the operator's dtype.  As in the reference the row index is the matvec's input
+ * index, so M is the transpose of the matrix applied by MultAx (its complex
+ * conjugate when H_eff is Hermitian).  Device buffer, stream-ordered. */
+int heff_op_get_matrix(heff_op *op, void *M_out);
+/* All eigenpairs of a Hermitian n x n device matrix (lda >= n), replacing the dense
+ * eig::solver path (LAPACK ?syevr / ?heevd on get_matrix, used by the reference for
+ * problem sizes <= eig_max_size = 4096, AlgorithmFinite.cpp:318): evals (device, n
+ * doubles) ascending, evecs (device, n x n, leading dimension n) the matching
+ * orthonormal eigenvectors.  FP64 one-sided Jacobi on the Gershgorin-shifted
+ * positive-definite matrix; n <= 16384.  Synchronises the stream. */
+int heff_dense_eig(heff_dtype dtype, int64_t n, const void *A, int64_t lda, double *evals, void *evecs, void *stream);
 /* Jacobi preconditioner, replacing MatVecMPOS::MultPc(T*, T*, T shift) with
  * jcbMaxBlockSize == 1 (matvec_mpos.cpp:1349-1364): y = x / (diag - shift), the
  * denominator kept >= 1e-10 max(|shift|, 1) in magnitude.  Device buffers,

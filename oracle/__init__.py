@@ -19,6 +19,7 @@ from .clib import (  # noqa: F401
     expval,
     env_update,
     dense_heff,
+    get_matrix,
     mpo_ising,
     mpo_edge_left,
     mpo_edge_right,

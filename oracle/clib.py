@@ -42,6 +42,10 @@ def lib():
             f.restype = ctypes.c_int
         L.oracle_dense_heff_d.argtypes = [_DP, _I64x, _DP, _I64x, _DP, _I64x, _DP, _I64x]
         L.oracle_dense_heff_d.restype = ctypes.c_int
+        for nm in ("oracle_get_matrix_d", "oracle_get_matrix_z"):
+            f = getattr(L, nm)
+            f.argtypes = [_DP, _I64x, _DP, _I64x, _DP, _I64x, _DP, _I64x]
+            f.restype = ctypes.c_int
         L.oracle_mpo_ising.argtypes = [_DP, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.oracle_mpo_ising.restype = None
         for name in ("oracle_mpo_edge_left", "oracle_mpo_edge_right"):
@@ -133,6 +137,19 @@ def dense_heff(mps_shape, mpo, envL, envR):
     if rc != 0:
         raise ValueError("oracle_dense_heff: dimension mismatch")
     return H
+
+
+def get_matrix(mps_shape, mpo, envL, envR):
+    """MatVecMPO::get_matrix (matvec_mpo.cpp:313-332): M[(s,a,b),(s',a',b')], the transpose of dense_heff."""
+    c = _is_cplx(mpo, envL, envR)
+    mpo, envL, envR = (_f(x, c) for x in (mpo, envL, envR))
+    n = int(np.prod(mps_shape))
+    M = np.zeros((n, n), dtype=np.complex128 if c else np.float64, order="F")
+    md = (ctypes.c_int64 * 3)(*mps_shape)
+    fn = lib().oracle_get_matrix_z if c else lib().oracle_get_matrix_d
+    if fn(_p(M), md, _p(mpo), _dims(mpo), _p(envL), _dims(envL), _p(envR), _dims(envR)) != 0:
+        raise ValueError("oracle_get_matrix: dimension mismatch")
+    return M
 
 
 def mpo_ising(J, h, eshift=0.0):

@@ -63,9 +63,9 @@ int oracle_env_update_z(int side, double *out, const double *env, const int64_t 
                       (const double _Complex *)mpo, wd);
 }
 
-/* matvec_mpo.cpp:427-428: envL.contract(mpo,{2},{0}).contract(envR,{2},{2}).shuffle({2,0,4,3,1,5}) gives
- * H[s',a',b', s,a,b]... here restated directly as H[(s',a',b'),(s,a,b)] = sum_{m,n} L[a,a',m] W[m,n,s,s'] R[b,b',n]
- * so that y = H x reproduces oracle_matvec_d for x = theta. */
+/* The matrix of the matvec, H[(s',a',b'),(s,a,b)] = sum_{m,n} L[a,a',m] W[m,n,s,s'] R[b,b',n], so that y = H x
+ * reproduces oracle_matvec_d for x = theta (contraction_tblis.cpp:277-290).  The reference's get_matrix
+ * (oracle_get_matrix_*) is its transpose. */
 int oracle_dense_heff_d(double *H, const int64_t md[3], const double *W, const int64_t wd[4], const double *L, const int64_t ld[3], const double *R,
                         const int64_t rd[3]) {
     const int64_t S = md[0], cL = md[1], cR = md[2], DL = wd[0], DR = wd[1];
@@ -86,6 +86,16 @@ int oracle_dense_heff_d(double *H, const int64_t md[3], const double *W, const i
                         }
             }
     return 0;
+}
+
+int oracle_get_matrix_d(double *M, const int64_t md[3], const double *W, const int64_t wd[4], const double *L, const int64_t ld[3], const double *R,
+                        const int64_t rd[3]) {
+    return get_matrix_impl_d(M, md, W, wd, L, ld, R, rd);
+}
+int oracle_get_matrix_z(double *M, const int64_t md[3], const double *W, const int64_t wd[4], const double *L, const int64_t ld[3], const double *R,
+                        const int64_t rd[3]) {
+    return get_matrix_impl_z((double _Complex *)M, md, (const double _Complex *)W, wd, (const double _Complex *)L, ld, (const double _Complex *)R,
+                             rd);
 }
 
 /* IsingRandomField::get_mpo, IsingRandomField.cpp:122-129, Pauli matrices qm/spin/half.cpp:9-17.

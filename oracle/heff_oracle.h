@@ -48,9 +48,14 @@ int oracle_env_update_d(int side, double *out, const double *env, const int64_t 
 int oracle_env_update_z(int side, double *out, const double *env, const int64_t env_dims[3], const double *mps, const int64_t mps_dims[3],
                         const double *mpo, const int64_t mpo_dims[4]);
 
-/* Dense H_eff matrix, MatVecMPO::get_tensor/get_matrix (matvec_mpo.cpp:416-435):
- * H[(s',a',b'), (s,a,b)] column-major, rows = spin*chiL*chiR. */
+/* Dense matrix of the matvec: H[(s',a',b'), (s,a,b)] column-major (y = H theta), rows = spin*chiL*chiR. */
 int oracle_dense_heff_d(double *H, const int64_t mps_dims[3], const double *mpo, const int64_t mpo_dims[4], const double *envL,
+                        const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3]);
+/* MatVecMPO::get_tensor/get_matrix (matvec_mpo.cpp:313-332): M[(s,a,b), (s',a',b')] column-major, the
+ * transpose of the dense matvec matrix above.  _z: interleaved complex buffers. */
+int oracle_get_matrix_d(double *M, const int64_t mps_dims[3], const double *mpo, const int64_t mpo_dims[4], const double *envL,
+                        const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3]);
+int oracle_get_matrix_z(double *M, const int64_t mps_dims[3], const double *mpo, const int64_t mpo_dims[4], const double *envL,
                         const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3]);
 
 /* IsingRandomField::get_mpo (IsingRandomField.cpp:122-129): W[3,3,2,2] real. */

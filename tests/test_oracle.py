@@ -163,3 +163,15 @@ def test_expansion_term_restatement(side, c):
     P = rn.expansion_term_einsum(side, B, M, W, 0.7)
     assert np.linalg.norm(P - _expansion_literal(side, B, M, W, 0.7)) < 1e-13 * np.linalg.norm(P)
     assert not np.any(rn.expansion_term_einsum(side, B, M, W, 0.0))
+
+
+@pytest.mark.parametrize("c", [False, True])
+def test_get_matrix_restatement_is_transpose_of_matvec_matrix(c):
+    """get_tensor's shuffle {2,0,4,3,1,5} puts the input index first: get_matrix = (matrix of the matvec)^T."""
+    th, W, L, R = ph.heff_inputs(4, D=3, cplx=c, seed=41, chiR=3)
+    M = oracle.get_matrix(th.shape, W, L, R)
+    H = np.einsum("axm,mnst,byn->txysab", L, W, R).reshape(th.size, th.size, order="F")
+    assert np.linalg.norm(M - H.T) < 1e-13 * np.linalg.norm(H)
+    # the literal Eigen expression (contract, contract, shuffle, column-major cast)
+    G = np.tensordot(np.tensordot(L, W, axes=([2], [0])), R, axes=([2], [2])).transpose(2, 0, 4, 3, 1, 5)
+    assert np.linalg.norm(M - G.reshape(th.size, th.size, order="F")) < 1e-13 * np.linalg.norm(H)
