@@ -167,6 +167,18 @@ def env_update(side, out, env, env_dims, mps, mps_dims, mpo, mpo_dims, stream=No
     return out
 
 
+def matrix_vector_product_multi(res, mps, mps_dims, mpos, mpo_dims, envL, envL_dims, envR, envR_dims, stream=None):
+    """Multi-MPO matrix_vector_product (contraction_tblis.cpp:307-420): a list of device site MPOs [D, D', d, d]
+    applied one at a time; mps [prod d, chiL, chiR] (site 1 fastest)."""
+    cplx = mps.is_complex()
+    fn = lib().heff_matvec_multi_z if cplx else lib().heff_matvec_multi_d
+    arr = (_P * len(mpos))(*[ctypes.c_void_p(m.data_ptr()) for m in mpos])
+    md = (ctypes.c_int64 * (4 * len(mpos)))(*[int(x) for d4 in mpo_dims for x in d4])
+    rc = fn(ptr(res), ptr(mps), dims(mps_dims), len(mpos), arr, md, ptr(envL), dims(envL_dims), ptr(envR), dims(envR_dims), _stream_handle(stream))
+    check(rc, "heff_matvec_multi")
+    return res
+
+
 def get_expansion_term(side, P, env, env_dims, mps, mps_dims, mpo, mpo_dims, alpha, stream=None):
     """EnvBase::get_expansion_term (EnvBase.cpp:303-364) on device tensors; side 'L' or 'R'.  P holds
     spin*chiL*chiR*D elements ([spin, chiL, chiR*DR] for L, the reference's [spin, chiL*DL, chiR] order for R)."""

@@ -91,6 +91,8 @@ def declare(L, sig):
     sig(L, "heff_op_device_error", _I, [_P, ctypes.POINTER(ctypes.c_int)])
     sig(L, "heff_op_diagonal", _I, [_P, _P])
     sig(L, "heff_op_get_matrix", _I, [_P, _P])
+    for n in ("heff_matvec_multi_d", "heff_matvec_multi_z"):
+        sig(L, n, _I, [_P, _P, _I64P, _I, ctypes.POINTER(_P), _I64P, _P, _I64P, _P, _I64P, _P])
     sig(L, "heff_dense_eig", _I, [_I, _I64, _P, _I64, _P, _P, _P])
     sig(L, "heff_op_multpc", _I, [_P, _P, _P, ctypes.c_double])
     sig(L, "heff_gemm_bf16_f32", _I, [_P, _P, _P, _I64, _I64, _I64, _P])

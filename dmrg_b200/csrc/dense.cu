@@ -99,7 +99,11 @@ static int dn_grid(int64_t n) {
 
 template<bool CPLX>
 static int get_matrix_impl(heff_op *op, void *Mout) {
-    using T             = typename Scalar<CPLX>::T;
+    using T = typename Scalar<CPLX>::T;
+    if(op->sequential) {  // as MatVecMPOS::get_tensor, matvec_mpos.cpp:1587
+        set_last_error_msg("get_matrix: not implemented for more than one (unmerged) MPO");
+        return HEFF_BAD_ARG;
+    }
     const MatvecDims &d = op->d;
     const size_t smem   = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S);
     if(smem > 48 * 1024) return HEFF_BAD_SHAPE;

@@ -40,9 +40,106 @@ struct HostC {
     double re = 0, im = 0;
     HostC() = default;
     HostC(double r, double i) : re(r), im(i) {}
+    explicit HostC(double r) : re(r), im(0.0) {}
     HostC operator+(const HostC &o) const { return {re + o.re, im + o.im}; }
     HostC operator*(const HostC &o) const { return {re * o.re - im * o.im, re * o.im + im * o.re}; }
 };
+
+// Operator over more than 5 site MPOs: like the reference (matvec_mpos.cpp:104-123) the MPOs are not merged; the
+// matvec applies them one at a time (matvec_multi).  FP64 only (the split-BF16 path needs the merged MPO).
+template<bool CPLX>
+static int create_sequential(heff_op **out, int nsites, const void *const *mpos, const int64_t *mdims, const void *envL, const int64_t ld[3],
+                             const void *envR, const int64_t rd[3], heff_precision prec, cudaStream_t stream) {
+    using T  = typename Scalar<CPLX>::T;
+    using HT = typename std::conditional<CPLX, HostC, double>::type;
+    if(prec != HEFF_PREC_FP64) {
+        set_last_error_msg("operator over %d site MPOs: mixed precision needs the merged MPO (at most 5 sites)", nsites);
+        return HEFF_BAD_ARG;
+    }
+    int64_t S = 1;
+    for(int i = 0; i < nsites; i++) S *= mdims[4 * i + 2];
+    const int64_t md[3] = {S, ld[0], rd[0]};
+    MultiDims     mdm;
+    HEFF_TRY(check_multi_dims(md, nsites, mdims, ld, rd, mdm));
+    const int64_t D0 = mdims[0], DK = mdims[4 * (nsites - 1) + 1];
+    heff_op      *op   = new heff_op();
+    op->cplx           = CPLX;
+    op->d              = MatvecDims{S, ld[0], rd[0], D0, DK};
+    op->precision      = HEFF_PREC_FP64;
+    op->stream         = stream;
+    op->sequential     = true;
+    op->multi          = mdm;
+    op->mpo_dims[0] = D0, op->mpo_dims[1] = DK, op->mpo_dims[2] = S, op->mpo_dims[3] = S;
+    const size_t es   = sizeof(T);
+    auto         fail = [&](int rc) {
+        heff_op_destroy(op);
+        return rc;
+    };
+    // site MPOs to the device; the s == s' part of the merged MPO on the host:
+    //   Wd[m0, mK, s] = sum_{m_1..m_{K-1}} prod_i W_i[m_{i-1}, m_i, s_i, s_i]
+    std::vector<HT> Wd;
+    int64_t         Dc = D0, Sc = 1;
+    for(int i = 0; i < nsites; i++) {
+        const int64_t *di = mdims + 4 * i;
+        const size_t   n  = (size_t)(di[0] * di[1] * di[2] * di[3]);
+        std::vector<HT> Wi(n);
+        if(cudaMemcpy(Wi.data(), mpos[i], n * es, cudaMemcpyDefault) != cudaSuccess) return fail(HEFF_CUDA_ERROR);
+        void *dW = nullptr;
+        if(cudaMalloc(&dW, n * es) != cudaSuccess) return fail(HEFF_OOM);
+        op->seq_W.push_back(dW);
+        if(cudaMemcpy(dW, Wi.data(), n * es, cudaMemcpyHostToDevice) != cudaSuccess) return fail(HEFF_CUDA_ERROR);
+        const int64_t   Dn = di[1], d = di[2];
+        std::vector<HT> nxt((size_t)(D0 * Dn * Sc * d), HT{});
+        for(int64_t t = 0; t < d; t++)
+            for(int64_t sc = 0; sc < Sc; sc++)
+                for(int64_t n2 = 0; n2 < Dn; n2++)
+                    for(int64_t m0 = 0; m0 < D0; m0++) {
+                        HT acc{};
+                        for(int64_t k = 0; k < Dc; k++) {
+                            const HT prev = i == 0 ? (k == m0 ? HT(1.0) : HT(0.0)) : Wd[m0 + D0 * (k + Dc * sc)];
+                            acc           = acc + prev * Wi[k + di[0] * (n2 + Dn * (t + d * t))];
+                        }
+                        nxt[m0 + D0 * (n2 + Dn * (sc + Sc * t))] = acc;
+                    }
+        Wd = std::move(nxt);
+        Dc = Dn;
+        Sc *= d;
+    }
+    const int64_t nWfull = D0 * DK * S * S;
+    if(nWfull <= (int64_t)1 << 24) {  // the diagonal-only merged MPO, laid out like a merged MPO for the diagonal kernel
+        std::vector<HT> Wf((size_t)nWfull, HT{});
+        for(int64_t s = 0; s < S; s++)
+            for(int64_t n2 = 0; n2 < DK; n2++)
+                for(int64_t m0 = 0; m0 < D0; m0++) Wf[m0 + D0 * (n2 + DK * (s + S * s))] = Wd[m0 + D0 * (n2 + DK * s)];
+        if(cudaMalloc(&op->W, nWfull * es) != cudaSuccess) return fail(HEFF_OOM);
+        if(cudaMemcpy(op->W, Wf.data(), nWfull * es, cudaMemcpyHostToDevice) != cudaSuccess) return fail(HEFF_CUDA_ERROR);
+    }
+    const MatvecDims &d  = op->d;
+    const int64_t     nL = d.cL * d.cL * d.DL, nR = d.size_Rp();
+    if(cudaMalloc(&op->L, nL * es) != cudaSuccess) return fail(HEFF_OOM);
+    if(cudaMalloc(&op->Rp, nR * es) != cudaSuccess) return fail(HEFF_OOM);
+    const int64_t nscr = multi_scratch_elems(mdm);
+    if(cudaMalloc(&op->scratch, nscr * es) != cudaSuccess) return fail(HEFF_OOM);
+    op->scratch_bytes = (size_t)nscr * es;
+    void *Rtmp        = nullptr;
+    if(cudaMalloc(&Rtmp, nR * es) != cudaSuccess) return fail(HEFF_OOM);
+    cudaError_t e = cudaMemcpyAsync(op->L, envL, nL * es, cudaMemcpyDefault, stream);
+    if(e == cudaSuccess) e = cudaMemcpyAsync(Rtmp, envR, nR * es, cudaMemcpyDefault, stream);
+    int rc = e == cudaSuccess ? permute_R<CPLX>(reinterpret_cast<const T *>(Rtmp), reinterpret_cast<T *>(op->Rp), d, stream) : HEFF_CUDA_ERROR;
+    const cudaError_t e2 = cudaStreamSynchronize(stream);
+    cudaFree(Rtmp);
+    if(e != cudaSuccess) {
+        set_last_cuda_error(e, "heff_op_create copies", __FILE__, __LINE__);
+        return fail(HEFF_CUDA_ERROR);
+    }
+    if(rc != HEFF_OK) return fail(rc);
+    if(e2 != cudaSuccess) {
+        set_last_cuda_error(e2, "heff_op_create sync", __FILE__, __LINE__);
+        return fail(HEFF_CUDA_ERROR);
+    }
+    *out = op;
+    return HEFF_OK;
+}
 
 template<bool CPLX>
 static int create_impl(heff_op **out, int nsites, const void *const *mpos, const int64_t *mdims, const void *envL, const int64_t ld[3],
@@ -50,7 +147,8 @@ static int create_impl(heff_op **out, int nsites, const void *const *mpos, const
     using T  = typename Scalar<CPLX>::T;
     using HT = typename std::conditional<CPLX, HostC, double>::type;
     static_assert(sizeof(HT) == sizeof(T), "host/device scalar size");
-    if(!out || nsites < 1 || nsites > 5 || !mpos || !mdims || !envL || !envR || !ld || !rd) return HEFF_BAD_ARG;
+    if(!out || nsites < 1 || !mpos || !mdims || !envL || !envR || !ld || !rd) return HEFF_BAD_ARG;
+    if(nsites > 5) return create_sequential<CPLX>(out, nsites, mpos, mdims, envL, ld, envR, rd, prec, stream);
     // --- gather the site MPOs on the host and merge them (setup only, tiny) ---
     std::vector<HT> W;
     int64_t         wd[4];
@@ -235,6 +333,14 @@ static int apply_impl(heff_op *op, const void *x, void *y) {
         set_last_error_msg("MultAx: in and out must not alias");
         return HEFF_BAD_ARG;
     }
+    if(op->sequential) {
+        std::vector<const T *> W(op->seq_W.size());
+        for(size_t i = 0; i < W.size(); i++) W[i] = reinterpret_cast<const T *>(op->seq_W[i]);
+        HEFF_TRY(matvec_multi<CPLX>(op->multi, reinterpret_cast<const T *>(x), reinterpret_cast<T *>(y), reinterpret_cast<const T *>(op->L),
+                                    reinterpret_cast<const T *>(op->Rp), W.data(), reinterpret_cast<T *>(op->scratch), op->stream));
+        op->num_mv++;
+        return HEFF_OK;
+    }
     MatvecScratch<CPLX> ws;
     ws.carve(reinterpret_cast<T *>(op->scratch), op->d);
     HEFF_TRY(matvec_fp64<CPLX>(op->d, reinterpret_cast<const T *>(x), reinterpret_cast<T *>(y), reinterpret_cast<const T *>(op->L),
@@ -274,6 +380,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->stage_x) cudaFree(op->stage_x);
     if(op->eig_ws) cudaFree(op->eig_ws);
     if(op->Rtmp) cudaFree(op->Rtmp);
+    for(void *p : op->seq_W) cudaFree(p);
     if(op->diag) cudaFree(op->diag);
     if(op->eig_host) cudaFreeHost(op->eig_host);
     if(op->eig_event) cudaEventDestroy(op->eig_event);
@@ -332,6 +439,10 @@ extern "C" int heff_op_set_stream(heff_op *op, void *stream) {
 extern "C" int heff_op_set_precision(heff_op *op, heff_precision precision) {
     if(!op) return HEFF_BAD_ARG;
     if(precision != HEFF_PREC_FP64 && precision != HEFF_PREC_MIXED) return HEFF_BAD_ARG;
+    if(op->sequential && precision != HEFF_PREC_FP64) {
+        set_last_error_msg("operator over more than 5 site MPOs: FP64 only");
+        return HEFF_BAD_ARG;
+    }
     op->precision = precision;
     return HEFF_OK;
 }

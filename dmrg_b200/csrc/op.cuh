@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "matvec.cuh"
+#include "multi.cuh"
 
 struct heff_op {
     bool               cplx = false;
@@ -11,6 +12,11 @@ struct heff_op {
     heff_precision     precision   = HEFF_PREC_FP64;
     cudaStream_t       stream      = nullptr;
     void              *L = nullptr, *Rp = nullptr, *W = nullptr;  // device: envL (reference layout), R', merged W
+    // more than 5 site MPOs (matvec_mpos.cpp:104-123): applied one at a time (multi.cu); W then holds only the
+    // s == s' entries of the merged MPO (for the preconditioner diagonal)
+    bool               sequential = false;
+    heff::MultiDims    multi{};
+    std::vector<void *> seq_W;
     void              *scratch       = nullptr;                    // x' | T1 | T2
     size_t             scratch_bytes = 0;
     void              *stage_x       = nullptr;  // device staging for MultAx with host buffers

@@ -59,6 +59,10 @@ static int pc_grid(int64_t n) {
 
 int op_diagonal_ready(heff_op *op) {
     if(op->diag_ready) return HEFF_OK;
+    if(!op->W) {
+        set_last_error_msg("preconditioner diagonal: the site MPOs are too large to tabulate their s == s' part");
+        return HEFF_BAD_SHAPE;
+    }
     const MatvecDims &d  = op->d;
     const int64_t     n  = d.size_mps();
     const size_t      es = op->cplx ? 16 : 8;

@@ -61,6 +61,17 @@ int heff_matvec_d(double *res, const double *mps, const int64_t mps_dims[3], con
 int heff_matvec_z(heff_z *res, const heff_z *mps, const int64_t mps_dims[3], const heff_z *mpo, const int64_t mpo_dims[4], const heff_z *envL,
                   const int64_t envL_dims[3], const heff_z *envR, const int64_t envR_dims[3], void *stream);
 
+/* res = H_eff * mps with a chain of nmpo site MPOs (mpos[i] device pointers, unshuffled
+ * [D_{i-1}, D_i, d_i, d_i], dims 4 per MPO in mpo_dims), replacing the multi-MPO
+ * matrix_vector_product (contraction_tblis.cpp:307-420, used for more than 5 sites,
+ * matvec_mpos.cpp:104-123): the MPOs are applied one at a time, never merged;
+ * mps [prod d_i, chiL, chiR] with site 1's index fastest.  The reference also
+ * accepts MPOs pre-shuffled {2,3,0,1}; this entry point takes them unshuffled. */
+int heff_matvec_multi_d(double *res, const double *mps, const int64_t mps_dims[3], int nmpo, const double *const *mpos, const int64_t *mpo_dims,
+                        const double *envL, const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3], void *stream);
+int heff_matvec_multi_z(heff_z *res, const heff_z *mps, const int64_t mps_dims[3], int nmpo, const heff_z *const *mpos, const int64_t *mpo_dims,
+                        const heff_z *envL, const int64_t envL_dims[3], const heff_z *envR, const int64_t envR_dims[3], void *stream);
+
 /* Same product and arguments as heff_matvec_d, but allocating no device memory.
  * No counterpart in the reference: it exists for callers that cannot let a
  * library call cudaMalloc (a process that has already split all device memory
@@ -151,7 +162,10 @@ typedef struct heff_op heff_op;
 
 /* Constructor: MatVecMPOS<T>(mpos, env_pair) (matvec_mpos.cpp:40-130).  The
  * nsites site MPOs (each [mL, mR, d, d]) are merged into one
- * [mL0, mR_last, prod d, prod d] MPO as in matvec_mpos.cpp:104-119 (nsites <= 5).
+ * [mL0, mR_last, prod d, prod d] MPO as in matvec_mpos.cpp:104-119 (nsites <= 5);
+ * with more sites they are kept apart and applied one at a time (as
+ * matvec_mpos.cpp:120-123 / contraction_tblis.cpp:307-420; FP64 only, no
+ * heff_op_get_matrix).
  * envL [chiL, chiL, mL0], envR [chiR, chiR, mR_last].  Buffers live in `where`
  * (host or device); the operator keeps its own device copies, laid out for the
  * kernels.  precision selects the FP64 tensor-core path or the mixed split

@@ -16,6 +16,34 @@ def matvec_einsum(mps, mpo, envL, envR):
     return np.einsum("axm,sab,mnst,byn->txy", envL, mps, mpo, envR, optimize=True)
 
 
+def matvec_multi_literal(mps, mpos, envL, envR):
+    """The multi-MPO matrix_vector_product (contraction_tblis.cpp:307-420, Eigen path) restated step by step
+    with tensordot (same result-dim order as Eigen's contract) and column-major reshapes.  mpos are
+    unshuffled [m, n, s, s']; the reference first shuffles them {2,3,0,1} (:313-320)."""
+    shf = [np.transpose(W, (2, 3, 0, 1)) for W in mpos]
+    K = len(shf)
+
+    def prod(fr, to):  # mpodimprod (:337-346)
+        p = 1
+        if to == 0:
+            return p
+        for idx in range(fr, to):
+            if idx >= K:
+                break
+            p *= shf[idx].shape[1]
+        return p
+
+    shp6 = (prod(0, 1), prod(1, K), mps.shape[2], envL.shape[1], envL.shape[2], 1)
+    t = np.tensordot(mps, envL, axes=([1], [0])).reshape(shp6, order="F").transpose(0, 1, 2, 3, 5, 4)  # :375
+    for idx in range(K):  # :377-398
+        mpo = shf[idx]
+        shp6 = (prod(idx + 1, idx + 2), prod(idx + 2, K), t.shape[2], t.shape[3], prod(0, idx + 1), mpo.shape[3])
+        t = np.tensordot(t, mpo, axes=([0, 5], [0, 2])).reshape(shp6, order="F")
+    d0, d1, d2, d3 = t.shape[0] * t.shape[1] * t.shape[2], t.shape[3], t.shape[4], t.shape[5]
+    out = np.tensordot(t.reshape((d0, d1, d2, d3), order="F"), envR, axes=([0, 3], [0, 2])).transpose(1, 0, 2)  # :415
+    return np.asfortranarray(out)
+
+
 def expansion_term_einsum(side, env, mps, mpo, alpha):
     """EnvBase::get_expansion_term(mps, mpo, alpha) (EnvBase.cpp:303-364), Eigen semantics restated:
     a contraction's result lists the free dims of the left operand, then of the right one.

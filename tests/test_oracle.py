@@ -175,3 +175,23 @@ def test_get_matrix_restatement_is_transpose_of_matvec_matrix(c):
     # the literal Eigen expression (contract, contract, shuffle, column-major cast)
     G = np.tensordot(np.tensordot(L, W, axes=([2], [0])), R, axes=([2], [2])).transpose(2, 0, 4, 3, 1, 5)
     assert np.linalg.norm(M - G.reshape(th.size, th.size, order="F")) < 1e-13 * np.linalg.norm(H)
+
+
+@pytest.mark.parametrize("nsites,c", [(1, False), (2, True), (3, False), (6, True)])
+def test_multi_mpo_literal_equals_merged(nsites, c):
+    """The reference's sequential multi-MPO contraction equals the matvec with the merged MPO
+    (matvec_mpos.cpp:104-119 order: site 1's physical index fastest)."""
+    rng = np.random.default_rng(nsites)
+    g = (lambda *s: rng.standard_normal(s) + 1j * rng.standard_normal(s)) if c else (lambda *s: rng.standard_normal(s))
+    Ds = [3, 2, 4, 3, 2, 3, 2][: nsites + 1]
+    mpos = [np.asfortranarray(g(Ds[i], Ds[i + 1], 2, 2)) for i in range(nsites)]
+    W = mpos[0]
+    for Wi in mpos[1:]:
+        W = oracle.mpo_merge(W, Wi)
+    chiL, chiR = 5, 4
+    th = np.asfortranarray(g(2 ** nsites, chiL, chiR))
+    L = np.asfortranarray(g(chiL, chiL, Ds[0]))
+    R = np.asfortranarray(g(chiR, chiR, Ds[nsites]))
+    y = rn.matvec_multi_literal(th, mpos, L, R)
+    ref = rn.matvec_einsum(th, W, L, R)
+    assert np.linalg.norm(y - ref) < 1e-12 * np.linalg.norm(ref)
