@@ -1,4 +1,5 @@
 // tcgen05 BF16 GEMM (see gemm_bf16x.cuh).
+#include <algorithm>
 #include <cstring>
 
 #include "gemm_bf16x.cuh"
@@ -88,38 +89,67 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 
 constexpr int X_GROUP_M = 8;
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
+}
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__device__ __forceinline__ void x_tile_mn(const XGemmArgs &p, int tile, int &m0, int &n0) {
+    const int num_m = (p.M + X_BM - 1) / X_BM, num_n = (p.N + X_BN - 1) / X_BN;
+    const int per_group = X_GROUP_M * num_n;
+    const int first_m   = (tile / per_group) * X_GROUP_M;
+    const int gsize     = min(num_m - first_m, X_GROUP_M);
+    m0                  = (first_m + (tile % per_group) % gsize) * X_BM;
+    n0                  = ((tile % per_group) / gsize) * X_BN;
+}
+
+__device__ __forceinline__ void x_store(const XGemmArgs &p, int row, int n, float v) {
+    if(p.mode == X_OUT_F32)
+        reinterpret_cast<float *>(p.C)[row + p.ldc * n] = v;
+    else if(p.mode == X_OUT_F32_ACC)
+        reinterpret_cast<float *>(p.C)[row + p.ldc * n] += v;
+    else if(p.mode == X_OUT_F64)
+        reinterpret_cast<double *>(p.C)[row + p.ldc * n] = (double)v;
+    else {
+        const bool im = n >= p.n_half;
+        const int  nn = im ? n - p.n_half : n;
+        reinterpret_cast<double *>(p.C)[2 * (row + p.ldc * nn) + (im ? 1 : 0)] = (double)v;
+    }
+}
+
+// Persistent CTA (one per SM): walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (grouped order)
+//   warp 0 lane 0: TMA producer over the k-blocks of all its tiles (one continuous smem ring)
+//   warp 1 lane 0: MMA issuer into TMEM accumulator buffer (j & 1) for the CTA's j-th tile
+//   warps 2-5:     epilogue of tile j from buffer (j & 1) while the MMAs of tile j+1 run in the other buffer
 __global__ void __launch_bounds__(X_THREADS, 1)
     gemm_bf16x_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const XGemmArgs p) {
     extern __shared__ __align__(1024) unsigned char xsm_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(xsm_raw) + 1023) & ~uintptr_t(1023));
     uint64_t      *full      = reinterpret_cast<uint64_t *>(smem + X_STAGES * X_STAGE_BYTES);
     uint64_t      *empty     = full + X_STAGES;
-    uint64_t      *tmem_full = empty + X_STAGES;
-    uint32_t      *tmem_slot = reinterpret_cast<uint32_t *>(tmem_full + 1);
+    uint64_t      *acc_full  = empty + X_STAGES;  // [2]
+    uint64_t      *acc_empty = acc_full + 2;      // [2]
+    uint32_t      *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2);
+    int           *s_fail    = reinterpret_cast<int *>(tmem_slot + 1);  // an epilogue wait timed out
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int       tile_m, tile_n;
-    {
-        const int num_m = (p.M + X_BM - 1) / X_BM, num_n = (p.N + X_BN - 1) / X_BN;
-        const int pid = blockIdx.x, per_group = X_GROUP_M * num_n;
-        const int first_m = (pid / per_group) * X_GROUP_M;
-        const int gsize   = min(num_m - first_m, X_GROUP_M);
-        tile_m            = first_m + (pid % per_group) % gsize;
-        tile_n            = (pid % per_group) / gsize;
-    }
-    const int m0 = tile_m * X_BM, n0 = tile_n * X_BN;
-    const int KB = (p.K + X_BK - 1) / X_BK;
+    const int ntiles = ((p.M + X_BM - 1) / X_BM) * ((p.N + X_BN - 1) / X_BN);
+    const int KB     = (p.K + X_BK - 1) / X_BK;
 
     if(threadIdx.x == 0) {
         for(int s = 0; s < X_STAGES; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(tmem_full, 1);
+        for(int b = 0; b < 2; b++) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 128);
+        }
+        *s_fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if(warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)), "r"(X_BN) : "memory");
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)), "r"(2 * X_BN) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     tc_fence_before();
@@ -128,79 +158,93 @@ __global__ void __launch_bounds__(X_THREADS, 1)
     const uint32_t tmem_base = *tmem_slot;
 
     if(warp == 0) {
-        if(lane == 0) {
-            // TMA producer
-            for(int kb = 0; kb < KB; kb++) {
-                const int      st = kb % X_STAGES;
-                const uint32_t ph = (kb / X_STAGES) & 1;
-                if(!mbar_wait(&empty[st], ph ^ 1)) {
-                    atomicExch(p.err, 1);
-                    break;
+        if(lane == 0) {  // TMA producer
+            int  it = 0;
+            bool ok = true;
+            for(int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                int m0, n0;
+                x_tile_mn(p, t, m0, n0);
+                for(int kb = 0; kb < KB; kb++, it++) {
+                    const int      st = it % X_STAGES;
+                    const uint32_t ph = (it / X_STAGES) & 1;
+                    if(!mbar_wait(&empty[st], ph ^ 1)) {
+                        atomicExch(p.err, 1);
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *a = smem + st * X_STAGE_BYTES, *b = a + X_A_BYTES;
+                    mbar_expect_tx(&full[st], X_STAGE_BYTES);
+                    tma_load_2d(&tmA, &full[st], a, kb * X_BK, m0);
+                    tma_load_2d(&tmB, &full[st], b, kb * X_BK, n0);
                 }
-                unsigned char *a = smem + st * X_STAGE_BYTES, *b = a + X_A_BYTES;
-                mbar_expect_tx(&full[st], X_STAGE_BYTES);
-                tma_load_2d(&tmA, &full[st], a, kb * X_BK, m0);
-                tma_load_2d(&tmB, &full[st], b, kb * X_BK, n0);
             }
         }
     } else if(warp == 1) {
-        if(lane == 0) {
-            // MMA issuer
-            for(int kb = 0; kb < KB; kb++) {
-                const int      st = kb % X_STAGES;
-                const uint32_t ph = (kb / X_STAGES) & 1;
-                if(!mbar_wait(&full[st], ph)) {
-                    atomicExch(p.err, 2);
+        if(lane == 0) {  // MMA issuer
+            int  it = 0, j = 0;
+            bool ok = true;
+            for(int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, j++) {
+                const int      buf = j & 1;
+                const uint32_t acc = tmem_base + (uint32_t)(buf * X_BN);
+                if(!mbar_wait(&acc_empty[buf], ((j >> 1) & 1) ^ 1)) {  // the epilogue drained this buffer
+                    atomicExch(p.err, 4);
                     break;
                 }
                 tc_fence_after();
-                const uint32_t a = saddr(smem + st * X_STAGE_BYTES), b = a + X_A_BYTES;
+                for(int kb = 0; kb < KB; kb++, it++) {
+                    const int      st = it % X_STAGES;
+                    const uint32_t ph = (it / X_STAGES) & 1;
+                    if(!mbar_wait(&full[st], ph)) {
+                        atomicExch(p.err, 2);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a = saddr(smem + st * X_STAGE_BYTES), b = a + X_A_BYTES;
 #pragma unroll
-                for(int k = 0; k < X_BK / 16; k++) umma_bf16(tmem_base, sdesc_sw128(a + 32 * k), sdesc_sw128(b + 32 * k), (kb | k) != 0);
-                umma_commit(&empty[st]);
+                    for(int k = 0; k < X_BK / 16; k++) umma_bf16(acc, sdesc_sw128(a + 32 * k), sdesc_sw128(b + 32 * k), (kb | k) != 0);
+                    umma_commit(&empty[st]);
+                }
+                if(ok) umma_commit(&acc_full[buf]);  // fires when every MMA of this tile has completed
             }
-            umma_commit(tmem_full);  // fires when every MMA issued above has completed
         }
     } else {
         // epilogue: warps 2..5 -> TMEM lane quarters 2,3,0,1
-        const int  q   = warp & 3;
-        const int  row = m0 + q * 32 + lane;
-        const bool ok  = mbar_wait(tmem_full, 0);
-        if(!ok) atomicExch(p.err, 3);
-        tc_fence_after();
-        if(ok && KB > 0) {
+        const int q = warp & 3;
+        int       j = 0;
+        for(int t = blockIdx.x; t < ntiles; t += gridDim.x, j++) {
+            const int buf = j & 1;
+            int       m0, n0;
+            x_tile_mn(p, t, m0, n0);
+            if(!mbar_wait(&acc_full[buf], (j >> 1) & 1)) {
+                atomicExch(p.err, 3);
+                atomicOr(s_fail, 1);
+            }
+            epi_bar();  // every epilogue warp takes the same decision
+            if(*s_fail) break;
+            tc_fence_after();
+            const int row = m0 + q * 32 + lane;
             for(int c = 0; c < X_BN; c += 32) {
-                if(n0 + c >= p.N) break;
                 uint32_t r[32];
-                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)c, r);
+                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * X_BN + c), r);
                 if(row < p.M) {
 #pragma unroll
-                    for(int j = 0; j < 32; j++) {
-                        const int n = n0 + c + j;
-                        if(n < p.N) {
-                            const float v = __uint_as_float(r[j]);
-                            if(p.mode == X_OUT_F32)
-                                reinterpret_cast<float *>(p.C)[row + p.ldc * n] = v;
-                            else if(p.mode == X_OUT_F32_ACC)
-                                reinterpret_cast<float *>(p.C)[row + p.ldc * n] += v;
-                            else if(p.mode == X_OUT_F64)
-                                reinterpret_cast<double *>(p.C)[row + p.ldc * n] = (double)v;
-                            else {
-                                const bool im = n >= p.n_half;
-                                const int  nn = im ? n - p.n_half : n;
-                                reinterpret_cast<double *>(p.C)[2 * (row + p.ldc * nn) + (im ? 1 : 0)] = (double)v;
-                            }
-                        }
+                    for(int jj = 0; jj < 32; jj++) {
+                        const int n = n0 + c + jj;
+                        if(n < p.N) x_store(p, row, n, __uint_as_float(r[jj]));
                     }
                 }
             }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[buf]);  // TMEM buffer free for the tile after next
+            epi_bar();                     // *s_fail is read by all before the next wait may set it
         }
     }
     tc_fence_before();
     __syncthreads();
     if(warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(X_BN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(2 * X_BN) : "memory");
     }
 }
 
@@ -252,7 +296,8 @@ int gemm_bf16x(const CUtensorMap &tmA, const CUtensorMap &tmB, const XGemmArgs &
     }
     const int64_t tiles = cdiv(a.M, X_BM) * cdiv(a.N, X_BN);
     if(tiles > 0x7fffffff) return HEFF_BAD_SHAPE;
-    gemm_bf16x_kernel<<<(unsigned)tiles, X_THREADS, X_SMEM_BYTES, s>>>(tmA, tmB, a);
+    const int grid = (int)std::min<int64_t>(tiles, device_sm_count());  // persistent: one CTA per SM
+    gemm_bf16x_kernel<<<(unsigned)grid, X_THREADS, X_SMEM_BYTES, s>>>(tmA, tmB, a);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }

@@ -8,9 +8,10 @@
 // B' = [b_hi | b_mid | b_hi] gives a_hi b_hi + a_hi b_mid + a_mid b_hi in one GEMM).
 //
 // CTA: 192 threads = warp 0 TMA producer, warp 1 TMEM allocator + MMA issuer, warps 2-5 epilogue
-// (tcgen05.ld 32x32b: warp w reads TMEM lanes 32*(w%4) .. +31).  Tile 128 x 256 x 64, one tile per
-// CTA.  Every mbarrier wait is bounded: on timeout the kernel raises *err, skips its remaining work,
-// still frees its TMEM and returns.  No cluster multicast anywhere.
+// (tcgen05.ld 32x32b: warp w reads TMEM lanes 32*(w%4) .. +31).  Tile 128 x 256 x 64.  Persistent: one CTA
+// per SM walks its share of the tiles with two TMEM accumulators (512 columns), so the epilogue of a tile
+// overlaps the MMAs of the next.  Every mbarrier wait is bounded: on timeout the kernel raises *err, skips its
+// remaining work, still frees its TMEM and returns.  No cluster multicast anywhere.
 #pragma once
 #include <cuda.h>
 

@@ -270,6 +270,7 @@ static int mixed_setup(heff_op *op) {
     HEFF_TRY(make_tmap_bf16(&m->tB1, m->B1, cf * m->N1, m->Kx1, m->Kx1, X_BN));
     HEFF_TRY(make_tmap_bf16(&m->tA2, m->A2, m->M2, m->Kx2, m->Kx2, X_BM));
     HEFF_TRY(make_tmap_bf16(&m->tB2, m->B2, cf * m->N2, m->Kx2, m->Kx2, X_BN));
+
     const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS +
                             wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
     if(mix_smem > 200 * 1024) return HEFF_BAD_SHAPE;

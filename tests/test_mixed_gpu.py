@@ -21,7 +21,10 @@ from conftest import relerr
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (128, 256, 512), (200, 300, 136), (1000, 700, 1024), (64, 40, 8)])
+# (1536, 4096, 2048): 192 tiles on 148 SMs -> one whole wave and 44 tiles split in K (several units per CTA, both
+# TMEM accumulators, the ordered reduction of partial tiles); (1100, 3000, 4000): split tiles with ragged M, N, K edges
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (128, 256, 512), (200, 300, 136), (1000, 700, 1024), (64, 40, 8), (1536, 4096, 2048),
+                                   (1100, 3000, 4000)])
 def test_bf16_gemm_vs_fp64(cuda, M, N, K):
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
     A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16).contiguous()
