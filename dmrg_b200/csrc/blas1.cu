@@ -341,11 +341,169 @@ __global__ void orth_axpy_kernel(const T *__restrict__ V, int64_t ldv, int64_t n
     }
 }
 
+// ---- Fast path of orth_cgs2 for k <= 24 and 16-byte rows (real: two rows per double2; complex: one element).
+// Every thread first loads its row of all k basis columns (16-byte loads, all in flight together), then does
+// the arithmetic: the loads-first order and the 16-byte width are what bring these HBM-bound passes near the
+// copy bandwidth.  Three modes, each ending in the same deterministic last-block reduction as orth_dot_kernel:
+//   MODE 0: h1 = V^H w, ||w||^2                                    (decides the second pass, as orth_dot pass 0)
+//   MODE 1: v = (w - V h1) s1 with s1 = 1/beta1 unless a second pass follows; in the same sweep over V,
+//           h2 = V^H v and ||v||^2 (used only when the second pass runs)
+//   MODE 2: v = (v - V h2) / beta  (launched always, returns at once unless the second pass is needed)
+template<bool CPLX, int KM, int MODE>
+__global__ void __launch_bounds__(256, 1) orth_fast_kernel(const double2 *V, int64_t ldu, int64_t nu, int k, const double2 *in, double2 *out,
+                                                           double *__restrict__ partials, unsigned *__restrict__ counter, double *__restrict__ st,
+                                                           typename Scalar<CPLX>::T *__restrict__ hres) {
+    using T = typename Scalar<CPLX>::T;
+    if(MODE == 2 && st[1] == 0.0) return;  // uniform over the grid
+    __shared__ double sre[8][KM + 1], sim[8][KM + 1];
+    __shared__ double shr[KM], shi[KM];
+    __shared__ bool   s_last;
+    const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nb = gridDim.x;
+    if(MODE != 0) {
+        const double *h = st + (MODE == 1 ? ORTH_H1 : ORTH_H2);
+        for(int j = threadIdx.x; j < KM; j += blockDim.x) {
+            shr[j] = j < k ? h[2 * j] : 0.0;
+            shi[j] = j < k ? h[2 * j + 1] : 0.0;
+        }
+    }
+    double scale = 1.0;
+    if(MODE == 1) scale = st[1] != 0.0 ? 1.0 : (st[3] > 1e-300 ? 1.0 / sqrt(st[3]) : 0.0);
+    if(MODE == 2) scale = st[3] > 1e-300 ? 1.0 / sqrt(st[3]) : 0.0;
+    __syncthreads();
+    double are[KM + 1], aim[KM + 1];
+#pragma unroll
+    for(int j = 0; j <= KM; j++) are[j] = aim[j] = 0.0;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nu; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 v[KM];
+#pragma unroll
+        for(int j = 0; j < KM; j++) v[j] = V[i + ldu * (j < k ? j : 0)];
+        double2 r = in[i];
+        if(MODE != 0) {
+            double ax = 0, ay = 0;
+#pragma unroll
+            for(int j = 0; j < KM; j++) {
+                if constexpr(CPLX) {
+                    ax = fma(v[j].x, shr[j], fma(-v[j].y, shi[j], ax));
+                    ay = fma(v[j].x, shi[j], fma(v[j].y, shr[j], ay));
+                } else {
+                    ax = fma(v[j].x, shr[j], ax);
+                    ay = fma(v[j].y, shr[j], ay);
+                }
+            }
+            r = make_double2((r.x - ax) * scale, (r.y - ay) * scale);
+            out[i] = r;
+        }
+        if(MODE != 2) {
+#pragma unroll
+            for(int j = 0; j < KM; j++)
+                if(j < k) {
+                    if constexpr(CPLX) {
+                        are[j] = fma(v[j].x, r.x, fma(v[j].y, r.y, are[j]));  // conj(v) r
+                        aim[j] = fma(v[j].x, r.y, fma(-v[j].y, r.x, aim[j]));
+                    } else {
+                        are[j] = fma(v[j].x, r.x, fma(v[j].y, r.y, are[j]));
+                    }
+                }
+            are[KM] = fma(r.x, r.x, fma(r.y, r.y, are[KM]));
+        }
+    }
+    if(MODE == 2) return;
+    // block partial sums (column j < k, and the norm in slot k), fixed order
+#pragma unroll
+    for(int j = 0; j <= KM; j++) {
+        double a = are[j], b = aim[j];
+        for(int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            if(CPLX) b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if(lane == 0) sre[warp][j] = a, sim[warp][j] = b;
+    }
+    __syncthreads();
+    for(int j = threadIdx.x; j <= k; j += blockDim.x) {
+        const int src = j < k ? j : KM;
+        double    a = 0, b = 0;
+        for(int w = 0; w < 8; w++) a += sre[w][src], b += sim[w][src];
+        partials[((int64_t)j * nb + blockIdx.x) * 2 + 0] = a;
+        partials[((int64_t)j * nb + blockIdx.x) * 2 + 1] = b;
+    }
+    __threadfence();
+    __syncthreads();
+    if(threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == (unsigned)(nb - 1);
+    __syncthreads();
+    if(!s_last) return;
+    __threadfence();
+    double *h = st + (MODE == 0 ? ORTH_H1 : ORTH_H2);
+    for(int j = warp; j <= k; j += 8) {
+        double a = 0, b = 0;
+        for(int blk = lane; blk < nb; blk += 32) {
+            a += __ldcg(&partials[((int64_t)j * nb + blk) * 2 + 0]);
+            b += __ldcg(&partials[((int64_t)j * nb + blk) * 2 + 1]);
+        }
+        for(int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if(lane == 0) h[2 * j] = a, h[2 * j + 1] = CPLX ? b : 0.0;
+    }
+    __syncthreads();
+    const bool second = MODE == 1 && st[1] != 0.0;
+    if(threadIdx.x == 0) {
+        double hn2 = 0;
+        for(int j = 0; j < k; j++) hn2 += h[2 * j] * h[2 * j] + h[2 * j + 1] * h[2 * j + 1];
+        const double nrm2 = h[2 * k];
+        if(MODE == 0) {
+            st[0] = nrm2;
+            st[3] = nrm2 - hn2;
+            st[1] = (nrm2 - hn2 > 0.5 * nrm2) ? 0.0 : 1.0;  // severe cancellation: orthogonalise again
+        } else if(second) {
+            st[2] = nrm2;
+            st[3] = nrm2 - hn2;
+        }
+        *counter = 0u;
+    }
+    __syncthreads();
+    if(MODE == 0 || second) {
+        for(int j = threadIdx.x; j < k; j += blockDim.x) {
+            double re = st[ORTH_H1 + 2 * j], im = st[ORTH_H1 + 2 * j + 1];
+            if(second) re += st[ORTH_H2 + 2 * j], im += st[ORTH_H2 + 2 * j + 1];
+            hres[j] = orth_make<T>(re, im);
+        }
+        if(threadIdx.x == 0) {
+            hres[k]     = orth_make<T>(sqrt(fmax(st[3], 0.0)), 0.0);
+            hres[k + 1] = orth_make<T>(st[0], st[1]);
+        }
+    }
+}
+
+template<bool CPLX, int KM>
+static int orth_fast(const double2 *V, int64_t ldu, int64_t nu, int k, const double2 *w, double2 *v, double *partials, unsigned *counter, double *st,
+                     typename Scalar<CPLX>::T *hres, cudaStream_t s) {
+    const int nb = (int)std::min<int64_t>(std::min<int64_t>(MD_BLOCKS, 4 * (int64_t)device_sm_count()), std::max<int64_t>(1, (nu + 255) / 256));
+    orth_fast_kernel<CPLX, KM, 0><<<nb, 256, 0, s>>>(V, ldu, nu, k, w, nullptr, partials, counter, st, hres);
+    HEFF_LAUNCH_CHECK();
+    orth_fast_kernel<CPLX, KM, 1><<<nb, 256, 0, s>>>(V, ldu, nu, k, w, v, partials, counter, st, hres);
+    HEFF_LAUNCH_CHECK();
+    orth_fast_kernel<CPLX, KM, 2><<<nb, 256, 0, s>>>(V, ldu, nu, k, v, v, partials, counter, st, hres);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
 template<bool CPLX>
 int orth_cgs2(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *w, typename Scalar<CPLX>::T *v,
               double *partials, unsigned *counter, double *st, typename Scalar<CPLX>::T *hres, cudaStream_t s) {
     using T = typename Scalar<CPLX>::T;
     if(k <= 0 || k + 1 > 2 * MD_MAXK || k > MD_MAXK) return HEFF_BAD_ARG;
+    // fast path: 16-byte rows (complex always; real when the rows pair up on 16-byte boundaries)
+    const bool rows16 = CPLX || (n % 2 == 0 && ldv % 2 == 0 && ((uintptr_t)V & 15) == 0 && ((uintptr_t)w & 15) == 0 && ((uintptr_t)v & 15) == 0);
+    if(k <= 24 && rows16) {
+        const double2 *V2  = reinterpret_cast<const double2 *>(V);
+        const int64_t  ldu = CPLX ? ldv : ldv / 2, nu = CPLX ? n : n / 2;
+        const double2 *w2  = reinterpret_cast<const double2 *>(w);
+        double2       *v2  = reinterpret_cast<double2 *>(v);
+        if(k <= 8) return orth_fast<CPLX, 8>(V2, ldu, nu, k, w2, v2, partials, counter, st, hres, s);
+        if(k <= 16) return orth_fast<CPLX, 16>(V2, ldu, nu, k, w2, v2, partials, counter, st, hres, s);
+        return orth_fast<CPLX, 24>(V2, ldu, nu, k, w2, v2, partials, counter, st, hres, s);
+    }
     const int nb = (int)std::min<int64_t>(std::min<int64_t>(MD_BLOCKS, 4 * (int64_t)device_sm_count()), std::max<int64_t>(1, (n + 255) / 256));
     orth_dot_kernel<T><<<nb, 256, 0, s>>>(V, ldv, n, k, w, partials, counter, st, hres, 0);
     HEFF_LAUNCH_CHECK();
