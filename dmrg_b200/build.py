@@ -5,6 +5,7 @@ into ``_build/`` and linked into one shared library with the CUDA runtime
 linked statically, so the library needs nothing but the NVIDIA driver at run time.
 """
 import concurrent.futures as cf
+import hashlib
 import os
 import subprocess
 import sys
@@ -23,17 +24,30 @@ def _sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
-def _headers_mtime():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
+def _headers_digest():
+    hs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h")))
     hs.append(os.path.join(HERE, "..", "include", "heff.h"))
-    return max(os.path.getmtime(h) for h in hs if os.path.exists(h))
+    h = hashlib.sha1()
+    for p in hs:
+        if os.path.exists(p):
+            with open(p, "rb") as f:
+                h.update(f.read())
+    return h.hexdigest()
 
 
 def _compile(src, verbose_ptxas=False):
+    """Compile one source unless its object was built from identical source, headers and flags (content hash:
+    file times can miss an edit made within the same timestamp tick)."""
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    hdr = _headers_mtime()
-    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr):
-        return obj, ""
+    h = hashlib.sha1()
+    with open(src, "rb") as f:
+        h.update(f.read())
+    h.update(_headers_digest().encode())
+    h.update(" ".join(ARCH + COMMON).encode())
+    digest = h.hexdigest()
+    stamp = obj + ".sha1"
+    if os.path.exists(obj) and os.path.exists(stamp) and open(stamp).read() == digest:
+        return obj, None  # up to date
     cmd = [NVCC] + ARCH + COMMON + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [NVCC] + COMMON + ["-x", "cu"] + ARCH + ["-c", src, "-o", obj]
@@ -42,6 +56,8 @@ def _compile(src, verbose_ptxas=False):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    with open(stamp, "w") as f:
+        f.write(digest)
     return obj, r.stderr
 
 
@@ -57,7 +73,7 @@ def build(verbose=False, jobs=None):
         for _, log in results:
             if log:
                 sys.stderr.write(log)
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+    if not os.path.exists(LIB) or any(log is not None for _, log in results):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lcuda"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -1,5 +1,6 @@
 // H_eff * theta: layout kernels, MPO mixing kernel, matvec driver, expectation value,
 // and the stateless C entry points heff_matvec_{d,z} / heff_expval_{d,z}.
+#include <algorithm>
 #include "matvec.cuh"
 #include "runtime.cuh"
 #include "wlist.cuh"
@@ -39,6 +40,15 @@ __global__ void permute_mps_kernel(const T *__restrict__ x, T *__restrict__ xp, 
     }
 }
 
+// x'[o] for o in [o0, o1) (the x' columns (s,b) of a slab of b)
+template<class T>
+__global__ void permute_mps_range_kernel(const T *__restrict__ x, T *__restrict__ xp, int64_t S, int64_t cL, int64_t o0, int64_t o1) {
+    for(int64_t o = o0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < o1; o += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = o % cL, r = o / cL, s = r % S, b = r / S;
+        xp[o]           = x[s + S * (a + cL * b)];
+    }
+}
+
 // R'[b + cR*n + cR*DR*b'] = R[b + cR*(b' + cR*n)]
 template<class T>
 __global__ void permute_R_kernel(const T *__restrict__ R, T *__restrict__ Rp, int64_t cR, int64_t DR, int64_t n) {
@@ -63,14 +73,14 @@ __device__ __forceinline__ void zero(double2 &v) { v = make_double2(0.0, 0.0); }
 constexpr int MIX_THREADS = 128;
 template<class T>
 __global__ void __launch_bounds__(MIX_THREADS) mix_kernel(const T *__restrict__ T1, T *__restrict__ T2, const T *__restrict__ W, int S, int cL,
-                                                         int cR, int DL, int DR) {
+                                                         int cR, int DL, int DR, int b0) {
     extern __shared__ __align__(16) unsigned char mix_smem[];
     T        *sW  = reinterpret_cast<T *>(mix_smem);
     const int nW  = DL * DR * S * S;
     T        *sIn = sW + nW;
     unsigned char *lmem = reinterpret_cast<unsigned char *>(sIn + (size_t)DL * S * MIX_THREADS);
     for(int i = threadIdx.x; i < nW; i += blockDim.x) sW[i] = W[i];
-    const int     b   = blockIdx.y;
+    const int     b   = b0 + blockIdx.y;  // columns b0 .. b0 + gridDim.y - 1
     const int     ap  = blockIdx.x * MIX_THREADS + threadIdx.x;
     const bool    act = ap < cL;
     const int64_t cLD = (int64_t)cL * DL;
@@ -115,7 +125,7 @@ int permute_R(const typename Scalar<CPLX>::T *R, typename Scalar<CPLX>::T *Rp, c
 
 template<bool CPLX>
 static int launch_mix(const MatvecDims &d, const typename Scalar<CPLX>::T *T1, typename Scalar<CPLX>::T *T2, const typename Scalar<CPLX>::T *W,
-                      cudaStream_t s) {
+                      cudaStream_t s, int64_t b0 = 0, int64_t nb = -1) {
     using T           = typename Scalar<CPLX>::T;
     const size_t smem = sizeof(T) * ((size_t)d.DL * d.DR * d.S * d.S + (size_t)d.DL * d.S * MIX_THREADS) +
                         wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
@@ -127,9 +137,11 @@ static int launch_mix(const MatvecDims &d, const typename Scalar<CPLX>::T *T1, t
         HEFF_CUDA(cudaFuncSetAttribute(mix_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         if(dev >= 0 && dev < 64) attr_done[dev] = 1;
     }
-    if(d.cR > 65535) return HEFF_BAD_SHAPE;
-    dim3 grid((unsigned)cdiv(d.cL, MIX_THREADS), (unsigned)d.cR);
-    mix_kernel<T><<<grid, MIX_THREADS, smem, s>>>(T1, T2, W, (int)d.S, (int)d.cL, (int)d.cR, (int)d.DL, (int)d.DR);
+    if(nb < 0) nb = d.cR;
+    if(nb > 65535) return HEFF_BAD_SHAPE;
+    if(nb == 0) return HEFF_OK;
+    dim3 grid((unsigned)cdiv(d.cL, MIX_THREADS), (unsigned)nb);
+    mix_kernel<T><<<grid, MIX_THREADS, smem, s>>>(T1, T2, W, (int)d.S, (int)d.cL, (int)d.cR, (int)d.DL, (int)d.DR, (int)b0);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }
@@ -202,6 +214,72 @@ int matvec_left_stages(const MatvecDims &d, const typename Scalar<CPLX>::T *x, c
     g1.beta  = make_double2(0.0, 0.0);
     HEFF_TRY(gemm_f64<CPLX>(/*ta=*/true, /*tb=*/false, false, g1, s));
     return launch_mix<CPLX>(d, T1, out, W, s);
+}
+
+// y = H_eff x with x and y in HOST memory, copies overlapped with the computation.  The slab of theta with
+// columns b in [b0, b1) is contiguous (theta[s + S(a + cL b)]), and GEMM 1 and the mix of that slab need
+// nothing else: slab c is copied in on the copy stream and processed on compute stream c % 2 as soon as it
+// has landed.  GEMM 2's output columns b' are independent: slab c' of y is computed on stream c' % 2 once
+// every mix is done and copied out right after.  Two compute streams let a slab's GEMM fill the tail wave of
+// the previous one.  Synchronises before returning.
+template<bool CPLX>
+int matvec_fp64_host(const MatvecDims &d, const typename Scalar<CPLX>::T *xh, typename Scalar<CPLX>::T *yh, const typename Scalar<CPLX>::T *L,
+                     const typename Scalar<CPLX>::T *Rp, const typename Scalar<CPLX>::T *W, const MatvecScratch<CPLX> &ws, typename Scalar<CPLX>::T *dx,
+                     typename Scalar<CPLX>::T *dy, const HostPipe &hp) {
+    using T               = typename Scalar<CPLX>::T;
+    const int         nin = (int)std::min<int64_t>(hp.n_in, d.cR), nout = (int)std::min<int64_t>(hp.n_out, d.cR);
+    cudaStream_t      cs[2] = {hp.s, hp.aux};
+    const int64_t     colx = d.S * d.cL;  // elements per b column of theta / y
+    auto              slab = [&](int c, int nc, int64_t &b0, int64_t &b1) {
+        b0 = d.cR * c / nc;
+        b1 = d.cR * (c + 1) / nc;
+    };
+    // everything queued on the caller's stream before this call precedes the copies into dx
+    HEFF_CUDA(cudaEventRecord(hp.ev[0], hp.s));
+    HEFF_CUDA(cudaStreamWaitEvent(hp.copy, hp.ev[0], 0));
+    HEFF_CUDA(cudaStreamWaitEvent(hp.aux, hp.ev[0], 0));
+    for(int c = 0; c < nin; c++) {
+        int64_t b0, b1;
+        slab(c, nin, b0, b1);
+        if(b1 == b0) continue;
+        HEFF_CUDA(cudaMemcpyAsync(dx + colx * b0, xh + colx * b0, sizeof(T) * colx * (b1 - b0), cudaMemcpyHostToDevice, hp.copy));
+        HEFF_CUDA(cudaEventRecord(hp.ev[1 + c], hp.copy));
+        cudaStream_t s = cs[c & 1];
+        HEFF_CUDA(cudaStreamWaitEvent(s, hp.ev[1 + c], 0));
+        const int64_t o0 = d.cL * d.S * b0, o1 = d.cL * d.S * b1;
+        permute_mps_range_kernel<<<grid_1d(o1 - o0), 256, 0, s>>>(dx, ws.xp, d.S, d.cL, o0, o1);
+        HEFF_LAUNCH_CHECK();
+        GemmArgs g1{};
+        g1.M = (int)(d.cL * d.DL), g1.N = (int)(d.S * (b1 - b0)), g1.K = (int)d.cL, g1.batch = 1;
+        g1.A = L, g1.lda = d.cL, g1.B = ws.xp + o0, g1.ldb = d.cL, g1.C = ws.T1 + d.cL * d.DL * d.S * b0, g1.ldc = d.cL * d.DL;
+        g1.alpha = make_double2(1.0, 0.0), g1.beta = make_double2(0.0, 0.0);
+        HEFF_TRY(gemm_f64<CPLX>(/*ta=*/true, /*tb=*/false, false, g1, s));
+        HEFF_TRY(launch_mix<CPLX>(d, ws.T1, ws.T2, W, s, b0, b1 - b0));
+    }
+    // every mix (both streams) before any GEMM 2 slab
+    HEFF_CUDA(cudaEventRecord(hp.ev[HostPipe::MAXS + 1], hp.aux));
+    HEFF_CUDA(cudaStreamWaitEvent(hp.s, hp.ev[HostPipe::MAXS + 1], 0));
+    HEFF_CUDA(cudaEventRecord(hp.ev[HostPipe::MAXS + 2], hp.s));
+    HEFF_CUDA(cudaStreamWaitEvent(hp.aux, hp.ev[HostPipe::MAXS + 2], 0));
+    for(int c = 0; c < nout; c++) {
+        int64_t b0, b1;
+        slab(c, nout, b0, b1);
+        if(b1 == b0) continue;
+        cudaStream_t s = cs[c & 1];
+        GemmArgs     g2{};
+        g2.M = (int)(d.S * d.cL), g2.N = (int)(b1 - b0), g2.K = (int)(d.cR * d.DR), g2.batch = 1;
+        g2.A = ws.T2, g2.lda = d.S * d.cL, g2.B = Rp + d.cR * d.DR * b0, g2.ldb = d.cR * d.DR, g2.C = dy + colx * b0, g2.ldc = d.S * d.cL;
+        g2.alpha = make_double2(1.0, 0.0), g2.beta = make_double2(0.0, 0.0);
+        HEFF_TRY(gemm_f64<CPLX>(false, false, false, g2, s));
+        HEFF_CUDA(cudaEventRecord(hp.ev[HostPipe::MAXS + 3 + c], s));
+        HEFF_CUDA(cudaStreamWaitEvent(hp.copy, hp.ev[HostPipe::MAXS + 3 + c], 0));
+        HEFF_CUDA(cudaMemcpyAsync(yh + colx * b0, dy + colx * b0, sizeof(T) * colx * (b1 - b0), cudaMemcpyDeviceToHost, hp.copy));
+    }
+    // the caller's stream resumes after the last copy out; the host waits for it
+    HEFF_CUDA(cudaEventRecord(hp.ev[2 * HostPipe::MAXS + 3], hp.copy));
+    HEFF_CUDA(cudaStreamWaitEvent(hp.s, hp.ev[2 * HostPipe::MAXS + 3], 0));
+    HEFF_CUDA(cudaStreamSynchronize(hp.s));
+    return HEFF_OK;
 }
 
 // ---- deterministic dot product ----
@@ -282,6 +360,10 @@ template int matvec_left_stages<false>(const MatvecDims &, const double *, const
                                        cudaStream_t);
 template int matvec_left_stages<true>(const MatvecDims &, const double2 *, const double2 *, const double2 *, double2 *, double2 *, double2 *, double,
                                       cudaStream_t);
+template int matvec_fp64_host<false>(const MatvecDims &, const double *, double *, const double *, const double *, const double *,
+                                     const MatvecScratch<false> &, double *, double *, const HostPipe &);
+template int matvec_fp64_host<true>(const MatvecDims &, const double2 *, double2 *, const double2 *, const double2 *, const double2 *,
+                                    const MatvecScratch<true> &, double2 *, double2 *, const HostPipe &);
 template int dot_device<false>(const double *, const double *, int64_t, double *, double *, cudaStream_t);
 template int dot_device<true>(const double2 *, const double2 *, int64_t, double2 *, double *, cudaStream_t);
 

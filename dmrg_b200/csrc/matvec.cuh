@@ -43,6 +43,14 @@ struct MatvecScratch {
     }
 };
 
+// Streams and events of the host-buffer matvec pipeline (matvec_fp64_host), owned by the operator.
+struct HostPipe {
+    static constexpr int MAXS = 16;  // slabs per side at most
+    cudaStream_t         s = nullptr, aux = nullptr, copy = nullptr;
+    cudaEvent_t          ev[2 * MAXS + 4] = {};
+    int                  n_in = 8, n_out = 8;  // measured at chi=1024 complex: 4/4 27.2, 8/8 29.0, 16/8 29.2 TFLOP/s end to end
+};
+
 // y = H_eff x with pre-permuted R'.  L and W in reference layout.  Launches 4 kernels on s.
 // ev (optional): 5 events recorded before P and after P, G1, MIX, G2 (stage timing).
 template<bool CPLX>
@@ -59,5 +67,12 @@ int dot_device(const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T
 template<bool CPLX>
 int matvec_left_stages(const MatvecDims &d, const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T *L, const typename Scalar<CPLX>::T *W,
                        typename Scalar<CPLX>::T *out, typename Scalar<CPLX>::T *xp, typename Scalar<CPLX>::T *T1, double alpha, cudaStream_t s);
+
+// y = H_eff x with x, y in host memory: slabbed copies overlapped with GEMM 1 / mix and GEMM 2 (dx, dy device
+// staging of the full vectors).  Synchronises hp.s before returning.
+template<bool CPLX>
+int matvec_fp64_host(const MatvecDims &d, const typename Scalar<CPLX>::T *xh, typename Scalar<CPLX>::T *yh, const typename Scalar<CPLX>::T *L,
+                     const typename Scalar<CPLX>::T *Rp, const typename Scalar<CPLX>::T *W, const MatvecScratch<CPLX> &ws, typename Scalar<CPLX>::T *dx,
+                     typename Scalar<CPLX>::T *dy, const HostPipe &hp);
 
 }  // namespace heff

@@ -381,6 +381,13 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->eig_ws) cudaFree(op->eig_ws);
     if(op->Rtmp) cudaFree(op->Rtmp);
     for(void *p : op->seq_W) cudaFree(p);
+    if(op->pipe) {
+        if(op->pipe->aux) cudaStreamDestroy(op->pipe->aux);
+        if(op->pipe->copy) cudaStreamDestroy(op->pipe->copy);
+        for(cudaEvent_t e : op->pipe->ev)
+            if(e) cudaEventDestroy(e);
+        delete op->pipe;
+    }
     if(op->diag) cudaFree(op->diag);
     if(op->eig_host) cudaFreeHost(op->eig_host);
     if(op->eig_event) cudaEventDestroy(op->eig_event);
@@ -414,15 +421,45 @@ extern "C" int heff_op_multax_block(heff_op *op, const void *x, int64_t ldx, voi
     return HEFF_OK;
 }
 
+// Host-buffer matvec with the copies overlapped (matvec_fp64_host): FP64 operators of at least 8 MB per vector.
+template<bool CPLX>
+static int multax_host_pipelined(heff_op *op, const void *x_host, void *y_host, void *dx, void *dy) {
+    using T = typename Scalar<CPLX>::T;
+    if(!op->pipe) {
+        HostPipe *hp = new HostPipe();
+        op->pipe     = hp;
+        HEFF_CUDA(cudaStreamCreateWithFlags(&hp->aux, cudaStreamNonBlocking));
+        HEFF_CUDA(cudaStreamCreateWithFlags(&hp->copy, cudaStreamNonBlocking));
+        for(cudaEvent_t &e : hp->ev) HEFF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    op->pipe->s = op->stream;
+    MatvecScratch<CPLX> ws;
+    ws.carve(reinterpret_cast<T *>(op->scratch), op->d);
+    HEFF_TRY(matvec_fp64_host<CPLX>(op->d, reinterpret_cast<const T *>(x_host), reinterpret_cast<T *>(y_host), reinterpret_cast<const T *>(op->L),
+                                    reinterpret_cast<const T *>(op->Rp), reinterpret_cast<const T *>(op->W), ws, reinterpret_cast<T *>(dx),
+                                    reinterpret_cast<T *>(dy), *op->pipe));
+    op->num_mv++;
+    return HEFF_OK;
+}
+
 extern "C" int heff_op_multax_host(heff_op *op, const void *x_host, void *y_host) {
     if(!op || !x_host || !y_host) return HEFF_BAD_ARG;
     const int64_t n     = op->d.size_mps();
     const size_t  bytes = (size_t)n * (op->cplx ? 16 : 8);
-    if(!op->stage_x) {
+    if(op->stage_bytes < 2 * bytes + 256) {  // grown for a rebind to larger dimensions
+        if(op->stage_x) {
+            HEFF_CUDA(cudaStreamSynchronize(op->stream));
+            cudaFree(op->stage_x);
+            op->stage_x     = nullptr;
+            op->stage_bytes = 0;
+        }
         HEFF_CUDA(cudaMalloc(&op->stage_x, 2 * bytes + 256));
+        op->stage_bytes = 2 * bytes + 256;
     }
     void *dx = op->stage_x;
     void *dy = reinterpret_cast<char *>(op->stage_x) + ((bytes + 255) / 256) * 256;
+    if(op->precision == HEFF_PREC_FP64 && !op->sequential && bytes >= ((size_t)8 << 20))
+        return op->cplx ? multax_host_pipelined<true>(op, x_host, y_host, dx, dy) : multax_host_pipelined<false>(op, x_host, y_host, dx, dy);
     HEFF_CUDA(cudaMemcpyAsync(dx, x_host, bytes, cudaMemcpyHostToDevice, op->stream));
     HEFF_TRY(op_apply(op, dx, dy));
     HEFF_CUDA(cudaMemcpyAsync(y_host, dy, bytes, cudaMemcpyDeviceToHost, op->stream));

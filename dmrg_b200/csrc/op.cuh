@@ -20,6 +20,8 @@ struct heff_op {
     void              *scratch       = nullptr;                    // x' | T1 | T2
     size_t             scratch_bytes = 0;
     void              *stage_x       = nullptr;  // device staging for MultAx with host buffers
+    size_t             stage_bytes   = 0;
+    heff::HostPipe    *pipe          = nullptr;  // streams/events of the overlapped host-buffer matvec (created on first use)
     int64_t            num_mv        = 0;
     // fixed-capacity operators (op_create_capacity / op_rebind): element capacities, R staging, host MPO copy
     int64_t            cap_env = 0, cap_W = 0, cap_scratch = 0;

@@ -152,3 +152,28 @@ def test_matvec_rejects_bad_shapes(cuda):
     hb.matrix_vector_product(res, d[0], th.shape, d[1], W.shape, d[2], L.shape, d[3], R.shape)
     torch.cuda.synchronize()
     assert relerr(hb.to_host(res, th.shape), oracle.matvec(th, W, L, R)) < TOL
+
+
+@pytest.mark.parametrize("chiL,chiR,c", [(512, 512, False), (400, 371, True), (1400, 200, False)])
+def test_host_buffer_matvec_overlapped_path(cuda, chiL, chiR, c):
+    """MultAx with host buffers of >= 8 MB takes the overlapped path (slabbed copies on a copy stream, two compute
+    streams): bit-identical to the device-pointer MultAx, with pageable and pinned buffers, call after call."""
+    th, W, L, R = ph.heff_inputs(chiL, D=3, cplx=c, seed=chiL + chiR, chiR=chiR)
+    assert th.nbytes >= 8 << 20
+    op = hb.MatVecMPOS([W], L, R, cplx=c)
+    x = hb.to_device(th)
+    y = torch.empty_like(x)
+    op.MultAx(x, y)
+    torch.cuda.synchronize()
+    y_dev = y.cpu().numpy()
+    for _ in range(2):
+        y_host = op.MultAx_host(th).ravel(order="F")
+        assert np.array_equal(y_host, y_dev)
+        op.MultAx(x, y)  # interleaved device-pointer call on the same operator
+    # pinned buffers through the C ABI
+    xp = torch.from_numpy(np.ascontiguousarray(th.ravel(order="F"))).pin_memory()
+    yp = torch.empty_like(xp).pin_memory()
+    hb.check(hb.lib().heff_op_multax_host(op.handle, hb.ptr(xp), hb.ptr(yp)), "multax_host")
+    assert np.array_equal(yp.numpy(), y_dev)
+    assert relerr(y_dev.reshape(th.shape, order="F"), rn.matvec_blas(th, W, L, R)) < TOL
+    op.close()
