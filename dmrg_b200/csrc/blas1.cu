@@ -516,12 +516,171 @@ int orth_cgs2(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, 
     return HEFF_OK;
 }
 
+// ---- Device-side CG for the Jacobi-Davidson correction equation ------------------------------------------------
+//   (I - u u^H)(H - theta)(I - u u^H) d = -r0,   r0 and the iterates orthogonal to u (u normalised).
+// All scalars live in cs[] on the device, so an iteration needs no host round trip; once CG stops (converged,
+// or an indefinite direction) cs[CG_DONE] turns the remaining kernels into no-ops.  Reductions: per-block
+// partial sums, then the last block to finish sums them in block order (deterministic).
+enum { CG_RHO = 0, CG_RHO0, CG_ALPHA, CG_BETA, CG_CRE, CG_CIM, CG_DONE, CG_TOL2, CG_THETA, CG_SIZE };
+
+// Fixed-order reduction of NV per-thread doubles over the grid; true in the last block, with the sums in out[].
+template<int NV>
+__device__ bool grid_reduce_last(double (&v)[NV], double *__restrict__ partials, unsigned *__restrict__ counter, double (&out)[NV]) {
+    __shared__ double sred[8][NV];
+    __shared__ double sout[NV];
+    __shared__ bool   s_last;
+    const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nb = gridDim.x;
+#pragma unroll
+    for(int j = 0; j < NV; j++) {
+        double a = v[j];
+        for(int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if(lane == 0) sred[warp][j] = a;
+    }
+    __syncthreads();
+    if(threadIdx.x < NV) {
+        double a = 0;
+        for(int w = 0; w < (int)(blockDim.x >> 5); w++) a += sred[w][threadIdx.x];
+        partials[(int64_t)threadIdx.x * nb + blockIdx.x] = a;
+    }
+    __threadfence();
+    __syncthreads();
+    if(threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == (unsigned)(nb - 1);
+    __syncthreads();
+    if(!s_last) return false;
+    __threadfence();
+    for(int j = warp; j < NV; j += (int)(blockDim.x >> 5)) {
+        double a = 0;
+        for(int blk = lane; blk < nb; blk += 32) a += __ldcg(&partials[(int64_t)j * nb + blk]);
+        for(int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if(lane == 0) sout[j] = a;
+    }
+    __syncthreads();
+    if(threadIdx.x == 0) *counter = 0u;
+#pragma unroll
+    for(int j = 0; j < NV; j++) out[j] = sout[j];
+    return true;
+}
+
+// d = 0, r = p = -r0; scalars
+template<class T>
+__global__ void cg_init_kernel(T *__restrict__ d, T *__restrict__ r, T *__restrict__ p, const T *__restrict__ r0, int64_t n, double *__restrict__ cs,
+                               double rho0, double theta, double tol2) {
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const T v = VOps<T>::scale(r0[i], -1.0);
+        d[i]      = VOps<T>::zero();
+        r[i]      = v;
+        p[i]      = v;
+    }
+    if(blockIdx.x == 0 && threadIdx.x == 0) {
+        cs[CG_RHO] = rho0, cs[CG_RHO0] = rho0, cs[CG_TOL2] = tol2, cs[CG_THETA] = theta;
+        cs[CG_DONE] = rho0 > 0 ? 0.0 : 1.0;
+    }
+}
+
+__device__ __forceinline__ void cj_acc(double &re, double &im, double a, double b) { re = fma(a, b, re); }
+__device__ __forceinline__ void cj_acc(double &re, double &im, double2 a, double2 b) {
+    re = fma(a.x, b.x, fma(a.y, b.y, re));  // conj(a) b
+    im = fma(a.x, b.y, fma(-a.y, b.x, im));
+}
+
+// q = z - theta p;  c = u^H q, pq = Re(p^H (q - c u)) = Re(p^H q - (p^H u) c);  alpha = rho / pq (done if pq <= 0)
+template<class T>
+__global__ void __launch_bounds__(256) cg_a_kernel(const T *__restrict__ z, const T *__restrict__ p, const T *__restrict__ u, T *__restrict__ q,
+                                                  int64_t n, double *__restrict__ cs, double *__restrict__ partials, unsigned *__restrict__ counter) {
+    if(cs[CG_DONE] != 0.0) return;
+    const double theta = cs[CG_THETA];
+    double       v[6]  = {0, 0, 0, 0, 0, 0};  // u^H q, p^H q, p^H u (re, im)
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const T zi = z[i], pi = p[i], ui = u[i];
+        const T qi = VOps<T>::addscaled(zi, -theta, pi);
+        q[i]       = qi;
+        cj_acc(v[0], v[1], ui, qi);
+        cj_acc(v[2], v[3], pi, qi);
+        cj_acc(v[4], v[5], pi, ui);
+    }
+    double s[6];
+    if(!grid_reduce_last<6>(v, partials, counter, s)) return;
+    if(threadIdx.x == 0) {
+        const double cre = s[0], cim = s[1];
+        const double pq  = s[2] - (s[4] * cre - s[5] * cim);  // Re(p^H q - (p^H u) c)
+        cs[CG_CRE] = cre, cs[CG_CIM] = cim;
+        if(!(pq > 0)) {
+            cs[CG_DONE] = 1.0;  // indefinite direction: keep what we have
+        } else {
+            cs[CG_ALPHA] = cs[CG_RHO] / pq;
+        }
+    }
+}
+
+// q <- q - c u;  d += alpha p;  r -= alpha q;  rho' = |r|^2;  done when rho' <= tol^2 rho0;  beta = rho'/rho
+template<class T>
+__global__ void __launch_bounds__(256) cg_b_kernel(const T *__restrict__ q, const T *__restrict__ u, const T *__restrict__ p, T *__restrict__ d,
+                                                  T *__restrict__ r, int64_t n, double *__restrict__ cs, double *__restrict__ partials,
+                                                  unsigned *__restrict__ counter) {
+    if(cs[CG_DONE] != 0.0) return;
+    const double alpha = cs[CG_ALPHA];
+    const T      c     = VOps<T>::make(cs[CG_CRE], cs[CG_CIM]);
+    double       v[1]  = {0};
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const T ui = u[i], pi = p[i], di = d[i], ri = r[i];
+        const T qp = VOps<T>::addscaled(q[i], -1.0, VOps<T>::axpy(VOps<T>::zero(), ui, c));  // q - c u
+        d[i]       = VOps<T>::addscaled(di, alpha, pi);
+        const T rn = VOps<T>::addscaled(ri, -alpha, qp);
+        r[i]       = rn;
+        double im  = 0;
+        cj_acc(v[0], im, rn, rn);
+    }
+    double s[1];
+    if(!grid_reduce_last<1>(v, partials, counter, s)) return;
+    if(threadIdx.x == 0) {
+        const double rho_new = s[0];
+        if(rho_new <= cs[CG_TOL2] * cs[CG_RHO0]) cs[CG_DONE] = 1.0;
+        cs[CG_BETA] = rho_new / cs[CG_RHO];
+        cs[CG_RHO]  = rho_new;
+    }
+}
+
+// p = r + beta p
+template<class T>
+__global__ void cg_c_kernel(const T *__restrict__ r, T *__restrict__ p, int64_t n, const double *__restrict__ cs) {
+    if(cs[CG_DONE] != 0.0) return;
+    const double beta = cs[CG_BETA];
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = VOps<T>::addscaled(r[i], beta, p[i]);
+}
+
+template<bool CPLX>
+int cg_init(typename Scalar<CPLX>::T *d, typename Scalar<CPLX>::T *r, typename Scalar<CPLX>::T *p, const typename Scalar<CPLX>::T *r0, int64_t n,
+            double *cs, double rho0, double theta, double tol2, cudaStream_t s) {
+    cg_init_kernel<typename Scalar<CPLX>::T><<<grid_for(n), 256, 0, s>>>(d, r, p, r0, n, cs, rho0, theta, tol2);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+template<bool CPLX>
+int cg_step(const typename Scalar<CPLX>::T *z, typename Scalar<CPLX>::T *p, const typename Scalar<CPLX>::T *u, typename Scalar<CPLX>::T *q,
+            typename Scalar<CPLX>::T *d, typename Scalar<CPLX>::T *r, int64_t n, double *cs, double *partials, unsigned *counter, cudaStream_t s) {
+    using T      = typename Scalar<CPLX>::T;
+    const int nb = (int)std::min<int64_t>(std::min<int64_t>(MD_BLOCKS, 4 * (int64_t)device_sm_count()), std::max<int64_t>(1, (n + 255) / 256));
+    cg_a_kernel<T><<<nb, 256, 0, s>>>(z, p, u, q, n, cs, partials, counter);
+    HEFF_LAUNCH_CHECK();
+    cg_b_kernel<T><<<nb, 256, 0, s>>>(q, u, p, d, r, n, cs, partials, counter);
+    HEFF_LAUNCH_CHECK();
+    cg_c_kernel<T><<<grid_for(n), 256, 0, s>>>(r, p, n, cs);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
 #define INST(C)                                                                                                                              \
     template int multi_dot<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, double *, cudaStream_t);   \
     template int multi_axpy<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, double, Scalar<C>::T *, cudaStream_t);   \
     template int combine<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, cudaStream_t);              \
     template int scale_dev<C>(Scalar<C>::T *, int64_t, const double *, bool, cudaStream_t);                                             \
     template int residual<C>(const Scalar<C>::T *, const Scalar<C>::T *, double, Scalar<C>::T *, int64_t, cudaStream_t);                  \
+    template int cg_init<C>(Scalar<C>::T *, Scalar<C>::T *, Scalar<C>::T *, const Scalar<C>::T *, int64_t, double *, double, double, double,      \
+                            cudaStream_t);                                                                                               \
+    template int cg_step<C>(const Scalar<C>::T *, Scalar<C>::T *, const Scalar<C>::T *, Scalar<C>::T *, Scalar<C>::T *, Scalar<C>::T *, int64_t, \
+                            double *, double *, unsigned *, cudaStream_t);                                                               \
     template int orth_cgs2<C>(const Scalar<C>::T *, int64_t, int64_t, int, const Scalar<C>::T *, Scalar<C>::T *, double *, unsigned *,     \
                               double *, Scalar<C>::T *, cudaStream_t);
 INST(false)

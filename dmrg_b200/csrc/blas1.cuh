@@ -35,4 +35,16 @@ template<bool CPLX>
 int orth_cgs2(const typename Scalar<CPLX>::T *V, int64_t ldv, int64_t n, int k, const typename Scalar<CPLX>::T *w, typename Scalar<CPLX>::T *v,
               double *partials, unsigned *counter, double *st, typename Scalar<CPLX>::T *hres, cudaStream_t s);
 
+// Device-side CG for the Jacobi-Davidson correction equation (I - uu^H)(H - theta)(I - uu^H) d = -r0 (see blas1.cu):
+// cg_init sets d = 0, r = p = -r0 and the scalars in cs (>= 16 doubles); each cg_step, after the caller has
+// formed z = H p, does the update with all scalars on the device.  cs[6] != 0 once CG has stopped (converged to
+// rho <= tol2 rho0, or an indefinite direction); later steps are no-ops.  partials >= 6 * MD_BLOCKS doubles.
+template<bool CPLX>
+int cg_init(typename Scalar<CPLX>::T *d, typename Scalar<CPLX>::T *r, typename Scalar<CPLX>::T *p, const typename Scalar<CPLX>::T *r0, int64_t n,
+            double *cs, double rho0, double theta, double tol2, cudaStream_t s);
+template<bool CPLX>
+int cg_step(const typename Scalar<CPLX>::T *z, typename Scalar<CPLX>::T *p, const typename Scalar<CPLX>::T *u, typename Scalar<CPLX>::T *q,
+            typename Scalar<CPLX>::T *d, typename Scalar<CPLX>::T *r, int64_t n, double *cs, double *partials, unsigned *counter, cudaStream_t s);
+constexpr int CG_DONE_SLOT = 6;
+
 }  // namespace heff

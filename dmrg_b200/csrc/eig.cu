@@ -116,7 +116,7 @@ struct Davidson {
     T *V = nullptr, *AV = nullptr, *V2 = nullptr, *AV2 = nullptr, *t = nullptr, *x = nullptr, *ax = nullptr, *r = nullptr;
     T *cg_p = nullptr, *cg_q = nullptr, *cg_z = nullptr, *cg_d = nullptr, *cg_r = nullptr;
     T *dh = nullptr, *dc = nullptr, *hres = nullptr;
-    double             *partials = nullptr, *dscal = nullptr, *orth_st = nullptr;
+    double             *partials = nullptr, *dscal = nullptr, *orth_st = nullptr, *cg_cs = nullptr;
     unsigned           *orth_counter = nullptr;
     std::vector<HT>     Hk, G2;
     std::vector<void *> allocs;
@@ -145,7 +145,7 @@ struct Davidson {
         const size_t vec = (es * n + 255) / 256 * 256;
         return vec * (4 * (maxb + 1) + 4 + (mixed ? 5 : 0)) + es * MD_MAXK * 3 + es * MD_MAXK * MD_MAXK +
                sizeof(double) * MD_BLOCKS * MD_MAXK * 4 + 16 * sizeof(double) + es * (MD_MAXK + 2) +
-               sizeof(double) * (8 + 4 * (MD_MAXK + 2)) + 20 * 256;
+               sizeof(double) * (8 + 4 * (MD_MAXK + 2)) + 21 * 256;
     }
     int setup(bool mixed) {
         const size_t es   = sizeof(T);
@@ -180,6 +180,7 @@ struct Davidson {
         HEFF_TRY(take((void **)&hres, es * (MD_MAXK + 2)));
         HEFF_TRY(take((void **)&orth_st, sizeof(double) * (8 + 4 * (MD_MAXK + 2))));
         HEFF_TRY(take((void **)&orth_counter, 256));
+        HEFF_TRY(take((void **)&cg_cs, sizeof(double) * 16));
         HEFF_CUDA(cudaMemsetAsync(orth_counter, 0, sizeof(unsigned), s));
         HEFF_TRY(eig_host_ready(op));
         Hk.assign((size_t)maxb * maxb, HT(0));
@@ -494,34 +495,22 @@ struct Davidson {
     }
 
     // CG on (I - u u^H)(H_mixed - theta)(I - u u^H) d = -r0 restricted to u^perp; d -> cg_d
+    // The CG scalars stay on the device (cg_init / cg_step); the host only polls the stop flag every second
+    // iteration, so at most one matvec runs past the stopping point.
     int correction(const T *u, const T *r0, double theta, double r0n) {
-        HEFF_CUDA(cudaMemsetAsync(cg_d, 0, sizeof(T) * n, s));
-        HEFF_CUDA(cudaMemcpyAsync(cg_r, r0, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-        HEFF_TRY(scale(cg_r, -1.0));
-        HEFF_CUDA(cudaMemcpyAsync(cg_p, cg_r, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-        double rho = r0n * r0n;
-        const double rho0 = rho;
+        HEFF_TRY(cg_init<CPLX>(cg_d, cg_r, cg_p, r0, n, cg_cs, r0n * r0n, theta, cfg.inner_tol * cfg.inner_tol, s));
         for(int it = 0; it < cfg.inner_iters; it++) {
             HEFF_TRY(apply(cg_p, cg_z, false));
-            HEFF_TRY(residual<CPLX>(cg_z, cg_p, theta, cg_q, n, s));  // q = (H - theta) p
-            HEFF_TRY(multi_dot<CPLX>(u, n, n, 1, cg_q, dh, partials, s));
-            HEFF_TRY(multi_axpy<CPLX>(u, n, n, 1, dh, -1.0, cg_q, s));  // q <- P q
-            HT pq;
-            HEFF_TRY(dot(cg_p, cg_q, pq));
-            const double pqr = HostScalar<CPLX>::re(pq);
-            if(!(pqr > 0)) break;  // indefinite direction: keep what we have
-            const double alpha = rho / pqr;
-            HEFF_TRY(axpy(alpha, cg_p, cg_d));
-            HEFF_TRY(axpy(-alpha, cg_q, cg_r));
-            double rho_new = 0;
-            HEFF_TRY(norm2(cg_r, rho_new));
-            if(rho_new <= cfg.inner_tol * cfg.inner_tol * rho0) break;
-            HEFF_TRY(scale(cg_p, rho_new / rho));
-            HEFF_TRY(axpy(1.0, cg_r, cg_p));
-            rho = rho_new;
+            HEFF_TRY(cg_step<CPLX>(cg_z, cg_p, u, cg_q, cg_d, cg_r, n, cg_cs, partials, orth_counter, s));
+            if((it & 1) == 1 && it + 1 < cfg.inner_iters) {
+                HEFF_CUDA(cudaMemcpyAsync(&cg_done_, cg_cs + CG_DONE_SLOT, sizeof(double), cudaMemcpyDeviceToHost, s));
+                HEFF_TRY(sync());
+                if(cg_done_ != 0.0) break;
+            }
         }
         return HEFF_OK;
     }
+    double cg_done_ = 0.0;
 
     // Phase 2: Jacobi-Davidson in FP64 starting from x (normalised).
     int refine(double &theta, double &rnorm, bool &conv) {
