@@ -13,6 +13,7 @@
 // adds ~sqrt(K) 2^-24).  The eigensolver uses this path for its inner iterations and restores FP64
 // accuracy by refinement with the FP64 matvec.  The environment operands (L, R') are split once per
 // operator; x and T2 are split per matvec.
+#include <algorithm>
 #include <cuda_bf16.h>
 
 #include "gemm_bf16x.cuh"
@@ -125,21 +126,32 @@ __global__ void split_R_kernel(const typename Scalar<CPLX>::T *__restrict__ Rp, 
         put_B<CPLX>(B2 + bp * Kx2, CPLX ? B2 + (bp + cR) * Kx2 : nullptr, Kp2, k, re_of(v), im_of(v));
     }
 }
-// B1'[(s + S b)][seg*Kp1 + a] from x[s + S*(a + cL*b)]; complex: Im rows at + N1
+// B1'[(s + S b)][seg*Kp1 + a] from x[s + S*(a + cL*b)]; complex: Im rows at + N1.
+// One block per (slab of ta values of a, one b): the S * ta inputs are a contiguous run of x (read
+// coalesced into shared memory), and every output row segment is ta consecutive bf16.
 template<bool CPLX>
-__global__ void split_x_kernel(const typename Scalar<CPLX>::T *__restrict__ x, __nv_bfloat16 *__restrict__ B1, int64_t S, int64_t cL, int64_t N1,
-                               int64_t Kp1, int64_t Kx1) {
-    const int64_t tot = cL * N1;
-    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t a = e % cL, n = e / cL, s = n % S, b = n / S;
-        const auto    v = x[s + S * (a + cL * b)];
-        put_B<CPLX>(B1 + n * Kx1, CPLX ? B1 + (n + N1) * Kx1 : nullptr, Kp1, a, re_of(v), im_of(v));
+__global__ void __launch_bounds__(256) split_x_kernel(const typename Scalar<CPLX>::T *__restrict__ x, __nv_bfloat16 *__restrict__ B1, int64_t S,
+                                                      int64_t cL, int64_t N1, int64_t Kp1, int64_t Kx1, int ta) {
+    using T = typename Scalar<CPLX>::T;
+    extern __shared__ __align__(16) unsigned char sx_smem[];
+    T            *sx  = reinterpret_cast<T *>(sx_smem);  // [S][ta]
+    const int64_t a0  = (int64_t)blockIdx.x * ta, b = blockIdx.y;
+    const int     na  = (int)(cL - a0 < (int64_t)ta ? cL - a0 : (int64_t)ta);
+    const T      *src = x + S * (a0 + cL * b);  // x[s + S (a0 + j + cL b)] for j < na: contiguous
+    for(int e = threadIdx.x; e < S * na; e += blockDim.x) sx[(e % S) * ta + e / S] = src[e];
+    __syncthreads();
+    for(int e = threadIdx.x; e < S * na; e += blockDim.x) {
+        const int     s = e / na, j = e % na;
+        const int64_t n = s + S * b;
+        const T       v = sx[s * ta + j];
+        put_B<CPLX>(B1 + n * Kx1, CPLX ? B1 + (n + N1) * Kx1 : nullptr, Kp1, a0 + j, re_of(v), im_of(v));
     }
 }
 
 // MIX: tile of 16 a' x 32 b.  Load phase a'-fastest (coalesced T1 reads) into shared memory; compute
 // phase b-fastest so the split T2 segments are written contiguously along k = b + cR*n.
 constexpr int MX_TA = 16, MX_TB = 32, MX_THREADS = MX_TA * MX_TB;
+constexpr int MX_SSTR = MX_TA * (MX_TB + 1);  // floats per staged (m, s) slice: a' rows padded to MX_TB + 1
 template<bool CPLX>
 __global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__restrict__ T1, const typename Scalar<CPLX>::T *__restrict__ W,
                                                               __nv_bfloat16 *__restrict__ A2, int S, int cL, int cR, int DL, int DR, int64_t M1,
@@ -150,23 +162,34 @@ __global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__re
     const int nW = DL * DR * S * S;
     float *sRe = reinterpret_cast<float *>(sW + nW);
     const int NP = DL * S;
-    float *sIm = sRe + NP * MX_THREADS;
-    unsigned char *lmem = reinterpret_cast<unsigned char *>(sIm + (CPLX ? NP * MX_THREADS : 0));
+    float *sIm = sRe + NP * MX_SSTR;
+    unsigned char *lmem = reinterpret_cast<unsigned char *>(sIm + (CPLX ? NP * MX_SSTR : 0));
     for(int i = threadIdx.x; i < nW; i += blockDim.x) sW[i] = W[i];
     const int a0 = blockIdx.x * MX_TA, b0 = blockIdx.y * MX_TB;
     {
-        const int al = threadIdx.x % MX_TA, bl = threadIdx.x / MX_TA;
-        const int ap = a0 + al, b = b0 + bl;
-        for(int ms = 0; ms < NP; ms++) {
-            const int m = ms / S, s = ms % S;
-            float     vr = 0.f, vi = 0.f;
-            if(ap < cL && b < cR) {
-                const int64_t idx = (ap + (int64_t)cL * m) + M1 * (s + (int64_t)S * b);
-                vr                = T1[idx];
-                if(CPLX) vi = T1[idx + M1 * N1];
+        // a'-fastest loads (coalesced along T1's rows), 8 in flight per thread; the staging row stride
+        // MX_TB + 1 keeps both this a'-fastest store and the b-fastest reads below free of bank conflicts
+        const int  al = threadIdx.x % MX_TA, bl = threadIdx.x / MX_TA;
+        const int  ap = a0 + al, b = b0 + bl;
+        const bool ok = ap < cL && b < cR;
+        for(int ms0 = 0; ms0 < NP; ms0 += 8) {
+            float vr[8], vi[8];
+#pragma unroll
+            for(int u = 0; u < 8; u++) {
+                const int ms = ms0 + u, m = ms / S, s = ms % S;
+                vr[u] = vi[u] = 0.f;
+                if(ok && ms < NP) {
+                    const int64_t idx = (ap + (int64_t)cL * m) + M1 * (s + (int64_t)S * b);
+                    vr[u]             = T1[idx];
+                    if(CPLX) vi[u] = T1[idx + M1 * N1];
+                }
             }
-            sRe[ms * MX_THREADS + al * MX_TB + bl] = vr;
-            if(CPLX) sIm[ms * MX_THREADS + al * MX_TB + bl] = vi;
+#pragma unroll
+            for(int u = 0; u < 8; u++)
+                if(ms0 + u < NP) {
+                    sRe[(ms0 + u) * MX_SSTR + al * (MX_TB + 1) + bl] = vr[u];
+                    if(CPLX) sIm[(ms0 + u) * MX_SSTR + al * (MX_TB + 1) + bl] = vi[u];
+                }
         }
     }
     __syncthreads();
@@ -177,14 +200,14 @@ __global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__re
     const int bl = threadIdx.x % MX_TB, al = threadIdx.x / MX_TB;
     const int ap = a0 + al, b = b0 + bl;
     if(ap >= cL || b >= cR) return;
-    const int me = al * MX_TB + bl;
+    const int me = al * (MX_TB + 1) + bl;
     for(int n = 0; n < DR; n++)
         for(int sp = 0; sp < S; sp++) {
             const int o  = n * S + sp;
             double    re = 0, im = 0;
             for(int e = off[o]; e < off[o + 1]; e++) {
                 const T      w    = wv[e];
-                const int    slot = idx[e] * MX_THREADS + me;
+                const int    slot = idx[e] * MX_SSTR + me;
                 const double xr   = sRe[slot];
                 if constexpr(CPLX) {
                     const double xi = sIm[slot];
@@ -271,7 +294,7 @@ static int mixed_setup(heff_op *op) {
     HEFF_TRY(make_tmap_bf16(&m->tA2, m->A2, m->M2, m->Kx2, m->Kx2, X_BM));
     HEFF_TRY(make_tmap_bf16(&m->tB2, m->B2, cf * m->N2, m->Kx2, m->Kx2, X_BN));
 
-    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS +
+    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_SSTR +
                             wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
     if(mix_smem > 200 * 1024) return HEFF_BAD_SHAPE;
     HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -287,12 +310,16 @@ static int mixed_apply_impl(heff_op *op, const void *x, void *y) {
     const auto  &d  = op->d;
     cudaStream_t s  = op->stream;
     const int    cf = CPLX ? 2 : 1;
-    split_x_kernel<CPLX><<<g1(m->K1 * m->N1), 256, 0, s>>>(reinterpret_cast<const T *>(x), m->B1, d.S, d.cL, m->N1, m->Kp1, m->Kx1);
+    // slab width: 256 values of a, fewer for large merged spins so the tile stays within 48 KB
+    const int ta = (int)std::max<int64_t>(32, std::min<int64_t>(256, (int64_t)(48 * 1024 / (sizeof(T) * d.S)) / 32 * 32));
+    if(d.cR > 65535 || (size_t)d.S * ta * sizeof(T) > 48 * 1024) return HEFF_BAD_SHAPE;
+    split_x_kernel<CPLX><<<dim3((unsigned)cdiv(d.cL, ta), (unsigned)d.cR), 256, (size_t)d.S * ta * sizeof(T), s>>>(
+        reinterpret_cast<const T *>(x), m->B1, d.S, d.cL, m->N1, m->Kp1, m->Kx1, ta);
     HEFF_LAUNCH_CHECK();
     XGemmArgs g1a{};
     g1a.M = (int)m->M1, g1a.N = (int)(cf * m->N1), g1a.K = (int)m->Kx1, g1a.C = m->T1, g1a.ldc = m->M1, g1a.mode = X_OUT_F32, g1a.err = m->err;
     HEFF_TRY(gemm_bf16x(m->tA1, m->tB1, g1a, s));
-    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_THREADS +
+    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_SSTR +
                             wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
     if(d.cR / MX_TB + 1 > 65535) return HEFF_BAD_SHAPE;
     dim3 grid((unsigned)cdiv(d.cL, MX_TA), (unsigned)cdiv(d.cR, MX_TB));
