@@ -33,6 +33,7 @@ STATUS = {
 F64, C128 = 0, 1
 MEM_DEVICE, MEM_HOST = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+FP64_DMMA, FP64_INT8 = 0, 1  # engines of the FP64-accurate matvecs (heff_op_set_fp64_engine)
 
 
 class HeffError(RuntimeError):
@@ -445,6 +446,10 @@ class MatVecMPOS:
 
     def set_precision(self, precision):
         check(lib().heff_op_set_precision(self.handle, int(precision)), "set_precision")
+
+    def set_fp64_engine(self, engine, nslices=0):
+        """FP64-accurate matvecs on the FP64 tensor cores (FP64_DMMA) or emulated on the INT8 tensor cores (FP64_INT8)."""
+        check(lib().heff_op_set_fp64_engine(self.handle, int(engine), int(nslices)), "set_fp64_engine")
 
     def set_profiling(self, enable=True):
         check(lib().heff_op_set_profiling(self.handle, int(bool(enable))), "set_profiling")

@@ -350,6 +350,21 @@ int dot_device(const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T
     return HEFF_OK;
 }
 
+template<bool CPLX>
+int permute_mps(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename Scalar<CPLX>::T *xp, cudaStream_t s) {
+    const int64_t n = d.size_mps();
+    permute_mps_kernel<<<grid_1d(n), 256, 0, s>>>(x, xp, d.S, d.cL, n);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+template<bool CPLX>
+int mix_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *T1, typename Scalar<CPLX>::T *T2, const typename Scalar<CPLX>::T *W, cudaStream_t s) {
+    return launch_mix<CPLX>(d, T1, T2, W, s);
+}
+template int permute_mps<false>(const MatvecDims &, const double *, double *, cudaStream_t);
+template int permute_mps<true>(const MatvecDims &, const double2 *, double2 *, cudaStream_t);
+template int mix_fp64<false>(const MatvecDims &, const double *, double *, const double *, cudaStream_t);
+template int mix_fp64<true>(const MatvecDims &, const double2 *, double2 *, const double2 *, cudaStream_t);
 template int permute_R<false>(const double *, double *, const MatvecDims &, cudaStream_t);
 template int permute_R<true>(const double2 *, double2 *, const MatvecDims &, cudaStream_t);
 template int matvec_fp64<false>(const MatvecDims &, const double *, double *, const double *, const double *, const double *,

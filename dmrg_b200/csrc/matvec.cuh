@@ -51,6 +51,13 @@ struct HostPipe {
     int                  n_in = 8, n_out = 8;  // measured at chi=1024 complex: 4/4 27.2, 8/8 29.0, 16/8 29.2 TFLOP/s end to end
 };
 
+// x'[a + cL (s + S b)] = x[s + S (a + cL b)] (the layout stage of the matvec).
+template<bool CPLX>
+int permute_mps(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename Scalar<CPLX>::T *xp, cudaStream_t s);
+// T2 = MPO mix of T1 (the MIX stage, FP64).
+template<bool CPLX>
+int mix_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *T1, typename Scalar<CPLX>::T *T2, const typename Scalar<CPLX>::T *W, cudaStream_t s);
+
 // y = H_eff x with pre-permuted R'.  L and W in reference layout.  Launches 4 kernels on s.
 // ev (optional): 5 events recorded before P and after P, G1, MIX, G2 (stage timing).
 template<bool CPLX>

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "matvec.cuh"
+#include "gemm_i8.cuh"
 #include "op.cuh"
 #include "runtime.cuh"
 
@@ -258,6 +259,7 @@ static int rebind_impl(heff_op *op, int nsites, const void *const *mpos_host, co
     using T  = typename Scalar<CPLX>::T;
     using HT = typename std::conditional<CPLX, HostC, double>::type;
     if(op->mixed && op->destroy_hook) op->destroy_hook(op);  // split operands belong to the old environments
+    op->emu_stale  = true;                                     // so do the digit planes of L and R' (rebuilt in place)
     op->diag_ready = false;
     std::vector<HT> W;
     int64_t         wd[4];
@@ -352,6 +354,7 @@ static int apply_impl(heff_op *op, const void *x, void *y) {
 int op_apply(heff_op *op, const void *x, void *y) {
     if(!op || !x || !y) return HEFF_BAD_ARG;
     if(op->precision == HEFF_PREC_MIXED && op->mixed_apply) return op->mixed_apply(op, x, y);
+    if(op->fp64_engine == HEFF_FP64_INT8 && emu_supported(op)) return emu_apply(op, x, y);
     return op->cplx ? apply_impl<true>(op, x, y) : apply_impl<false>(op, x, y);
 }
 
@@ -372,6 +375,7 @@ extern "C" int heff_op_create(heff_op **op, heff_dtype dtype, int nsites, const 
 extern "C" int heff_op_destroy(heff_op *op) {
     if(!op) return HEFF_OK;
     if(op->destroy_hook) op->destroy_hook(op);
+    emu_destroy(op);
     for(cudaEvent_t e : op->prof_events) cudaEventDestroy(e);
     if(op->L) cudaFree(op->L);
     if(op->Rp) cudaFree(op->Rp);
@@ -458,7 +462,7 @@ extern "C" int heff_op_multax_host(heff_op *op, const void *x_host, void *y_host
     }
     void *dx = op->stage_x;
     void *dy = reinterpret_cast<char *>(op->stage_x) + ((bytes + 255) / 256) * 256;
-    if(op->precision == HEFF_PREC_FP64 && !op->sequential && bytes >= ((size_t)8 << 20))
+    if(op->precision == HEFF_PREC_FP64 && op->fp64_engine == HEFF_FP64_DMMA && !op->sequential && bytes >= ((size_t)8 << 20))
         return op->cplx ? multax_host_pipelined<true>(op, x_host, y_host, dx, dy) : multax_host_pipelined<false>(op, x_host, y_host, dx, dy);
     HEFF_CUDA(cudaMemcpyAsync(dx, x_host, bytes, cudaMemcpyHostToDevice, op->stream));
     HEFF_TRY(op_apply(op, dx, dy));
@@ -484,11 +488,29 @@ extern "C" int heff_op_set_precision(heff_op *op, heff_precision precision) {
     return HEFF_OK;
 }
 
+extern "C" int heff_op_set_fp64_engine(heff_op *op, int engine, int nslices) {
+    if(!op) return HEFF_BAD_ARG;
+    if(engine != HEFF_FP64_DMMA && engine != HEFF_FP64_INT8) return HEFF_BAD_ARG;
+    if(nslices == 0) nslices = Z_DEFAULT_SLICES;
+    if(nslices < 3 || nslices > Z_MAX_SLICES) return HEFF_BAD_ARG;
+    if(nslices != op->emu_slices) {
+        if(op->emu) HEFF_CUDA(cudaStreamSynchronize(op->stream));
+        emu_destroy(op);  // planes are laid out per slice count
+        op->emu_slices = nslices;
+    }
+    op->fp64_engine = engine;
+    return HEFF_OK;
+}
+
 extern "C" int64_t heff_op_num_mv(const heff_op *op) { return op ? op->num_mv : -1; }
 
 extern "C" int heff_op_device_error(heff_op *op, int *code) {
     if(!op || !code) return HEFF_BAD_ARG;
-    return mixed_error_flag(op, code);
+    int m = 0, e = 0;
+    HEFF_TRY(mixed_error_flag(op, &m));
+    HEFF_TRY(emu_error_flag(op, &e));
+    *code = m ? m : e;
+    return HEFF_OK;
 }
 
 extern "C" int heff_op_set_profiling(heff_op *op, int enable) {

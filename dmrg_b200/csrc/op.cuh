@@ -42,6 +42,12 @@ struct heff_op {
     int                prof_cap      = 0, prof_used = 0;
     double             prof_ms[4]    = {0, 0, 0, 0};
     int64_t            prof_count    = 0;
+    // engine of the FP64-accurate matvecs: HEFF_FP64_DMMA, or HEFF_FP64_INT8 (emulated on the INT8 tensor cores,
+    // emu.cu; its digit planes of L and R' are rebuilt after a rebind)
+    int                fp64_engine   = HEFF_FP64_DMMA;
+    int                emu_slices    = 7;
+    void              *emu           = nullptr;
+    bool               emu_stale     = true;
     // mixed-precision state (owned by the mixed path; null until first use)
     void              *mixed         = nullptr;
     int (*mixed_apply)(heff_op *, const void *, void *) = nullptr;
@@ -52,6 +58,10 @@ namespace heff {
 int op_apply(heff_op *op, const void *x, void *y);
 int mixed_apply(heff_op *op, const void *x, void *y);     // mixed.cu
 int mixed_error_flag(heff_op *op, int *flag);              // mixed.cu
+bool emu_supported(const heff_op *op);                     // emu.cu: both GEMMs within the exact-INT32 range
+int emu_apply(heff_op *op, const void *x, void *y);        // emu.cu
+int emu_error_flag(heff_op *op, int *flag);                // emu.cu
+void emu_destroy(heff_op *op);                             // emu.cu
 int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_t Dmax, heff_precision prec, cudaStream_t stream);
 int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3], const void *envR,
               const int64_t rd[3]);

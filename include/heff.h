@@ -41,6 +41,7 @@ typedef enum {
 typedef enum { HEFF_F64 = 0, HEFF_C128 = 1 } heff_dtype;
 typedef enum { HEFF_MEM_DEVICE = 0, HEFF_MEM_HOST = 1 } heff_mem;
 typedef enum { HEFF_PREC_FP64 = 0, HEFF_PREC_MIXED = 1 } heff_precision;
+typedef enum { HEFF_FP64_DMMA = 0, HEFF_FP64_INT8 = 1 } heff_fp64_engine;
 
 /* Human-readable description of the last error raised on the calling thread. */
 const char *heff_last_error(void);
@@ -189,6 +190,14 @@ int heff_op_multax_block(heff_op *op, const void *x, int64_t ldx, void *y, int64
 int heff_op_multax_host(heff_op *op, const void *x_host, void *y_host);
 int heff_op_set_stream(heff_op *op, void *stream);
 int heff_op_set_precision(heff_op *op, heff_precision precision);
+/* Engine of the operator's FP64-accurate matvecs (HEFF_PREC_FP64 applies and the
+ * FP64 refinement steps of mixed eigensolves): HEFF_FP64_DMMA, the FP64 tensor
+ * cores (default); or HEFF_FP64_INT8, both GEMMs emulated on the INT8 tensor
+ * cores with `nslices` digit slices (0 = 7; 3..8) as in heff_gemm_i8_emu --
+ * normwise error a few 2^-48 relative at 7 slices.  Operators over more than 5
+ * site MPOs, and shapes whose GEMMs exceed the exact-INT32 range, keep DMMA.
+ * No counterpart in the reference (its matvec is Eigen FP64). */
+int heff_op_set_fp64_engine(heff_op *op, int engine, int nslices);
 /* Number of matvecs applied so far (MatVecMPOS::num_mv). */
 int64_t heff_op_num_mv(const heff_op *op);
 /* Stage timing (the reference's tid:: timers around MultAx, matvec_mpo.h:70-102):
@@ -198,8 +207,9 @@ int64_t heff_op_num_mv(const heff_op *op);
 int heff_op_set_profiling(heff_op *op, int enable);
 int heff_op_stage_times(heff_op *op, double ms[4], int64_t *count, int reset);
 /* Device-side status of the operator's tensor-core pipeline: *code = 0 when every
- * bounded wait in the mixed-precision kernels completed, nonzero when one timed out
- * (the kernel then skipped its work and returned).  Synchronises the stream. */
+ * bounded wait in the tensor-core kernels completed, nonzero when one timed out
+ * (the kernel then skipped its work and returned); 5 when the INT8 engine met a
+ * non-finite input (or one of magnitude >= 2^1022).  Synchronises the stream. */
 int heff_op_device_error(heff_op *op, int *code);
 /* Diagonal of H_eff, replacing MatVecMPOS::get_diagonal_new(0, ...)
  * (source/math/eig/matvec/matvec_mpos.cpp:300-407): diag[s + S(a + chiL b)] =
@@ -236,6 +246,27 @@ int heff_op_multpc(heff_op *op, const void *x, void *y, double shift);
  * so the split-precision building block can be validated on its own.
  * Synchronises the stream; HEFF_TIMEOUT if a pipeline wait timed out. */
 int heff_gemm_bf16_f32(const void *A, const void *B, float *C, int64_t M, int64_t N, int64_t K, void *stream);
+
+/* FP64-accurate GEMM on the INT8 tensor cores (tcgen05 kind::i8, exact INT32
+ * accumulation): C[m + M*n] = sum_k A[m*K + k] * B[n*K + k] (no conjugation),
+ * dtype HEFF_F64 or HEFF_C128, device buffers, A (M x K) and B (N x K) with K
+ * contiguous, C column-major.  Each row is scaled by a power of two and split
+ * into `nslices` signed 7-bit digit planes (0 = default 7, at most 8); digit
+ * products of equal weight are summed exactly and the weights combined in FP64,
+ * so the normwise error is a few 2^-(7*nslices-1) of |A||B| (2^-48 at 7).  No
+ * counterpart in the reference (its products are Eigen FP64); exposed so the
+ * emulated-FP64 building block can be validated on its own.  Synchronises the
+ * stream; HEFF_NAN_INPUT for a non-finite entry (or one of magnitude >= 2^1022),
+ * HEFF_BAD_SHAPE when K is too long for exact INT32 sums (K' * nslices >= 2^19,
+ * K' = round16(K), doubled for complex), HEFF_TIMEOUT if a pipeline wait timed out. */
+int heff_gemm_i8_emu(int dtype, const void *A, const void *B, void *C, int64_t M, int64_t N, int64_t K, int nslices, void *stream);
+/* Tile width of the INT8 emulated-FP64 GEMMs: 128, 192 or 256 columns, or 0 for
+ * the automatic choice (fewest waves on the device); the initial value comes
+ * from the environment variable HEFF_I8_BN.  Results do not depend on it (every
+ * width sums the same exact level products in the same order).  Returns the
+ * previous setting, or -1 for an invalid width.  Process-wide tuning knob; no
+ * counterpart in the reference. */
+int heff_i8_set_tile_width(int bn);
 
 /* ---------------------------------------------------------------------------
  * Eigensolver (the caller side of MultAx: eig::solver, source/math/eig/solver.h:15-88)
