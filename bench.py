@@ -205,12 +205,45 @@ def measure_mixed_and_eigs(hb, torch, op64, mpos, L, R, x, y, flush, stream, F):
         solve(opm, True)
         s64 = [solve(op64, False) for _ in range(2)]
         smx = [solve(opm, True) for _ in range(2)]
+        # the same matvec and solves with the FP64-accurate products emulated on the INT8 tensor cores
+        op8 = hb.MatVecMPOS(mpos, L, R, cplx=True, stream=stream)
+        op8.set_fp64_engine(hb.FP64_INT8)
+        y8 = torch.empty_like(x)
+        for _ in range(3):
+            op8.MultAx(x, y8)
+        ev8 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(10)]
+        for k, (a, b) in enumerate(ev8):
+            flush.fill_(float(k))
+            a.record(stream)
+            op8.MultAx(x, y8)
+            b.record(stream)
+        stream.synchronize()
+        i8_ms = sum(a.elapsed_time(b) for a, b in ev8) / len(ev8)
+        rel8 = float(torch.linalg.norm(y8 - y) / torch.linalg.norm(y))
+        solve(op8, False)
+        s8 = [solve(op8, False) for _ in range(2)]
+        opm.set_fp64_engine(hb.FP64_INT8)
+        solve(opm, True)
+        sm8 = [solve(opm, True) for _ in range(2)]
+        op8.close()
     opm.close()
     t64 = statistics.median(t for _, _, t in s64)
     tmx = statistics.median(t for _, _, t in smx)
+    t8 = statistics.median(t for _, _, t in s8)
+    tm8 = statistics.median(t for _, _, t in sm8)
     e64, r64 = s64[-1][0], s64[-1][1]
     emx, rmx = smx[-1][0], smx[-1][1]
+    int8 = {
+        "path": "both GEMMs emulated in FP64 accuracy on the INT8 tensor cores (tcgen05 kind::i8): 7 signed 7-bit digit planes per "
+                "operand row, equal-weight digit products folded into K, exact INT32 level sums, FP64 recombination",
+        "matvec": {"tflops_fp64_equiv": F / (i8_ms / 1e3) / 1e12, "ms": i8_ms, "rel_err_vs_dmma": rel8, "speedup_vs_dmma": None},
+        "eigensolves": {"fp64_int8_solves_per_s": 1.0 / t8, "mixed_int8_refinement_solves_per_s": 1.0 / tm8,
+                        "abs_dE_fp64_int8": abs(s8[-1][0] - e64), "abs_dE_mixed_int8": abs(sm8[-1][0] - e64),
+                        "speedup_fp64_int8_vs_dmma": t64 / t8, "speedup_mixed_int8_vs_dmma_fp64": t64 / tm8,
+                        "converged": [s8[-1][1]["converged"], sm8[-1][1]["converged"]], "seconds": [t8, tm8]},
+    }
     return {
+        "int8_engine": int8,
         "mixed_matvec": {"tflops": F / (mixed_ms / 1e3) / 1e12, "ms": mixed_ms, "rel_err_vs_fp64": rel,
                          "speedup_vs_fp64_matvec": None, "path": "split-BF16 (hi+mid, 3 products) tcgen05 GEMMs, FP32 accumulation",
                          "flops": "algorithmic (dense FP64 count); the tensor cores execute 3x that in BF16"},
@@ -566,6 +599,8 @@ def main():
     line.update(extras)
     if "mixed_matvec" in line:
         line["mixed_matvec"]["speedup_vs_fp64_matvec"] = ms_per_step / line["mixed_matvec"]["ms"]
+    if "int8_engine" in line:
+        line["int8_engine"]["matvec"]["speedup_vs_dmma"] = ms_per_step / line["int8_engine"]["matvec"]["ms"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     op.close()

@@ -2,6 +2,7 @@
 
     python -m dmrg_b200.profile_cases matvec --chi 1024 --dtype c128 --precision mixed --reps 3
     python -m dmrg_b200.profile_cases eigs --chi 1024 --dtype f64 --precision fp64
+    python -m dmrg_b200.profile_cases matvec --chi 1024 --dtype c128 --engine int8 --reps 2
     python -m dmrg_b200.profile_cases fdmrg --L 16 --chi 32 --sweeps 1
 
 The matvec case builds the standalone two-site workload (theta[4,chi,chi], Hermitian-slice environments
@@ -50,6 +51,7 @@ def main(argv=None):
     ap.add_argument("--dtype", choices=["f64", "c128"], default="c128")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--engine", choices=["dmma", "int8"], default="dmma", help="engine of the FP64-accurate matvecs")
     a = ap.parse_args(argv)
     if a.case == "fdmrg":  # two-site ground-state sweeps of the random-field Ising chain, fixed fields in [0.5, 1.5)
         h = 0.5 + np.array([(((i * 0x9E3779B97F4A7C15) >> 11) % 1000003) / 1000003.0 for i in range(1, a.L + 1)])
@@ -63,6 +65,8 @@ def main(argv=None):
     L = hb.to_host(hb.make_env(chi, D, cplx, seed=1, swap_base=swap), (chi, chi, D))
     R = hb.to_host(hb.make_env(chi, D, cplx, seed=2, swap_base=swap), (chi, chi, D))
     op = hb.MatVecMPOS(two_site_ising(D, cplx), L, R, cplx=cplx, precision=prec)
+    if a.engine == "int8":
+        op.set_fp64_engine(hb.FP64_INT8)
     x = hb.make_vector(op.rows(), cplx, seed=3)
     y = torch.empty_like(x)
     if a.case == "matvec":
