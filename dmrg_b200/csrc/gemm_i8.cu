@@ -156,27 +156,42 @@ __global__ void __launch_bounds__(256) z_slice_k_kernel(const typename Scalar<CP
     }
 }
 
-// M-major source src[r + ld k]: thread per (row, 16-column group), rows on consecutive threads (coalesced loads)
+// M-major source src[r + ld k]: one CTA per tile of 32 rows x 64 columns, read along the rows (coalesced) into
+// shared memory, then one thread per (row, 16-column group) emits the digits, so a warp writes 64 contiguous
+// bytes per row and plane.
+constexpr int ZM_TR = 32, ZM_TK = 64, ZM_THREADS = ZM_TR * ZM_TK / 16;
 template<bool CPLX>
-__global__ void __launch_bounds__(256) z_slice_m_kernel(const typename Scalar<CPLX>::T *__restrict__ src, int64_t rows, int64_t K, int64_t ld,
-                                                         const double *__restrict__ inv, int8_t *__restrict__ planes, int64_t kx, int ns, int *err) {
-    const int64_t ng = (K + 15) / 16, Kh = ng * 16, tot = rows * ng, plane = rows * kx;
-    for(int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = e % rows, g = e / rows;
-        const double  sc = inv[r];
-        double        yr[16], yi[16];
-#pragma unroll
-        for(int j = 0; j < 16; j++) {
-            yr[j] = yi[j] = 0.0;
-            const int64_t k = g * 16 + j;
-            if(k < K) {
-                const auto v = src[r + ld * k];
-                yr[j]        = z_re(v) * sc;
-                yi[j]        = z_im(v) * sc;
-            }
-        }
-        z_emit<CPLX, false>(yr, yi, planes, plane, kx, Kh, r, g, ns, err);
+__global__ void __launch_bounds__(ZM_THREADS) z_slice_m_kernel(const typename Scalar<CPLX>::T *__restrict__ src, int64_t rows, int64_t K,
+                                                                int64_t ld, const double *__restrict__ inv, int8_t *__restrict__ planes, int64_t kx,
+                                                                int ns, int *err) {
+    using T = typename Scalar<CPLX>::T;
+    __shared__ T  tile[ZM_TK][ZM_TR + 1];
+    const int64_t ng = (K + 15) / 16, Kh = ng * 16, plane = rows * kx;
+    const int64_t r0 = (int64_t)blockIdx.x * ZM_TR, k0 = (int64_t)blockIdx.y * ZM_TK;
+    for(int idx = threadIdx.x; idx < ZM_TR * ZM_TK; idx += ZM_THREADS) {
+        const int     rl = idx % ZM_TR, kl = idx / ZM_TR;
+        const int64_t r = r0 + rl, k = k0 + kl;
+        T             v;
+        if constexpr(CPLX)
+            v = make_double2(0.0, 0.0);
+        else
+            v = 0.0;
+        if(r < rows && k < K) v = src[r + ld * k];
+        tile[kl][rl] = v;
     }
+    __syncthreads();
+    const int     rl = threadIdx.x / (ZM_TK / 16), gl = threadIdx.x % (ZM_TK / 16);
+    const int64_t r = r0 + rl, g = k0 / 16 + gl;
+    if(r >= rows || g >= ng) return;
+    const double sc = inv[r];
+    double       yr[16], yi[16];
+#pragma unroll
+    for(int j = 0; j < 16; j++) {
+        const T v = tile[16 * gl + j][rl];
+        yr[j]     = z_re(v) * sc;
+        yi[j]     = z_im(v) * sc;
+    }
+    z_emit<CPLX, false>(yr, yi, planes, plane, kx, Kh, r, g, ns, err);
 }
 
 static int z_grid(int64_t n, int per_block = 256) {
@@ -221,7 +236,9 @@ int z_slice_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K,
 template<bool CPLX>
 int z_slice_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, const ZPlanes &p, int *err, cudaStream_t s) {
     if(rows <= 0) return HEFF_OK;
-    z_slice_m_kernel<CPLX><<<z_grid(rows * cdiv(K, 16)), 256, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.kx, p.nslice, err);
+    const int64_t gx = cdiv(rows, ZM_TR), gy = cdiv(K, ZM_TK);
+    if(gx > 0x7fffffff || gy > 65535) return HEFF_BAD_SHAPE;
+    z_slice_m_kernel<CPLX><<<dim3((unsigned)gx, (unsigned)gy), ZM_THREADS, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.kx, p.nslice, err);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }
