@@ -248,7 +248,7 @@ def xdmrg(h, energy_target, **kw):
 
 
 def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, precision=PREC_FP64, seed=0, ritz="SA", target=0.0,
-          energy_shift_per_site=0.0, algorithm=0, precond=-1, stream=None):
+          energy_shift_per_site=0.0, algorithm=0, precond=-1, fp64_engine=FP64_DMMA, stream=None):
     """Two-site DMRG of the random-field Ising chain on the device (heff_dmrg_run); returns the result dict."""
     from ._sigs import DmrgConfig, DmrgResult
 
@@ -269,12 +269,14 @@ def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, preci
     cfg.energy_shift_per_site = energy_shift_per_site
     cfg.algorithm = int(algorithm)
     cfg.precond = int(precond)
+    cfg.fp64_engine = int(fp64_engine)
     res = DmrgResult()
     check(lib().heff_dmrg_run(ctypes.byref(cfg), ctypes.byref(res), _stream_handle(stream)), "heff_dmrg_run")
     return res.as_dict()
 
 
-def ensemble(realisations, nthreads=16, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, J=1.0, precision=PREC_FP64):
+def ensemble(realisations, nthreads=16, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, J=1.0, precision=PREC_FP64,
+             fp64_engine=FP64_DMMA):
     """Independent fDMRG realisations (heff_ensemble_run).  realisations: list of (h_fields, chi_max or None, seed).
     Returns (list of result dicts, list of status codes, wall seconds)."""
     from ._sigs import DmrgConfig, DmrgResult
@@ -295,6 +297,7 @@ def ensemble(realisations, nthreads=16, chi_max=64, sweeps=10, trunc_lim=1e-12, 
         c.trunc_lim = trunc_lim
         c.eig_tol = eig_tol
         c.precision = precision
+        c.fp64_engine = int(fp64_engine)
         c.seed = int(seed)
     res = (DmrgResult * n)()
     st = (ctypes.c_int * n)()
@@ -337,7 +340,8 @@ class EigServer:
         self._keep = {}
 
     @staticmethod
-    def request(mpo, envL, envR, spin, chiL, chiR, cplx, theta0=None, ritz="SA", target=0.0, tol=1e-10, precision=PREC_FP64, theta_out=None):
+    def request(mpo, envL, envR, spin, chiL, chiR, cplx, theta0=None, ritz="SA", target=0.0, tol=1e-10, precision=PREC_FP64, theta_out=None,
+                fp64_engine=FP64_DMMA):
         """Builds an heff_request; mpo: host numpy [mL,mR,spin,spin]; envs/theta0: device tensors; theta_out: host numpy or None."""
         from ._sigs import Request
 
@@ -356,6 +360,7 @@ class EigServer:
         r.tol = float(tol)
         r.precision = int(precision)
         r.theta_out = theta_out.ctypes.data if theta_out is not None else None
+        r.fp64_engine = int(fp64_engine)
         return r, (W, envL, envR, theta0, theta_out)
 
     @staticmethod

@@ -33,7 +33,7 @@ class DmrgConfig(ctypes.Structure):
     _fields_ = [("L", ctypes.c_int), ("J", ctypes.c_double), ("h", _DP), ("chi_max", ctypes.c_int64), ("sweeps", ctypes.c_int),
                 ("trunc_lim", ctypes.c_double), ("eig_tol", ctypes.c_double), ("ritz", ctypes.c_int), ("target", ctypes.c_double),
                 ("precision", ctypes.c_int), ("seed", ctypes.c_int64), ("energy_shift_per_site", ctypes.c_double), ("algorithm", ctypes.c_int),
-                ("precond", ctypes.c_int)]
+                ("precond", ctypes.c_int), ("fp64_engine", ctypes.c_int)]
 
 
 class DmrgResult(ctypes.Structure):
@@ -57,7 +57,8 @@ class ServerConfig(ctypes.Structure):
 class Request(ctypes.Structure):
     _fields_ = [("dtype", ctypes.c_int), ("spin", ctypes.c_int64), ("chiL", ctypes.c_int64), ("chiR", ctypes.c_int64), ("mpoL", ctypes.c_int64),
                 ("mpoR", ctypes.c_int64), ("mpo", _P), ("envL", _P), ("envR", _P), ("env_where", ctypes.c_int), ("theta0", _P),
-                ("ritz", ctypes.c_int), ("target", ctypes.c_double), ("tol", ctypes.c_double), ("precision", ctypes.c_int), ("theta_out", _P)]
+                ("ritz", ctypes.c_int), ("target", ctypes.c_double), ("tol", ctypes.c_double), ("precision", ctypes.c_int), ("theta_out", _P),
+                ("fp64_engine", ctypes.c_int)]
 
 
 class Response(ctypes.Structure):

@@ -153,7 +153,7 @@ struct DmrgWorkspace {
         ptrs.push_back(*p);
         return HEFF_OK;
     }
-    int init(int L, int64_t chi, heff_precision prec, cudaStream_t stream, int64_t Dmax = 3) {
+    int init(int L, int64_t chi, heff_precision prec, cudaStream_t stream, int64_t Dmax = 3, int engine = HEFF_FP64_DMMA) {
         const int64_t d = 2;
         Lcap = L;
         chicap = chi;
@@ -183,6 +183,10 @@ struct DmrgWorkspace {
         const size_t  scr_elems = std::max<size_t>((size_t)env_scratch_elems(md_max, wd_max), (size_t)schmidt_scratch_bytes(d, d, chi, chi, chi) / 8 + 64);
         HEFF_TRY(get(&scr, scr_elems));
         HEFF_TRY(op_create_capacity(&op, false, d * d, chi, Dmax, prec, stream));
+        if(engine == HEFF_FP64_INT8) {
+            op->fp64_engine = HEFF_FP64_INT8;
+            HEFF_TRY(emu_reserve(op, d * d, chi, Dmax));  // digit planes for the largest bond, once
+        }
         heff_eig_config ec;
         heff_eig_config_default(&ec);
         return eig_reserve(op, d * d * chi * chi, ec.max_basis, prec == HEFF_PREC_MIXED);
@@ -199,6 +203,8 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     cudaStream_t  s = ws.s;
     std::memset(&res, 0, sizeof(res));
     ws.op->precision = (heff_precision)cfg.precision;
+    if(cfg.fp64_engine != HEFF_FP64_DMMA && cfg.fp64_engine != HEFF_FP64_INT8) return HEFF_BAD_ARG;
+    ws.op->fp64_engine = cfg.fp64_engine;
     // --- model (host copies stay alive until the stream has consumed them): H, or (H - E_t)^2 for xDMRG
     std::vector<std::vector<double>>    Wh(L);
     std::vector<std::array<int64_t, 4>> wd(L);
@@ -377,7 +383,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
 int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s) {
     if(cfg.L < 2 || cfg.L > 4096 || !cfg.h || cfg.chi_max < 1) return HEFF_BAD_ARG;
     DmrgWorkspace ws;
-    HEFF_TRY(ws.init(cfg.L, cfg.chi_max, (heff_precision)cfg.precision, s, cfg.algorithm == 1 ? 9 : 3));
+    HEFF_TRY(ws.init(cfg.L, cfg.chi_max, (heff_precision)cfg.precision, s, cfg.algorithm == 1 ? 9 : 3, cfg.fp64_engine));
     return dmrg_run_ws(cfg, res, ws);
 }
 
@@ -403,10 +409,13 @@ int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_re
     for(int t = 0; t < nthreads; t++) {
         HEFF_CUDA(cudaStreamCreateWithFlags(&streams[t], cudaStreamNonBlocking));
         wss[t] = std::make_unique<DmrgWorkspace>();
-        int64_t Dmax = 3;
-        for(int i = 0; i < n; i++)
+        int64_t Dmax   = 3;
+        int     engine = HEFF_FP64_DMMA;
+        for(int i = 0; i < n; i++) {
             if(cfgs[i].algorithm == 1) Dmax = 9;
-        int rc = wss[t]->init(Lmax, chimax, (heff_precision)cfgs[0].precision, streams[t], Dmax);
+            if(cfgs[i].fp64_engine == HEFF_FP64_INT8) engine = HEFF_FP64_INT8;
+        }
+        int rc = wss[t]->init(Lmax, chimax, (heff_precision)cfgs[0].precision, streams[t], Dmax, engine);
         if(rc != HEFF_OK) return rc;
     }
     auto t0 = std::chrono::steady_clock::now();

@@ -16,9 +16,13 @@
 
 namespace heff {
 
+// Buffer layout: err (256 B) | rmax[rmax_cap] | scales | planes A1 | B1 | A2 | B2.  The error flag and the
+// row-maximum accumulators sit at fixed offsets (zeroed when the buffer is allocated and left zero by the
+// kernels), so a rebind to other dimensions never finds stale bytes there.
 struct EmuState {
-    void   *buf = nullptr;  // A1 | B1 | A2 | B2 planes | scales | rmax (A2) | err
+    void   *buf = nullptr;
     size_t  cap = 0;
+    int64_t rmax_cap = 0;  // rows of T2 the accumulators cover
     int    *err = nullptr;
     ZPlanes A1, B1, A2, B2;
 };
@@ -61,51 +65,85 @@ void emu_destroy(heff_op *op) {
 
 static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
 
+struct EmuSizes {
+    size_t A1, B1, A2, B2, S, R;
+    size_t total() const { return 256 + R + S + A1 + B1 + A2 + B2; }
+};
+static EmuSizes emu_sizes(const EmuDims &e, int ns, int64_t rmax_rows) {
+    EmuSizes z;
+    z.A1 = up256((size_t)ns * e.M1 * e.kx1), z.B1 = up256((size_t)ns * e.cf * e.N1 * e.kx1);
+    z.A2 = up256((size_t)ns * e.M2 * e.kx2), z.B2 = up256((size_t)ns * e.cf * e.N2 * e.kx2);
+    z.S  = up256(sizeof(double) * 2 * (size_t)(e.M1 + e.N1 + e.M2 + e.N2));
+    z.R  = up256(sizeof(unsigned long long) * (size_t)rmax_rows);
+    return z;
+}
+
+// (Re)allocates the buffer for `need` bytes with row-maximum room for rmax_rows rows (zeroed).
+static int emu_alloc(heff_op *op, EmuState *st, size_t need, int64_t rmax_rows) {
+    if(st->buf) {
+        HEFF_CUDA(cudaStreamSynchronize(op->stream));
+        cudaFree(st->buf);
+        st->buf = nullptr;
+        st->cap = 0;
+    }
+    cudaError_t ce = cudaMalloc(&st->buf, need);
+    if(ce != cudaSuccess) {
+        set_last_cuda_error(ce, "emulated-FP64 digit planes", __FILE__, __LINE__);
+        return HEFF_OOM;
+    }
+    st->cap      = need;
+    st->rmax_cap = rmax_rows;
+    HEFF_CUDA(cudaMemsetAsync(st->buf, 0, need, op->stream));
+    op->emu_stale = true;
+    return HEFF_OK;
+}
+
 // Carves the planes for the operator's current dimensions out of the state's buffer (grown when needed).
 static int emu_layout(heff_op *op, EmuState *st) {
     const EmuDims e  = emu_dims(op);
     const int     ns = op->emu_slices;
-    const size_t  bA1 = up256((size_t)ns * e.M1 * e.kx1), bB1 = up256((size_t)ns * e.cf * e.N1 * e.kx1);
-    const size_t  bA2 = up256((size_t)ns * e.M2 * e.kx2), bB2 = up256((size_t)ns * e.cf * e.N2 * e.kx2);
-    const size_t  bS  = up256(sizeof(double) * 2 * (size_t)(e.M1 + e.N1 + e.M2 + e.N2));
-    const size_t  bR  = up256(sizeof(unsigned long long) * (size_t)e.M2);
-    const size_t  need = bA1 + bB1 + bA2 + bB2 + bS + bR + 256;
-    if(need > st->cap) {
-        if(st->buf) {
-            HEFF_CUDA(cudaStreamSynchronize(op->stream));
-            cudaFree(st->buf);
-            st->buf = nullptr;
-            st->cap = 0;
-        }
-        cudaError_t ce = cudaMalloc(&st->buf, need);
-        if(ce != cudaSuccess) {
-            set_last_cuda_error(ce, "emulated-FP64 digit planes", __FILE__, __LINE__);
-            return HEFF_OOM;
-        }
-        st->cap = need;
-        // the row-maximum accumulators (and the error flag) start at zero; the kernels leave them zero
-        HEFF_CUDA(cudaMemsetAsync(st->buf, 0, need, op->stream));
-        op->emu_stale = true;
-    }
+    EmuSizes      z  = emu_sizes(e, ns, std::max<int64_t>(st->rmax_cap, e.M2));
+    if(z.total() > st->cap || e.M2 > st->rmax_cap) HEFF_TRY(emu_alloc(op, st, z.total(), std::max<int64_t>(st->rmax_cap, e.M2)));
     unsigned char *p = reinterpret_cast<unsigned char *>(st->buf);
-    auto           planes = [&](ZPlanes &z, size_t bytes, int64_t rows, int64_t kx) {
-        z.planes = reinterpret_cast<int8_t *>(p), z.rows = rows, z.kx = kx, z.nslice = ns;
+    st->err          = reinterpret_cast<int *>(p);
+    p += 256;
+    st->A2.rmax = reinterpret_cast<unsigned long long *>(p);
+    p += z.R;
+    double *sc = reinterpret_cast<double *>(p);
+    st->A1.inv = sc, st->A1.fac = sc + e.M1, sc += 2 * e.M1;
+    st->B1.inv = sc, st->B1.fac = sc + e.N1, sc += 2 * e.N1;
+    st->A2.inv = sc, st->A2.fac = sc + e.M2, sc += 2 * e.M2;
+    st->B2.inv = sc, st->B2.fac = sc + e.N2;
+    p += z.S;
+    auto planes = [&](ZPlanes &q, size_t bytes, int64_t rows, int64_t kx) {
+        q.planes = reinterpret_cast<int8_t *>(p), q.rows = rows, q.kx = kx, q.nslice = ns;
         p += bytes;
     };
-    planes(st->A1, bA1, e.M1, e.kx1);
-    planes(st->B1, bB1, e.cf * e.N1, e.kx1);
-    planes(st->A2, bA2, e.M2, e.kx2);
-    planes(st->B2, bB2, e.cf * e.N2, e.kx2);
-    double *sc   = reinterpret_cast<double *>(p);
-    st->A1.inv   = sc, st->A1.fac = sc + e.M1, sc += 2 * e.M1;
-    st->B1.inv   = sc, st->B1.fac = sc + e.N1, sc += 2 * e.N1;
-    st->A2.inv   = sc, st->A2.fac = sc + e.M2, sc += 2 * e.M2;
-    st->B2.inv   = sc, st->B2.fac = sc + e.N2;
-    p += bS;
-    st->A2.rmax = reinterpret_cast<unsigned long long *>(p);
-    p += bR;
-    st->err = reinterpret_cast<int *>(p);
+    planes(st->A1, z.A1, e.M1, e.kx1);
+    planes(st->B1, z.B1, e.cf * e.N1, e.kx1);
+    planes(st->A2, z.A2, e.M2, e.kx2);
+    planes(st->B2, z.B2, e.cf * e.N2, e.kx2);
     return HEFF_OK;
+}
+
+int emu_reserve(heff_op *op, int64_t S, int64_t cmax, int64_t Dmax) {
+    if(!op->emu) op->emu = new EmuState();
+    EmuState *st = reinterpret_cast<EmuState *>(op->emu);
+    EmuDims   e;
+    e.cf = op->cplx ? 2 : 1;
+    e.M1 = cmax * Dmax, e.N1 = S * cmax, e.K1 = cmax, e.kx1 = z_kx(e.K1, op->cplx);
+    e.M2 = S * cmax, e.N2 = cmax, e.K2 = cmax * Dmax, e.kx2 = z_kx(e.K2, op->cplx);
+    const EmuSizes z = emu_sizes(e, op->emu_slices, e.M2);
+    if(z.total() <= st->cap && e.M2 <= st->rmax_cap) return HEFF_OK;
+    return emu_alloc(op, st, z.total(), e.M2);
+}
+
+size_t emu_bytes(int64_t S, int64_t cL, int64_t cR, int64_t DL, int64_t DR, bool cplx, int nslices) {
+    EmuDims e;
+    e.cf = cplx ? 2 : 1;
+    e.M1 = cL * DL, e.N1 = S * cR, e.K1 = cL, e.kx1 = z_kx(e.K1, cplx);
+    e.M2 = S * cL, e.N2 = cR, e.K2 = cR * DR, e.kx2 = z_kx(e.K2, cplx);
+    return emu_sizes(e, nslices, e.M2).total();
 }
 
 template<bool CPLX>

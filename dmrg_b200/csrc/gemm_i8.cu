@@ -589,11 +589,15 @@ static int z_forced_bn() {
     return f;
 }
 
-int z_choose_bn(int64_t M, int64_t N) {
+int z_choose_bn(int64_t M, int64_t N, int64_t K) {
     if(const int forced = z_forced_bn()) return forced;
+    // cost = waves x width x per-MAC weight.  The weights are measured (B200, 7 slices, the matvec GEMMs of
+    // chi=1024, real and complex): with few k-blocks per slice the levels are short and summing them in C
+    // costs more than the 128-wide tile's extra operand traffic; with long K the widest tile is best.
     const int64_t sms  = device_sm_count();
+    const int64_t kbs  = cdiv(K, Z_BK);
     const int     bn[3] = {256, 192, 128};
-    const double  w[3]  = {1.0, 1.04, 1.12};  // per-MAC cost of the narrower tiles (more operand traffic per MAC)
+    const double  w[3]  = {1.0, kbs <= 16 ? 0.95 : 1.06, kbs <= 8 ? 0.85 : 1.3};
     int           best = 256;
     double        bc   = 1e300;
     for(int i = 0; i < 3; i++) {
@@ -625,7 +629,7 @@ int gemm_i8_ozaki(const ZPlanes &A, const ZPlanes &B, const ZGemmArgs &a, cudaSt
     if(a.M <= 0 || a.N <= 0) return HEFF_OK;
     if(a.K <= 0 || a.K % 16 || a.nslice < 1 || a.nslice > Z_MAX_SLICES || !z_k_ok(a.K, a.nslice) || (a.cplx && a.N % 2)) return HEFF_BAD_ARG;
     if(A.kx != a.K || B.kx != a.K || A.rows < a.M || B.rows < a.N || A.nslice < a.nslice || B.nslice < a.nslice) return HEFF_BAD_ARG;
-    const int   bn = z_choose_bn(a.M, a.N);
+    const int   bn = z_choose_bn(a.M, a.N, a.K);
     CUtensorMap tA, tB;
     HEFF_TRY(make_tmap_planes(&tA, A, Z_BM));
     HEFF_TRY(make_tmap_planes(&tB, B, bn));

@@ -69,8 +69,8 @@ struct ZGemmArgs {
 
 // 3D tensor map over digit planes {kx, rows, nslice}, box {128, box_rows, 1}, 128-byte swizzle.
 int make_tmap_planes(CUtensorMap *map, const ZPlanes &p, int box_rows);
-// Tile width for a C' of M x N (fewest waves on the device's SMs, narrower tiles weighted by their extra traffic).
-int z_choose_bn(int64_t M, int64_t N);
+// Tile width for a C' of M x N over K' (fewest waves on the device's SMs, weighted by measured per-MAC costs).
+int z_choose_bn(int64_t M, int64_t N, int64_t K);
 
 // Row scales of a K-major source src[r * ld + k] (k < K): inv, fac (fac = sigma * extra).
 template<bool CPLX>

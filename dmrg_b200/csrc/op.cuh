@@ -62,6 +62,8 @@ bool emu_supported(const heff_op *op);                     // emu.cu: both GEMMs
 int emu_apply(heff_op *op, const void *x, void *y);        // emu.cu
 int emu_error_flag(heff_op *op, int *flag);                // emu.cu
 void emu_destroy(heff_op *op);                             // emu.cu
+int emu_reserve(heff_op *op, int64_t S, int64_t cmax, int64_t Dmax);  // emu.cu: digit-plane buffer for the largest bond
+size_t emu_bytes(int64_t S, int64_t cL, int64_t cR, int64_t DL, int64_t DR, bool cplx, int nslices);  // emu.cu
 int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_t Dmax, heff_precision prec, cudaStream_t stream);
 int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3], const void *envR,
               const int64_t rd[3]);

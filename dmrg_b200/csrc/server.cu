@@ -50,7 +50,8 @@ namespace heff {
 static int64_t r64(int64_t v) { return (v + 63) / 64 * 64; }
 
 // Device memory one request holds while it runs (operator copies + matvec scratch + mixed-precision
-// split operands + eigensolver basis), matching the allocations in op.cu, mixed.cu and eig.cu.
+// split operands or INT8-engine digit planes + eigensolver basis), matching the allocations in op.cu,
+// mixed.cu, emu.cu and eig.cu.
 size_t request_bytes(const heff_request &r, int max_basis) {
     const int64_t es = r.dtype == HEFF_C128 ? 16 : 8, cf = r.dtype == HEFF_C128 ? 2 : 1;
     const int64_t S = r.spin, cL = r.chiL, cR = r.chiR, DL = r.mpoL, DR = r.mpoR;
@@ -65,6 +66,7 @@ size_t request_bytes(const heff_request &r, int max_basis) {
         b += 2 * (S * cL) * nseg * r64(cR * DR) + 2 * cf * cR * nseg * r64(cR * DR);   // A2, B2
         b += 4 * (cL * DL) * cf * (S * cR);                                            // T1 (fp32)
     }
+    if(r.fp64_engine == HEFF_FP64_INT8) b += (int64_t)emu_bytes(S, cL, cR, DL, DR, r.dtype == HEFF_C128, 7);  // digit planes
     const int64_t vec = (es * n + 255) / 256 * 256;
     b += vec * (2 * (max_basis + 1) + 2 * max_basis + 4 + (mixed ? 5 : 0)) + (int64_t)(es * 128 * 131) + 8 * 512 * 128 * 4;
     return (size_t)b + (size_t)(4 << 20);
@@ -81,6 +83,7 @@ static void run_request(heff_server *srv, heff_server::Item &it, cudaStream_t st
     const int64_t rd[3]   = {r.chiR, r.chiR, r.mpoR};
     heff_op      *op      = nullptr;
     int rc = heff_op_create(&op, (heff_dtype)r.dtype, 1, mp, md, r.envL, ld, r.envR, rd, (heff_mem)r.env_where, (heff_precision)r.precision, stream);
+    if(rc == HEFF_OK && r.fp64_engine != HEFF_FP64_DMMA) rc = heff_op_set_fp64_engine(op, r.fp64_engine, 0);
     if(rc == HEFF_OK) {
         heff_eig_config cfg;
         heff_eig_config_default(&cfg);

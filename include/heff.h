@@ -329,6 +329,9 @@ typedef struct {
     int           precond;               /* eigensolver expansion (heff_eig_config.precond); default -1:
                                             Jacobi for xDMRG (as the reference's PRIMME set-up for H^2,
                                             optimize_folded_spectrum.cpp:303-304), Krylov for fDMRG */
+    int           fp64_engine;           /* heff_fp64_engine of the FP64-accurate matvecs (heff_op_set_fp64_engine);
+                                            default HEFF_FP64_DMMA.  With HEFF_FP64_INT8 the digit planes are
+                                            reserved once for chi_max, so sweeps still allocate nothing */
 } heff_dmrg_config;
 
 typedef struct {
@@ -380,6 +383,7 @@ typedef struct {
     double        tol;                         /* eigensolver tolerance, default 1e-10 */
     int           precision;                   /* heff_precision */
     void         *theta_out;                   /* HOST output eigenvector (rows elements) or NULL */
+    int           fp64_engine;                 /* heff_fp64_engine of the FP64-accurate matvecs, default 0 (DMMA) */
 } heff_request; /* buffers must stay valid until the request is answered; device buffers must be
                    complete (their producing work finished) when the request is submitted */
 
