@@ -84,13 +84,20 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_kernel(const T *__restrict__ 
     const int     ap  = blockIdx.x * MIX_THREADS + threadIdx.x;
     const bool    act = ap < cL;
     const int64_t cLD = (int64_t)cL * DL;
-    for(int s = 0; s < S; s++)
-        for(int m = 0; m < DL; m++) {
-            T v;
-            zero(v);
-            if(act) v = T1[(ap + (int64_t)cL * m) + cLD * (s + (int64_t)S * b)];
-            sIn[(m * S + s) * MIX_THREADS + threadIdx.x] = v;
+    // 8 loads in flight per thread before their shared-memory stores (slot ms = m*S + s)
+    const int NP = DL * S;
+    for(int ms0 = 0; ms0 < NP; ms0 += 8) {
+        T v[8];
+#pragma unroll
+        for(int u = 0; u < 8; u++) {
+            const int ms = ms0 + u, m = ms / S, s = ms % S;
+            zero(v[u]);
+            if(act && ms < NP) v[u] = T1[(ap + (int64_t)cL * m) + cLD * (s + (int64_t)S * b)];
         }
+#pragma unroll
+        for(int u = 0; u < 8; u++)
+            if(ms0 + u < NP) sIn[(ms0 + u) * MIX_THREADS + threadIdx.x] = v[u];
+    }
     __syncthreads();
     int   *off;
     short *idx;

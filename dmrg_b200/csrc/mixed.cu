@@ -31,6 +31,8 @@ struct MixedState {
     __nv_bfloat16 *A1 = nullptr, *B1 = nullptr, *A2 = nullptr, *B2 = nullptr;
     float         *T1  = nullptr;
     int           *err = nullptr;
+    unsigned char *wl  = nullptr;  // the MPO's nonzero list (wlist.cuh layout)
+    int            wl_bytes = 0;
     CUtensorMap    tA1, tB1, tA2, tB2;
 };
 
@@ -153,18 +155,17 @@ __global__ void __launch_bounds__(256) split_x_kernel(const typename Scalar<CPLX
 constexpr int MX_TA = 16, MX_TB = 32, MX_THREADS = MX_TA * MX_TB;
 constexpr int MX_SSTR = MX_TA * (MX_TB + 1);  // floats per staged (m, s) slice: a' rows padded to MX_TB + 1
 template<bool CPLX>
-__global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__restrict__ T1, const typename Scalar<CPLX>::T *__restrict__ W,
+__global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__restrict__ T1, const unsigned char *__restrict__ wl, int wl_bytes,
                                                               __nv_bfloat16 *__restrict__ A2, int S, int cL, int cR, int DL, int DR, int64_t M1,
                                                               int64_t N1, int64_t Kp2, int64_t Kx2) {
     using T = typename Scalar<CPLX>::T;
     extern __shared__ __align__(16) unsigned char mxs[];
-    T     *sW  = reinterpret_cast<T *>(mxs);
-    const int nW = DL * DR * S * S;
-    float *sRe = reinterpret_cast<float *>(sW + nW);
+    float *sRe = reinterpret_cast<float *>(mxs);
     const int NP = DL * S;
     float *sIm = sRe + NP * MX_SSTR;
     unsigned char *lmem = reinterpret_cast<unsigned char *>(sIm + (CPLX ? NP * MX_SSTR : 0));
-    for(int i = threadIdx.x; i < nW; i += blockDim.x) sW[i] = W[i];
+    // the MPO's nonzero list (built once per operator) lands in shared memory with the T1 tile, under the same barrier
+    for(int i = threadIdx.x; i < wl_bytes / 16; i += blockDim.x) reinterpret_cast<uint4 *>(lmem)[i] = reinterpret_cast<const uint4 *>(wl)[i];
     const int a0 = blockIdx.x * MX_TA, b0 = blockIdx.y * MX_TB;
     {
         // a'-fastest loads (coalesced along T1's rows), 8 in flight per thread; the staging row stride
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__re
     int   *off;
     short *idx;
     T     *wv;
-    build_wlist(sW, DL, DR, S, lmem, off, idx, wv);
+    wlist_views(lmem, DL, DR, S, off, idx, wv);
     const int bl = threadIdx.x % MX_TB, al = threadIdx.x / MX_TB;
     const int ap = a0 + al, b = b0 + bl;
     if(ap >= cL || b >= cR) return;
@@ -237,6 +238,7 @@ static void mixed_destroy(heff_op *op) {
     if(m->B2) cudaFree(m->B2);
     if(m->T1) cudaFree(m->T1);
     if(m->err) cudaFree(m->err);
+    if(m->wl) cudaFree(m->wl);
     delete m;
     op->mixed = nullptr;
 }
@@ -294,8 +296,11 @@ static int mixed_setup(heff_op *op) {
     HEFF_TRY(make_tmap_bf16(&m->tA2, m->A2, m->M2, m->Kx2, m->Kx2, X_BM));
     HEFF_TRY(make_tmap_bf16(&m->tB2, m->B2, cf * m->N2, m->Kx2, m->Kx2, X_BN));
 
-    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_SSTR +
-                            wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
+    m->wl_bytes = (int)wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
+    HEFF_TRY(al((void **)&m->wl, (size_t)m->wl_bytes));
+    wlist_global_kernel<T><<<1, 32, 0, s>>>(reinterpret_cast<const T *>(op->W), (int)d.DL, (int)d.DR, (int)d.S, m->wl);
+    HEFF_LAUNCH_CHECK();
+    const size_t mix_smem = (size_t)cf * 4 * d.DL * d.S * MX_SSTR + (size_t)m->wl_bytes;
     if(mix_smem > 200 * 1024) return HEFF_BAD_SHAPE;
     HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     HEFF_CUDA(cudaStreamSynchronize(s));
@@ -319,12 +324,11 @@ static int mixed_apply_impl(heff_op *op, const void *x, void *y) {
     XGemmArgs g1a{};
     g1a.M = (int)m->M1, g1a.N = (int)(cf * m->N1), g1a.K = (int)m->Kx1, g1a.C = m->T1, g1a.ldc = m->M1, g1a.mode = X_OUT_F32, g1a.err = m->err;
     HEFF_TRY(gemm_bf16x(m->tA1, m->tB1, g1a, s));
-    const size_t mix_smem = sizeof(T) * (size_t)(d.DL * d.DR * d.S * d.S) + (size_t)cf * 4 * d.DL * d.S * MX_SSTR +
-                            wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
+    const size_t mix_smem = (size_t)cf * 4 * d.DL * d.S * MX_SSTR + (size_t)m->wl_bytes;
     if(d.cR / MX_TB + 1 > 65535) return HEFF_BAD_SHAPE;
     dim3 grid((unsigned)cdiv(d.cL, MX_TA), (unsigned)cdiv(d.cR, MX_TB));
-    mix_mixed_kernel<CPLX><<<grid, MX_THREADS, mix_smem, s>>>(m->T1, reinterpret_cast<const T *>(op->W), m->A2, (int)d.S, (int)d.cL, (int)d.cR,
-                                                             (int)d.DL, (int)d.DR, m->M1, m->N1, m->Kp2, m->Kx2);
+    mix_mixed_kernel<CPLX><<<grid, MX_THREADS, mix_smem, s>>>(m->T1, m->wl, m->wl_bytes, m->A2, (int)d.S, (int)d.cL, (int)d.cR, (int)d.DL,
+                                                             (int)d.DR, m->M1, m->N1, m->Kp2, m->Kx2);
     HEFF_LAUNCH_CHECK();
     XGemmArgs g2{};
     g2.M = (int)m->M2, g2.N = (int)(cf * m->N2), g2.K = (int)m->Kx2, g2.C = y, g2.ldc = m->M2, g2.err = m->err;

@@ -56,4 +56,44 @@ __device__ void build_wlist(const T *sW, int DL, int DR, int S, unsigned char *m
     __syncthreads();
 }
 
+// The same list written by one thread (for a list built once and copied by every CTA of a kernel).
+template<class T>
+__device__ void build_wlist_serial(const T *W, int DL, int DR, int S, unsigned char *mem) {
+    const int    NO  = DR * S;
+    const size_t nnz = (size_t)DL * DR * S * S;
+    auto         al  = [](size_t b) { return (b + 15) / 16 * 16; };
+    int         *off = reinterpret_cast<int *>(mem);
+    short       *idx = reinterpret_cast<short *>(mem + al(4 * (NO + 1)));
+    T           *wv  = reinterpret_cast<T *>(mem + al(4 * (NO + 1)) + al(2 * nnz));
+    int          e   = 0;
+    for(int o = 0; o < NO; o++) {
+        const int n = o / S, sp = o % S;
+        off[o]      = e;
+        for(int s = 0; s < S; s++)
+            for(int m = 0; m < DL; m++) {
+                const T w = W[m + DL * (n + DR * (s + S * sp))];
+                if(wl_nz(w)) {
+                    idx[e] = (short)(m * S + s);
+                    wv[e]  = w;
+                    e++;
+                }
+            }
+    }
+    off[NO] = e;
+}
+template<class T>
+__global__ void wlist_global_kernel(const T *W, int DL, int DR, int S, unsigned char *out) {
+    if(threadIdx.x == 0 && blockIdx.x == 0) build_wlist_serial(W, DL, DR, S, out);
+}
+// Views of a list block laid out as above.
+template<class T>
+__device__ __forceinline__ void wlist_views(unsigned char *mem, int DL, int DR, int S, int *&off, short *&idx, T *&wv) {
+    const int    NO  = DR * S;
+    const size_t nnz = (size_t)DL * DR * S * S;
+    auto         al  = [](size_t b) { return (b + 15) / 16 * 16; };
+    off              = reinterpret_cast<int *>(mem);
+    idx              = reinterpret_cast<short *>(mem + al(4 * (NO + 1)));
+    wv               = reinterpret_cast<T *>(mem + al(4 * (NO + 1)) + al(2 * nnz));
+}
+
 }  // namespace heff
