@@ -23,7 +23,7 @@ struct EmuState {
     void   *buf = nullptr;
     size_t  cap = 0;
     int64_t rmax_cap = 0;  // rows of T2 the accumulators cover
-    int    *err = nullptr;
+    int    *err = nullptr;  // [0] sticky status; bad words of [1] x', [2] T2 (cleared per apply), [3] L, [4] R' (per slicing)
     ZPlanes A1, B1, A2, B2;
 };
 
@@ -157,31 +157,34 @@ static int emu_apply_impl(heff_op *op, const void *xv, void *yv) {
     const int     ns = op->emu_slices;
     cudaStream_t  s  = op->stream;
     const double  a_extra = 1.0 / 4096.0;  // the 2^-12 of the two leading digits' units, carried by the A side
+    int *err = st->err;
     if(op->emu_stale) {  // operator-side planes: L (A of G1) and R' (B of G2)
         const T *L = reinterpret_cast<const T *>(op->L), *Rp = reinterpret_cast<const T *>(op->Rp);
-        HEFF_TRY(z_scale_kmajor<CPLX>(L, e.M1, e.K1, e.K1, a_extra, st->A1, st->err, s));
-        HEFF_TRY(z_slice_kmajor<CPLX>(L, e.M1, e.K1, e.K1, false, st->A1, st->err, s));
-        HEFF_TRY(z_scale_kmajor<CPLX>(Rp, e.N2, e.K2, e.K2, 1.0, st->B2, st->err, s));
-        HEFF_TRY(z_slice_kmajor<CPLX>(Rp, e.N2, e.K2, e.K2, CPLX, st->B2, st->err, s));
+        HEFF_CUDA(cudaMemsetAsync(err + 3, 0, 2 * sizeof(int), s));
+        HEFF_TRY(z_scale_kmajor<CPLX>(L, e.M1, e.K1, e.K1, a_extra, st->A1, err + 3, s));
+        HEFF_TRY(z_slice_kmajor<CPLX>(L, e.M1, e.K1, e.K1, false, st->A1, err + 3, s));
+        HEFF_TRY(z_scale_kmajor<CPLX>(Rp, e.N2, e.K2, e.K2, 1.0, st->B2, err + 4, s));
+        HEFF_TRY(z_slice_kmajor<CPLX>(Rp, e.N2, e.K2, e.K2, CPLX, st->B2, err + 4, s));
         op->emu_stale = false;
     }
+    HEFF_CUDA(cudaMemsetAsync(err + 1, 0, 2 * sizeof(int), s));  // this apply's operands start clean
     MatvecScratch<CPLX> ws;
     ws.carve(reinterpret_cast<T *>(op->scratch), d);
     const T *x = reinterpret_cast<const T *>(xv);
     T       *y = reinterpret_cast<T *>(yv);
     HEFF_TRY(permute_mps<CPLX>(d, x, ws.xp, s));
-    HEFF_TRY(z_scale_kmajor<CPLX>(ws.xp, e.N1, e.K1, e.K1, 1.0, st->B1, st->err, s));
-    HEFF_TRY(z_slice_kmajor<CPLX>(ws.xp, e.N1, e.K1, e.K1, CPLX, st->B1, st->err, s));
+    HEFF_TRY(z_scale_kmajor<CPLX>(ws.xp, e.N1, e.K1, e.K1, 1.0, st->B1, err + 1, s));
+    HEFF_TRY(z_slice_kmajor<CPLX>(ws.xp, e.N1, e.K1, e.K1, CPLX, st->B1, err + 1, s));
     ZGemmArgs g1{};
     g1.M = (int)e.M1, g1.N = (int)(e.cf * e.N1), g1.K = (int)e.kx1, g1.nslice = ns, g1.fa = st->A1.fac, g1.fb = st->B1.fac;
-    g1.C = ws.T1, g1.ldc = e.M1, g1.cplx = CPLX, g1.err = st->err;
+    g1.C = ws.T1, g1.ldc = e.M1, g1.cplx = CPLX, g1.err = err, g1.bad_a = err + 3, g1.bad_b = err + 1;
     HEFF_TRY(gemm_i8_ozaki(st->A1, st->B1, g1, s));
     HEFF_TRY(mix_fp64<CPLX>(d, ws.T1, ws.T2, reinterpret_cast<const T *>(op->W), s));
-    HEFF_TRY(z_scale_mmajor<CPLX>(ws.T2, e.M2, e.K2, e.M2, a_extra, st->A2, st->err, s));
-    HEFF_TRY(z_slice_mmajor<CPLX>(ws.T2, e.M2, e.K2, e.M2, st->A2, st->err, s));
+    HEFF_TRY(z_scale_mmajor<CPLX>(ws.T2, e.M2, e.K2, e.M2, a_extra, st->A2, err + 2, s));
+    HEFF_TRY(z_slice_mmajor<CPLX>(ws.T2, e.M2, e.K2, e.M2, st->A2, err + 2, s));
     ZGemmArgs g2{};
     g2.M = (int)e.M2, g2.N = (int)(e.cf * e.N2), g2.K = (int)e.kx2, g2.nslice = ns, g2.fa = st->A2.fac, g2.fb = st->B2.fac;
-    g2.C = y, g2.ldc = e.M2, g2.cplx = CPLX, g2.err = st->err;
+    g2.C = y, g2.ldc = e.M2, g2.cplx = CPLX, g2.err = err, g2.bad_a = err + 2, g2.bad_b = err + 4;
     HEFF_TRY(gemm_i8_ozaki(st->A2, st->B2, g2, s));
     op->num_mv++;
     return HEFF_OK;

@@ -24,13 +24,14 @@ __device__ __forceinline__ double z_im(double2 v) { return v.y; }
 
 // sigma_r = 2^(Es - 1023), the smallest power of two above the row maximum mx (>= 0), at least 2^-1016 (an
 // all-zero row takes sigma = 1).  inv = 64 / sigma_r and fac = sigma_r * extra are exact powers of two.  A
-// maximum of 2^1022 or more (or inf) is out of range: the error flag is raised (code 5) and the row clamped.
-__device__ __forceinline__ void z_set_scale(double mx, double extra, double *inv, double *fac, int *err) {
+// maximum of 2^1022 or more (or inf) is out of range: the operand's bad word is raised and the row clamped
+// (the GEMM then writes NaN, as an FP64 product of such an input would).
+__device__ __forceinline__ void z_set_scale(double mx, double extra, double *inv, double *fac, int *bad) {
     const unsigned long long b = (unsigned long long)__double_as_longlong(mx);
     int                      Es = mx == 0.0 ? 1023 : (int)((b >> 52) & 0x7ff) + 1;
     if(Es < 7) Es = 7;
     if(Es > 2045) {
-        atomicExch(err, 5);
+        atomicExch(bad, 1);
         Es = 2045;
     }
     *inv = __longlong_as_double((long long)((unsigned long long)(2052 - Es) << 52));
@@ -40,7 +41,7 @@ __device__ __forceinline__ void z_set_scale(double mx, double extra, double *inv
 // one warp per row of a K-major source
 template<bool CPLX>
 __global__ void z_scale_k_kernel(const typename Scalar<CPLX>::T *__restrict__ src, int64_t rows, int64_t K, int64_t ld, double extra,
-                                 double *__restrict__ inv, double *__restrict__ fac, int *err) {
+                                 double *__restrict__ inv, double *__restrict__ fac, int *bad) {
     const int     lane = threadIdx.x & 31;
     const int64_t nw   = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for(int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += nw) {
@@ -53,7 +54,7 @@ __global__ void z_scale_k_kernel(const typename Scalar<CPLX>::T *__restrict__ sr
         }
 #pragma unroll
         for(int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if(lane == 0) z_set_scale(m, extra, inv + r, fac + r, err);
+        if(lane == 0) z_set_scale(m, extra, inv + r, fac + r, bad);
     }
 }
 
@@ -73,11 +74,11 @@ __global__ void z_rowmax_m_kernel(const typename Scalar<CPLX>::T *__restrict__ s
     }
     if(m > 0.0) atomicMax(rmax + r, (unsigned long long)__double_as_longlong(m));
 }
-__global__ void z_rowmax_fin_kernel(unsigned long long *rmax, int64_t rows, double extra, double *inv, double *fac, int *err) {
+__global__ void z_rowmax_fin_kernel(unsigned long long *rmax, int64_t rows, double extra, double *inv, double *fac, int *bad) {
     for(int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
         const double m = __longlong_as_double((long long)rmax[r]);
         rmax[r]        = 0ull;  // ready for the next use
-        z_set_scale(m, extra, inv + r, fac + r, err);
+        z_set_scale(m, extra, inv + r, fac + r, bad);
     }
 }
 
@@ -109,8 +110,8 @@ __device__ __forceinline__ bool z_bad16(const double (&y)[16]) {
 // Writes the ns digit planes of a 16-column group g of source row r (yr, yi already scaled by 64 / sigma_r).
 template<bool CPLX, bool BMODE>
 __device__ __forceinline__ void z_emit(double (&yr)[16], double (&yi)[16], int8_t *planes, int64_t plane, int64_t kx, int64_t Kh, int64_t r,
-                                       int64_t g, int ns, int *err) {
-    if(z_bad16(yr) || (CPLX && z_bad16(yi))) atomicExch(err, 5);
+                                       int64_t g, int ns, int *bad) {
+    if(z_bad16(yr) || (CPLX && z_bad16(yi))) atomicExch(bad, 1);
     for(int t = 0; t < ns; t++) {
         uint32_t wr[4], wnr[4], wi[4], wni[4];
         z_digits16(yr, wr, wnr);
@@ -136,7 +137,7 @@ __device__ __forceinline__ void z_emit(double (&yr)[16], double (&yi)[16], int8_
 template<bool CPLX, bool BMODE>
 __global__ void __launch_bounds__(256) z_slice_k_kernel(const typename Scalar<CPLX>::T *__restrict__ src, int64_t rows, int64_t K, int64_t ld,
                                                          const double *__restrict__ inv, int8_t *__restrict__ planes, int64_t prow, int64_t kx, int ns,
-                                                         int *err) {
+                                                         int *bad) {
     const int64_t ng = (K + 15) / 16, Kh = ng * 16, tot = rows * ng, plane = prow * kx;
     for(int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t g = e % ng, r = e / ng;
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(256) z_slice_k_kernel(const typename Scalar<CP
                 yi[j]        = z_im(v) * sc;
             }
         }
-        z_emit<CPLX, BMODE>(yr, yi, planes, plane, kx, Kh, r, g, ns, err);
+        z_emit<CPLX, BMODE>(yr, yi, planes, plane, kx, Kh, r, g, ns, bad);
     }
 }
 
@@ -163,7 +164,7 @@ constexpr int ZM_TR = 32, ZM_TK = 64, ZM_THREADS = ZM_TR * ZM_TK / 16;
 template<bool CPLX>
 __global__ void __launch_bounds__(ZM_THREADS) z_slice_m_kernel(const typename Scalar<CPLX>::T *__restrict__ src, int64_t rows, int64_t K,
                                                                 int64_t ld, const double *__restrict__ inv, int8_t *__restrict__ planes, int64_t kx,
-                                                                int ns, int *err) {
+                                                                int ns, int *bad) {
     using T = typename Scalar<CPLX>::T;
     __shared__ T  tile[ZM_TK][ZM_TR + 1];
     const int64_t ng = (K + 15) / 16, Kh = ng * 16, plane = rows * kx;
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(ZM_THREADS) z_slice_m_kernel(const typename Sc
         yr[j]     = z_re(v) * sc;
         yi[j]     = z_im(v) * sc;
     }
-    z_emit<CPLX, false>(yr, yi, planes, plane, kx, Kh, r, g, ns, err);
+    z_emit<CPLX, false>(yr, yi, planes, plane, kx, Kh, r, g, ns, bad);
 }
 
 static int z_grid(int64_t n, int per_block = 256) {
@@ -200,15 +201,15 @@ static int z_grid(int64_t n, int per_block = 256) {
 }
 
 template<bool CPLX>
-int z_scale_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *err, cudaStream_t s) {
+int z_scale_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *bad, cudaStream_t s) {
     if(rows <= 0) return HEFF_OK;
-    z_scale_k_kernel<CPLX><<<z_grid(rows * 32), 256, 0, s>>>(src, rows, K, ld, extra, p.inv, p.fac, err);
+    z_scale_k_kernel<CPLX><<<z_grid(rows * 32), 256, 0, s>>>(src, rows, K, ld, extra, p.inv, p.fac, bad);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }
 
 template<bool CPLX>
-int z_scale_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *err, cudaStream_t s) {
+int z_scale_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *bad, cudaStream_t s) {
     if(rows <= 0) return HEFF_OK;
     const int64_t rb      = cdiv(rows, 256);
     const int64_t nchunks = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(K, 65535), (int64_t)device_sm_count() * 8 / rb));
@@ -216,29 +217,29 @@ int z_scale_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K,
     if(rb > 0x7fffffff) return HEFF_BAD_SHAPE;
     z_rowmax_m_kernel<CPLX><<<dim3((unsigned)rb, (unsigned)cdiv(K, kchunk)), 256, 0, s>>>(src, rows, K, ld, kchunk, p.rmax);
     HEFF_LAUNCH_CHECK();
-    z_rowmax_fin_kernel<<<z_grid(rows), 256, 0, s>>>(p.rmax, rows, extra, p.inv, p.fac, err);
+    z_rowmax_fin_kernel<<<z_grid(rows), 256, 0, s>>>(p.rmax, rows, extra, p.inv, p.fac, bad);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }
 
 template<bool CPLX>
-int z_slice_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, bool bmode, const ZPlanes &p, int *err, cudaStream_t s) {
+int z_slice_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, bool bmode, const ZPlanes &p, int *bad, cudaStream_t s) {
     if(rows <= 0) return HEFF_OK;
     const int64_t tot = rows * cdiv(K, 16);
     if(CPLX && bmode)
-        z_slice_k_kernel<CPLX, true><<<z_grid(tot), 256, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.rows, p.kx, p.nslice, err);
+        z_slice_k_kernel<CPLX, true><<<z_grid(tot), 256, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.rows, p.kx, p.nslice, bad);
     else
-        z_slice_k_kernel<CPLX, false><<<z_grid(tot), 256, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.rows, p.kx, p.nslice, err);
+        z_slice_k_kernel<CPLX, false><<<z_grid(tot), 256, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.rows, p.kx, p.nslice, bad);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }
 
 template<bool CPLX>
-int z_slice_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, const ZPlanes &p, int *err, cudaStream_t s) {
+int z_slice_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, const ZPlanes &p, int *bad, cudaStream_t s) {
     if(rows <= 0) return HEFF_OK;
     const int64_t gx = cdiv(rows, ZM_TR), gy = cdiv(K, ZM_TK);
     if(gx > 0x7fffffff || gy > 65535) return HEFF_BAD_SHAPE;
-    z_slice_m_kernel<CPLX><<<dim3((unsigned)gx, (unsigned)gy), ZM_THREADS, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.kx, p.nslice, err);
+    z_slice_m_kernel<CPLX><<<dim3((unsigned)gx, (unsigned)gy), ZM_THREADS, 0, s>>>(src, rows, K, ld, p.inv, p.planes, p.kx, p.nslice, bad);
     HEFF_LAUNCH_CHECK();
     return HEFF_OK;
 }
@@ -286,12 +287,14 @@ __device__ __forceinline__ void z_tile_mn(const ZGemmArgs &p, int tile, int &m0,
 
 // Level g of tile (m0, n0) from TMEM columns [col0, col0 + BN) into C: the first level processed (g = s-1)
 // stores, the others add.  All loads of a 32-column chunk are issued before its stores.
+__device__ __forceinline__ double z_nan() { return __longlong_as_double(0x7ff8000000000000ll); }
+
 template<int BN>
-__device__ __forceinline__ void z_epilogue(const ZGemmArgs &p, uint32_t tmem_row, int row, int n0, int g) {
+__device__ __forceinline__ void z_epilogue(const ZGemmArgs &p, uint32_t tmem_row, int row, int n0, int g, bool poison) {
     const bool first = g == p.nslice - 1;
     double     lv    = 1.0;
     for(int i = 0; i < g; i++) lv *= 0.0078125;  // 2^-7g, exact
-    const double ra = row < p.M ? p.fa[row] * lv : 0.0;
+    const double ra = row < p.M ? (poison ? z_nan() : p.fa[row] * lv) : 0.0;
     for(int c = 0; c < BN; c += 32) {
         uint32_t r[32];
         tmem_ld32(tmem_row + (uint32_t)c, r);
@@ -345,11 +348,11 @@ __device__ __forceinline__ void z_epilogue(const ZGemmArgs &p, uint32_t tmem_row
 // tacc, FP64 partial at tpart (column pairs lo, hi); the same FP64 operations in the same order as z_epilogue,
 // so both give identical results.  The last level (g = 0) writes C once.
 template<int BN>
-__device__ __forceinline__ void z_epilogue_tsum(const ZGemmArgs &p, uint32_t tacc, uint32_t tpart, int row, int n0, int g) {
+__device__ __forceinline__ void z_epilogue_tsum(const ZGemmArgs &p, uint32_t tacc, uint32_t tpart, int row, int n0, int g, bool poison) {
     const bool first = g == p.nslice - 1, last = g == 0;
     double     lv    = 1.0;
     for(int i = 0; i < g; i++) lv *= 0.0078125;  // 2^-7g, exact
-    const double ra = row < p.M ? p.fa[row] * lv : 0.0;
+    const double ra = row < p.M ? (poison ? z_nan() : p.fa[row] * lv) : 0.0;
     for(int c = 0; c < BN; c += 32) {
         uint32_t r[32];
         tmem_ld32(tacc + (uint32_t)c, r);
@@ -501,9 +504,11 @@ __global__ void __launch_bounds__(Z_THREADS, 1)
         }
     } else {
         // epilogue: warps 2..5 -> TMEM lane quarters 2,3,0,1
-        const int q    = warp & 3;
-        int       j    = 0;
-        bool      stop = false;
+        const int  q      = warp & 3;
+        int        j      = 0;
+        bool       stop   = false;
+        const bool poison = (*p.bad_a | *p.bad_b) != 0;  // raised by the slicers, which ran before this kernel
+        if(poison && threadIdx.x == 64) atomicExch(p.err, 5);
         for(int t = blockIdx.x; t < ntiles && !stop; t += gridDim.x) {
             int m0, n0;
             z_tile_mn<BN>(p, t, m0, n0);
@@ -521,9 +526,9 @@ __global__ void __launch_bounds__(Z_THREADS, 1)
                 fence_after();
                 const uint32_t trow = tmem_base + ((uint32_t)(q * 32) << 16);
                 if constexpr(ZCfg<BN>::TMEM_SUM)
-                    z_epilogue_tsum<BN>(p, trow + (uint32_t)(buf * BN), trow + (uint32_t)ZCfg<BN>::PART_COL, m0 + q * 32 + lane, n0, g);
+                    z_epilogue_tsum<BN>(p, trow + (uint32_t)(buf * BN), trow + (uint32_t)ZCfg<BN>::PART_COL, m0 + q * 32 + lane, n0, g, poison);
                 else
-                    z_epilogue<BN>(p, trow + (uint32_t)(buf * BN), m0 + q * 32 + lane, n0, g);
+                    z_epilogue<BN>(p, trow + (uint32_t)(buf * BN), m0 + q * 32 + lane, n0, g, poison);
                 fence_before();
                 mbar_arrive(&acc_empty[buf]);  // TMEM buffer free for the unit after next
                 epi_bar();                     // *s_fail is read by all before the next wait may set it
@@ -629,6 +634,7 @@ int gemm_i8_ozaki(const ZPlanes &A, const ZPlanes &B, const ZGemmArgs &a, cudaSt
     if(a.M <= 0 || a.N <= 0) return HEFF_OK;
     if(a.K <= 0 || a.K % 16 || a.nslice < 1 || a.nslice > Z_MAX_SLICES || !z_k_ok(a.K, a.nslice) || (a.cplx && a.N % 2)) return HEFF_BAD_ARG;
     if(A.kx != a.K || B.kx != a.K || A.rows < a.M || B.rows < a.N || A.nslice < a.nslice || B.nslice < a.nslice) return HEFF_BAD_ARG;
+    if(!a.err || !a.bad_a || !a.bad_b) return HEFF_BAD_ARG;
     const int   bn = z_choose_bn(a.M, a.N, a.K);
     CUtensorMap tA, tB;
     HEFF_TRY(make_tmap_planes(&tA, A, Z_BM));
@@ -662,15 +668,16 @@ static int gemm_emu_impl(const void *Av, const void *Bv, void *C, int64_t M, int
     pb.planes = reinterpret_cast<int8_t *>(w + bPA), pb.rows = cf * N, pb.kx = kx, pb.nslice = ns;
     double *sc = reinterpret_cast<double *>(w + bPA + bPB);
     pa.inv = sc, pa.fac = sc + M, pb.inv = sc + 2 * M, pb.fac = sc + 2 * M + N;
-    int *err = reinterpret_cast<int *>(w + bPA + bPB + bS);
-    HEFF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    int *err = reinterpret_cast<int *>(w + bPA + bPB + bS);  // err, bad word of A, bad word of B
+    HEFF_CUDA(cudaMemsetAsync(err, 0, 3 * sizeof(int), s));
     const T *A = reinterpret_cast<const T *>(Av), *B = reinterpret_cast<const T *>(Bv);
-    HEFF_TRY(z_scale_kmajor<CPLX>(A, M, K, K, 1.0 / 4096.0, pa, err, s));
-    HEFF_TRY(z_scale_kmajor<CPLX>(B, N, K, K, 1.0, pb, err, s));
-    HEFF_TRY(z_slice_kmajor<CPLX>(A, M, K, K, false, pa, err, s));
-    HEFF_TRY(z_slice_kmajor<CPLX>(B, N, K, K, true, pb, err, s));
+    HEFF_TRY(z_scale_kmajor<CPLX>(A, M, K, K, 1.0 / 4096.0, pa, err + 1, s));
+    HEFF_TRY(z_scale_kmajor<CPLX>(B, N, K, K, 1.0, pb, err + 2, s));
+    HEFF_TRY(z_slice_kmajor<CPLX>(A, M, K, K, false, pa, err + 1, s));
+    HEFF_TRY(z_slice_kmajor<CPLX>(B, N, K, K, true, pb, err + 2, s));
     ZGemmArgs g{};
     g.M = (int)M, g.N = (int)(cf * N), g.K = (int)kx, g.nslice = ns, g.fa = pa.fac, g.fb = pb.fac, g.C = C, g.ldc = M, g.cplx = CPLX, g.err = err;
+    g.bad_a = err + 1, g.bad_b = err + 2;
     HEFF_TRY(gemm_i8_ozaki(pa, pb, g, s));
     int h = 0;
     HEFF_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -64,7 +64,8 @@ struct ZGemmArgs {
     void         *C;
     int64_t       ldc;      // column-major C: real C[m + ldc n]; complex C[m + ldc (n'/2)] (re, im) from B' rows n', n'+1
     int           cplx;
-    int          *err;
+    int          *err;           // sticky status: 1-4 a pipeline wait timed out, 5 an input was non-finite
+    const int    *bad_a, *bad_b;  // the operands' bad words (raised by their slicers); either set: C is NaN
 };
 
 // 3D tensor map over digit planes {kx, rows, nslice}, box {128, box_rows, 1}, 128-byte swizzle.
@@ -72,19 +73,20 @@ int make_tmap_planes(CUtensorMap *map, const ZPlanes &p, int box_rows);
 // Tile width for a C' of M x N over K' (fewest waves on the device's SMs, weighted by measured per-MAC costs).
 int z_choose_bn(int64_t M, int64_t N, int64_t K);
 
+// The slicers raise *bad (an int the caller clears) for a non-finite entry or one of magnitude >= 2^1022.
 // Row scales of a K-major source src[r * ld + k] (k < K): inv, fac (fac = sigma * extra).
 template<bool CPLX>
-int z_scale_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *err, cudaStream_t s);
+int z_scale_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *bad, cudaStream_t s);
 // Row scales of an M-major source src[r + ld * k] (uses p.rmax, left zeroed).
 template<bool CPLX>
-int z_scale_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *err, cudaStream_t s);
+int z_scale_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, double extra, ZPlanes &p, int *bad, cudaStream_t s);
 // Digit planes from a K-major source.  bmode (complex only): rows 2r = [re | -im], 2r+1 = [im | re];
 // otherwise row r = [re | im] (complex) or [v] (real); each half is round16(K) wide.
 template<bool CPLX>
-int z_slice_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, bool bmode, const ZPlanes &p, int *err, cudaStream_t s);
+int z_slice_kmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, bool bmode, const ZPlanes &p, int *bad, cudaStream_t s);
 // Digit planes (A-mode) from an M-major source src[r + ld * k].
 template<bool CPLX>
-int z_slice_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, const ZPlanes &p, int *err, cudaStream_t s);
+int z_slice_mmajor(const typename Scalar<CPLX>::T *src, int64_t rows, int64_t K, int64_t ld, const ZPlanes &p, int *bad, cudaStream_t s);
 
 // Plane row pitch for K source columns: round16(K), doubled for complex.
 inline int64_t z_kx(int64_t K, bool cplx) { return ((K + 15) / 16 * 16) * (cplx ? 2 : 1); }

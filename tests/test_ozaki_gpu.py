@@ -120,11 +120,15 @@ def test_i8_emu_rejects_nonfinite(cuda):
     A = torch.randn(64, 32, device="cuda", dtype=torch.float64)
     B = torch.randn(48, 32, device="cuda", dtype=torch.float64)
     A[5, 7] = float("nan")
-    rc, _ = emu(A, B)
+    rc, C = emu(A, B)
     assert rc == 2  # HEFF_NAN_INPUT
+    assert bool(torch.isnan(C).all())  # no finite garbage: the product is NaN, as an FP64 product would be
     A[5, 7] = float("inf")
-    rc, _ = emu(A, B)
-    assert rc == 2
+    rc, C = emu(A, B)
+    assert rc == 2 and bool(torch.isnan(C).all())
+    A[5, 7] = 1.0
+    rc, C = emu(A, B)  # a clean call after the bad ones
+    assert rc == 0 and rel(C, A @ B.T) < 5e-13
 
 
 def test_i8_emu_rejects_long_k(cuda):
@@ -200,4 +204,22 @@ def test_int8_engine_slices_and_invalid_args(cuda):
     assert errs[8] < errs[7] < 1e-12 < errs[4]
     assert hb.lib().heff_op_set_fp64_engine(op.handle, 2, 0) == 7  # HEFF_BAD_ARG
     assert hb.lib().heff_op_set_fp64_engine(op.handle, 1, 9) == 7
+    op.close()
+
+
+@pytest.mark.parametrize("c", [False, True])
+def test_int8_engine_nonfinite_input_gives_nan(cuda, c):
+    """A NaN in theta makes the INT8-engine matvec NaN (like the DMMA path) instead of a finite wrong answer; the next
+    clean matvec is correct again, and the operator's device status records the event (5)."""
+    th, W, L, R = ph.heff_inputs(40, D=3, cplx=c, seed=8)
+    op = hb.MatVecMPOS([W], L, R, cplx=c)
+    op.set_fp64_engine(hb.FP64_INT8)
+    bad = th.copy()
+    bad[1, 3, 5] = np.nan
+    y = op.MultAx_host(bad)
+    assert np.isnan(y).any()
+    y2 = op.MultAx_host(th)
+    assert relerr(y2, rn.matvec_blas(th, W, L, R)) < 1e-12
+    code = ctypes.c_int(-1)
+    assert hb.lib().heff_op_device_error(op.handle, ctypes.byref(code)) == 0 and code.value == 5
     op.close()
