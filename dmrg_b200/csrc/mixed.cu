@@ -150,47 +150,77 @@ __global__ void __launch_bounds__(256) split_x_kernel(const typename Scalar<CPLX
     }
 }
 
-// MIX: tile of 16 a' x 32 b.  Load phase a'-fastest (coalesced T1 reads) into shared memory; compute
-// phase b-fastest so the split T2 segments are written contiguously along k = b + cR*n.
-constexpr int MX_TA = 16, MX_TB = 32, MX_THREADS = MX_TA * MX_TB;
-constexpr int MX_SSTR = MX_TA * (MX_TB + 1);  // floats per staged (m, s) slice: a' rows padded to MX_TB + 1
+// Two adjacent outputs k, k+1 (k even, Kp even) of every A'-segment as bf16 pairs (4-byte stores).
 template<bool CPLX>
-__global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__restrict__ T1, const unsigned char *__restrict__ wl, int wl_bytes,
-                                                              __nv_bfloat16 *__restrict__ A2, int S, int cL, int cR, int DL, int DR, int64_t M1,
-                                                              int64_t N1, int64_t Kp2, int64_t Kx2) {
-    using T = typename Scalar<CPLX>::T;
+__device__ __forceinline__ void put_A_pair(__nv_bfloat16 *dst, int64_t Kp, int64_t k, double re0, double im0, double re1, double im1) {
+    __nv_bfloat16 h0, m0, h1, m1;
+    auto          st2 = [&](int64_t off, __nv_bfloat16 a, __nv_bfloat16 b) {
+        *reinterpret_cast<__nv_bfloat162 *>(dst + off) = __halves2bfloat162(a, b);
+    };
+    split2(re0, h0, m0);
+    split2(re1, h1, m1);
+    st2(k, h0, h1);
+    st2(Kp + k, h0, h1);
+    st2(2 * Kp + k, m0, m1);
+    if constexpr(CPLX) {
+        split2(im0, h0, m0);
+        split2(im1, h1, m1);
+        st2(3 * Kp + k, h0, h1);
+        st2(4 * Kp + k, h0, h1);
+        st2(5 * Kp + k, m0, m1);
+    }
+}
+
+// MIX: tile of TA a' x 64 b, 32*TA threads.  Load phase a'-fastest (coalesced T1 reads) into shared memory;
+// compute phase: each thread two adjacent b, so the split T2 segments are written as bf16 pairs, contiguous
+// along k = b + cR*n across the warp.  Staged rows of 64 b are padded to 66 floats: the a'-fastest stores hit
+// distinct banks and the float2 reads of the compute phase are aligned and conflict-free.
+constexpr int MX_TB = 64, MX_ROW = MX_TB + 2;
+template<int TA>
+constexpr int mx_sstr() {
+    return TA * MX_ROW;  // floats per staged (m, s) slice
+}
+template<bool CPLX, int TA>
+__global__ void __launch_bounds__(32 * TA) mix_mixed_kernel(const float *__restrict__ T1, const unsigned char *__restrict__ wl, int wl_bytes,
+                                                           __nv_bfloat16 *__restrict__ A2, int S, int cL, int cR, int DL, int DR, int64_t M1,
+                                                           int64_t N1, int64_t Kp2, int64_t Kx2) {
+    using T                 = typename Scalar<CPLX>::T;
+    constexpr int SSTR      = mx_sstr<TA>();
+    constexpr int NTHREADS  = 32 * TA;
     extern __shared__ __align__(16) unsigned char mxs[];
     float *sRe = reinterpret_cast<float *>(mxs);
     const int NP = DL * S;
-    float *sIm = sRe + NP * MX_SSTR;
-    unsigned char *lmem = reinterpret_cast<unsigned char *>(sIm + (CPLX ? NP * MX_SSTR : 0));
+    float *sIm = sRe + NP * SSTR;
+    unsigned char *lmem = reinterpret_cast<unsigned char *>(sIm + (CPLX ? NP * SSTR : 0));
     // the MPO's nonzero list (built once per operator) lands in shared memory with the T1 tile, under the same barrier
-    for(int i = threadIdx.x; i < wl_bytes / 16; i += blockDim.x) reinterpret_cast<uint4 *>(lmem)[i] = reinterpret_cast<const uint4 *>(wl)[i];
-    const int a0 = blockIdx.x * MX_TA, b0 = blockIdx.y * MX_TB;
+    for(int i = threadIdx.x; i < wl_bytes / 16; i += NTHREADS) reinterpret_cast<uint4 *>(lmem)[i] = reinterpret_cast<const uint4 *>(wl)[i];
+    const int a0 = blockIdx.x * TA, b0 = blockIdx.y * MX_TB;
     {
-        // a'-fastest loads (coalesced along T1's rows), 8 in flight per thread; the staging row stride
-        // MX_TB + 1 keeps both this a'-fastest store and the b-fastest reads below free of bank conflicts
-        const int  al = threadIdx.x % MX_TA, bl = threadIdx.x / MX_TA;
-        const int  ap = a0 + al, b = b0 + bl;
-        const bool ok = ap < cL && b < cR;
-        for(int ms0 = 0; ms0 < NP; ms0 += 8) {
-            float vr[8], vi[8];
+        // a'-fastest loads (coalesced along T1's rows), 8 in flight per thread, two halves of the b range
+        const int al = threadIdx.x % TA, bl = threadIdx.x / TA;  // bl < 32
+        const int ap = a0 + al;
+        for(int h = 0; h < 2; h++) {
+            const int  b  = b0 + bl + 32 * h;
+            const bool ok = ap < cL && b < cR;
+            for(int ms0 = 0; ms0 < NP; ms0 += 8) {
+                float vr[8], vi[8];
 #pragma unroll
-            for(int u = 0; u < 8; u++) {
-                const int ms = ms0 + u, m = ms / S, s = ms % S;
-                vr[u] = vi[u] = 0.f;
-                if(ok && ms < NP) {
-                    const int64_t idx = (ap + (int64_t)cL * m) + M1 * (s + (int64_t)S * b);
-                    vr[u]             = T1[idx];
-                    if(CPLX) vi[u] = T1[idx + M1 * N1];
+                for(int u = 0; u < 8; u++) {
+                    const int ms = ms0 + u, m = ms / S, s = ms % S;
+                    vr[u] = vi[u] = 0.f;
+                    if(ok && ms < NP) {
+                        const int64_t idx = (ap + (int64_t)cL * m) + M1 * (s + (int64_t)S * b);
+                        vr[u]             = T1[idx];
+                        if(CPLX) vi[u] = T1[idx + M1 * N1];
+                    }
                 }
+#pragma unroll
+                for(int u = 0; u < 8; u++)
+                    if(ms0 + u < NP) {
+                        sRe[(ms0 + u) * SSTR + al * MX_ROW + bl + 32 * h] = vr[u];
+                        if(CPLX) sIm[(ms0 + u) * SSTR + al * MX_ROW + bl + 32 * h] = vi[u];
+                    }
             }
-#pragma unroll
-            for(int u = 0; u < 8; u++)
-                if(ms0 + u < NP) {
-                    sRe[(ms0 + u) * MX_SSTR + al * (MX_TB + 1) + bl] = vr[u];
-                    if(CPLX) sIm[(ms0 + u) * MX_SSTR + al * (MX_TB + 1) + bl] = vi[u];
-                }
         }
     }
     __syncthreads();
@@ -198,29 +228,45 @@ __global__ void __launch_bounds__(MX_THREADS) mix_mixed_kernel(const float *__re
     short *idx;
     T     *wv;
     wlist_views(lmem, DL, DR, S, off, idx, wv);
-    const int bl = threadIdx.x % MX_TB, al = threadIdx.x / MX_TB;
-    const int ap = a0 + al, b = b0 + bl;
+    const int bp = threadIdx.x % 32, al = threadIdx.x / 32;
+    const int ap = a0 + al, b = b0 + 2 * bp;
     if(ap >= cL || b >= cR) return;
-    const int me = al * (MX_TB + 1) + bl;
+    const bool second = b + 1 < cR;
+    const bool paired = second && (cR % 2 == 0);  // k = b + cR*n even for every n
+    const int  me     = al * MX_ROW + 2 * bp;
     for(int n = 0; n < DR; n++)
         for(int sp = 0; sp < S; sp++) {
-            const int o  = n * S + sp;
-            double    re = 0, im = 0;
+            const int o   = n * S + sp;
+            double    re0 = 0, im0 = 0, re1 = 0, im1 = 0;
             for(int e = off[o]; e < off[o + 1]; e++) {
                 const T      w    = wv[e];
-                const int    slot = idx[e] * MX_SSTR + me;
-                const double xr   = sRe[slot];
+                const int    slot = idx[e] * SSTR + me;
+                const float2 xr   = *reinterpret_cast<const float2 *>(sRe + slot);
                 if constexpr(CPLX) {
-                    const double xi = sIm[slot];
-                    re += w.x * xr - w.y * xi;
-                    im += w.x * xi + w.y * xr;
+                    const float2 xi = *reinterpret_cast<const float2 *>(sIm + slot);
+                    re0 += w.x * xr.x - w.y * xi.x;
+                    im0 += w.x * xi.x + w.y * xr.x;
+                    re1 += w.x * xr.y - w.y * xi.y;
+                    im1 += w.x * xi.y + w.y * xr.y;
                 } else {
-                    re += w * xr;
+                    re0 += w * xr.x;
+                    re1 += w * xr.y;
                 }
             }
             const int64_t row = sp + (int64_t)S * ap, k = b + (int64_t)cR * n;
-            put_A<CPLX>(A2 + row * Kx2, Kp2, k, re, im);
+            if(paired) {
+                put_A_pair<CPLX>(A2 + row * Kx2, Kp2, k, re0, im0, re1, im1);
+            } else {
+                put_A<CPLX>(A2 + row * Kx2, Kp2, k, re0, im0);
+                if(second) put_A<CPLX>(A2 + row * Kx2, Kp2, k + 1, re1, im1);
+            }
         }
+}
+
+// Tile height: 16 a' when the staging fits in ~100 KB (two or more CTAs per SM), else 8.
+static int mx_ta(int64_t NP, int cf) { return (size_t)cf * 4 * NP * mx_sstr<16>() <= 100 * 1024 ? 16 : 8; }
+static size_t mx_smem(int64_t NP, int cf, int ta, int wl_bytes) {
+    return (size_t)cf * 4 * NP * (ta == 16 ? mx_sstr<16>() : mx_sstr<8>()) + (size_t)wl_bytes;
 }
 
 static int g1(int64_t n) {
@@ -300,9 +346,11 @@ static int mixed_setup(heff_op *op) {
     HEFF_TRY(al((void **)&m->wl, (size_t)m->wl_bytes));
     wlist_global_kernel<T><<<1, 32, 0, s>>>(reinterpret_cast<const T *>(op->W), (int)d.DL, (int)d.DR, (int)d.S, m->wl);
     HEFF_LAUNCH_CHECK();
-    const size_t mix_smem = (size_t)cf * 4 * d.DL * d.S * MX_SSTR + (size_t)m->wl_bytes;
+    const int    ta       = mx_ta(d.DL * d.S, cf);
+    const size_t mix_smem = mx_smem(d.DL * d.S, cf, ta, m->wl_bytes);
     if(mix_smem > 200 * 1024) return HEFF_BAD_SHAPE;
-    HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     HEFF_CUDA(cudaStreamSynchronize(s));
     return HEFF_OK;
 }
@@ -324,11 +372,16 @@ static int mixed_apply_impl(heff_op *op, const void *x, void *y) {
     XGemmArgs g1a{};
     g1a.M = (int)m->M1, g1a.N = (int)(cf * m->N1), g1a.K = (int)m->Kx1, g1a.C = m->T1, g1a.ldc = m->M1, g1a.mode = X_OUT_F32, g1a.err = m->err;
     HEFF_TRY(gemm_bf16x(m->tA1, m->tB1, g1a, s));
-    const size_t mix_smem = (size_t)cf * 4 * d.DL * d.S * MX_SSTR + (size_t)m->wl_bytes;
+    const int    mta      = mx_ta(d.DL * d.S, cf);
+    const size_t mix_smem = mx_smem(d.DL * d.S, cf, mta, m->wl_bytes);
     if(d.cR / MX_TB + 1 > 65535) return HEFF_BAD_SHAPE;
-    dim3 grid((unsigned)cdiv(d.cL, MX_TA), (unsigned)cdiv(d.cR, MX_TB));
-    mix_mixed_kernel<CPLX><<<grid, MX_THREADS, mix_smem, s>>>(m->T1, m->wl, m->wl_bytes, m->A2, (int)d.S, (int)d.cL, (int)d.cR, (int)d.DL,
-                                                             (int)d.DR, m->M1, m->N1, m->Kp2, m->Kx2);
+    dim3 grid((unsigned)cdiv(d.cL, mta), (unsigned)cdiv(d.cR, MX_TB));
+    if(mta == 16)
+        mix_mixed_kernel<CPLX, 16><<<grid, 32 * 16, mix_smem, s>>>(m->T1, m->wl, m->wl_bytes, m->A2, (int)d.S, (int)d.cL, (int)d.cR, (int)d.DL,
+                                                                  (int)d.DR, m->M1, m->N1, m->Kp2, m->Kx2);
+    else
+        mix_mixed_kernel<CPLX, 8><<<grid, 32 * 8, mix_smem, s>>>(m->T1, m->wl, m->wl_bytes, m->A2, (int)d.S, (int)d.cL, (int)d.cR, (int)d.DL,
+                                                                (int)d.DR, m->M1, m->N1, m->Kp2, m->Kx2);
     HEFF_LAUNCH_CHECK();
     XGemmArgs g2{};
     g2.M = (int)m->M2, g2.N = (int)(cf * m->N2), g2.K = (int)m->Kx2, g2.C = y, g2.ldc = m->M2, g2.err = m->err;
