@@ -369,21 +369,21 @@ def splitmix_fields(seed, L, lo=0.5, hi=1.5):
 
 
 def measure_ensemble(hb, n, sweeps, nthreads, seed=77):
-    """Bounded sample of the disorder ensemble: L uniform in {12,16,20,24}, chi_max uniform in {32,64}, h_i ~ U[0.5,1.5]
+    """Bounded sample of the disorder ensemble: L uniform in {12,16,20,24}, chi_max uniform in {32,64,128,256}, h_i ~ U[0.5,1.5]
     per realisation seed, real FP64 two-site fDMRG; realisations/s one at a time vs overlapped workers, and the
     largest energy difference between the two runs."""
     rng = np.random.default_rng(seed)
     reals = []
     for i in range(n):
         L = int(rng.choice([12, 16, 20, 24]))
-        chi = int(rng.choice([32, 64]))
+        chi = int(rng.choice([32, 64, 128, 256]))
         reals.append((splitmix_fields(seed * 100003 + i, L), chi, i))
     r1, s1, t1 = hb.ensemble(reals, nthreads=1, sweeps=sweeps)
     rp, sp, tp = hb.ensemble(reals, nthreads=nthreads, sweeps=sweeps)
     dE = max(abs(a["energy"] - b["energy"]) for a, b in zip(r1, rp))
     return {"realisations": n, "sweeps": sweeps, "workers": nthreads, "one_at_a_time_per_s": n / t1, "overlapped_per_s": n / tp,
             "speedup": t1 / tp, "max_abs_dE_between_runs": dE, "ok": int(all(s == 0 for s in s1 + sp)),
-            "workload": "L in {12,16,20,24}, chi_max in {32,64}, two-site fDMRG FP64, random-field Ising h~U[0.5,1.5]"}
+            "workload": "L in {12,16,20,24}, chi_max in {32,64,128,256}, two-site fDMRG FP64, random-field Ising h~U[0.5,1.5]"}
 
 
 def dist_env():
