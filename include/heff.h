@@ -256,7 +256,8 @@ int heff_gemm_bf16_f32(const void *A, const void *B, float *C, int64_t M, int64_
  * so the normwise error is a few 2^-(7*nslices-1) of |A||B| (2^-48 at 7).  No
  * counterpart in the reference (its products are Eigen FP64); exposed so the
  * emulated-FP64 building block can be validated on its own.  Synchronises the
- * stream; HEFF_NAN_INPUT for a non-finite entry (or one of magnitude >= 2^1022),
+ * stream; HEFF_NAN_INPUT for a non-finite entry (or one of magnitude >= 2^1022;
+ * C is then NaN, as an FP64 product would be),
  * HEFF_BAD_SHAPE when K is too long for exact INT32 sums (K' * nslices >= 2^19,
  * K' = round16(K), doubled for complex), HEFF_TIMEOUT if a pipeline wait timed out. */
 int heff_gemm_i8_emu(int dtype, const void *A, const void *B, void *C, int64_t M, int64_t N, int64_t K, int nslices, void *stream);
