@@ -11,17 +11,18 @@
 // The digit products of one level g are folded into the GEMM's K dimension (K' = (g+1) K: slice pairs
 // (t, g-t) one after the other), so a level is one accumulation in TMEM; levels beyond s-1 are dropped
 // (they are below 2^-(7s-1) of the leading term).  The epilogue turns each level's INT32 tile into FP64
-// exactly (an integer times powers of two) and accumulates the levels into C (first level stores, the
-// others add; the tile stays in L2 between its levels).  With s = 7 the products carry 48 bits relative to
+// exactly (an integer times powers of two) and sums the levels smallest first (in TMEM for 128-wide tiles,
+// else in C, which stays in L2 between a tile's levels).  With s = 7 the products carry 48 bits relative to
 // sigma_a sigma_b, i.e. normwise errors of a few 2^-48 -- the same order as an FP64 GEMM's K-dependent bound.
+// A non-finite operand entry raises the operand's bad word in the slicer; the GEMM then writes NaN.
 //
 // Complex operands use a real embedding: A' rows [re | im], B' rows 2n = [re | -im] and 2n+1 = [im | re],
 // so C'[m, 2n] = Re C[m, n] and C'[m, 2n+1] = Im C[m, n] with one real GEMM of K' = 2K.
 //
 // CTA: 192 threads = warp 0 TMA producer, warp 1 TMEM allocator + MMA issuer, warps 2-5 epilogue.  Tile
-// 128 x 256, k-block 128 bytes, 4-stage ring, two TMEM accumulators; persistent (one CTA per SM) over the
-// (tile, level) units.  Every mbarrier wait is bounded; on timeout *err is raised, the CTA skips its
-// remaining work, frees its TMEM and returns.  No cluster multicast.
+// 128 x BN (BN = 128, 192 or 256), k-block 128 bytes, 4-6-stage ring, two TMEM accumulators; persistent (one
+// CTA per SM) over the (tile, level) units.  Every mbarrier wait is bounded; on timeout *err is raised, the
+// CTA skips its remaining work, frees its TMEM and returns.  No cluster multicast.
 #pragma once
 #include <cuda.h>
 
