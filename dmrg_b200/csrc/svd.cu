@@ -107,8 +107,8 @@ __device__ __forceinline__ T rot_lo(T x, T y, T e, double sn, double tau) {
 // One round of the block Jacobi sweep: blockIdx.x = pair index.
 template<class T>
 __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, int64_t ldg, int m, T *__restrict__ V, int64_t ldv, int nv, int B,
-                                                           int round, double tol, double floor_abs, double *__restrict__ offmax,
-                                                           int *__restrict__ rotated) {
+                                                           int round, double tol, double floor_abs, const int *__restrict__ colmap,
+                                                           double *__restrict__ offmax, int *__restrict__ rotated) {
     using S                = JS<T>;
     constexpr int JROWS    = S::ROWS;
     __shared__ T      sG[JP][JP + 1];
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
     int p, q;
     rr_pair(B, round, blockIdx.x, p, q);
     const int tid = threadIdx.x;
-    if(tid < JP) s_idx[tid] = (tid < JB) ? p * JB + tid : q * JB + (tid - JB);
+    if(tid < JP) s_idx[tid] = colmap[(tid < JB) ? p * JB + tid : q * JB + (tid - JB)];
     __syncthreads();
 
     // ---- 1. Gram matrix of the 32 columns: thread owns entries (i, j) = (tid / 8, 4*(tid % 8) + 0..3)
@@ -332,7 +332,7 @@ static int g1(int64_t n) {
 int64_t svd_scratch_bytes(int64_t m, int64_t n, int64_t esize) {
     const int64_t npad = (n + JP - 1) / JP * JP;
     const int64_t ldg  = (m + 1) / 2 * 2;
-    return esize * (ldg * npad + npad * npad) + 8 * (npad + 64) + 4 * npad + 256;
+    return esize * (ldg * npad + npad * npad) + 8 * (npad + 64) + 8 * npad + 256;
 }
 
 // Rank rule of svd.cpp:257-280 on descending sigma (only exactly-nonzero values count, like
@@ -371,6 +371,7 @@ static int svd_truncated_t(const T *A, int64_t lda, int64_t m, int64_t n, int64_
     double       *dmax = sig + npad;  // [0] largest relative off-diagonal, [1] largest squared column norm
     int          *drot = reinterpret_cast<int *>(dmax + 8);
     int          *perm = reinterpret_cast<int *>(dmax + 64);
+    int          *cmap = perm + npad;  // column order of the current sweep (block b = columns cmap[16 b .. 16 b + 15])
     copy_pad_kernel<T><<<g1(ldg * npad), 256, 0, s>>>(A, lda, (int)m, (int)n, G, ldg, npad);
     HEFF_LAUNCH_CHECK();
     eye_kernel<T><<<g1((int64_t)npad * npad), 256, 0, s>>>(V, npad, npad);
@@ -381,10 +382,23 @@ static int svd_truncated_t(const T *A, int64_t lda, int64_t m, int64_t n, int64_
     const double eps   = 2.220446049250313e-16;
     double       floor_abs = 0.0;  // first sweep: relative criterion only
     int          sweep     = 0;
+    // Norm-ordered blocks (the block form of de Rijk's pivoting in LAPACK's ?gesvj): before every sweep the
+    // columns are ordered by norm and blocks are formed from neighbours, so clusters of close singular values
+    // meet inside one pair block, whose 32 x 32 problem is solved exactly.  On a spectrum with 3 % gaps this
+    // takes a 1024 x 1024 matrix from 40 sweeps without convergence to convergence in a few.
+    std::vector<double> hn(npad);
+    std::vector<int>    hmap(npad);
     for(; sweep < 40; sweep++) {
+        col_norms_kernel<T><<<(npad * 32 + 255) / 256, 256, 0, s>>>(G, ldg, (int)m, npad, sig);
+        HEFF_LAUNCH_CHECK();
+        HEFF_CUDA(cudaMemcpyAsync(hn.data(), sig, sizeof(double) * npad, cudaMemcpyDeviceToHost, s));
+        HEFF_CUDA(cudaStreamSynchronize(s));
+        std::iota(hmap.begin(), hmap.end(), 0);
+        std::stable_sort(hmap.begin(), hmap.end(), [&](int a, int b) { return hn[a] > hn[b]; });
+        HEFF_CUDA(cudaMemcpyAsync(cmap, hmap.data(), sizeof(int) * npad, cudaMemcpyHostToDevice, s));
         HEFF_CUDA(cudaMemsetAsync(dmax, 0, 8 * 8 + sizeof(int), s));
         for(int r = 0; r < B - 1; r++) {
-            jacobi_round_kernel<T><<<B / 2, JTHR, 0, s>>>(G, ldg, (int)m, V, npad, npad, B, r, tol, floor_abs, dmax, drot);
+            jacobi_round_kernel<T><<<B / 2, JTHR, 0, s>>>(G, ldg, (int)m, V, npad, npad, B, r, tol, floor_abs, cmap, dmax, drot);
             HEFF_LAUNCH_CHECK();
         }
         struct {

@@ -4,6 +4,7 @@
     python -m dmrg_b200.profile_cases eigs --chi 1024 --dtype f64 --precision fp64
     python -m dmrg_b200.profile_cases matvec --chi 1024 --dtype c128 --engine int8 --reps 2
     python -m dmrg_b200.profile_cases fdmrg --L 16 --chi 32 --sweeps 1
+    python -m dmrg_b200.profile_cases svd --chi 512 --reps 1
 
 The matvec case builds the standalone two-site workload (theta[4,chi,chi], Hermitian-slice environments
 generated on the device, merged two-site Ising MPO) and applies H_eff `reps` times after one warm-up
@@ -43,7 +44,7 @@ def main(argv=None):
     import dmrg_b200 as hb
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["matvec", "eigs", "fdmrg"])
+    ap.add_argument("case", choices=["matvec", "eigs", "fdmrg", "svd"])
     ap.add_argument("--L", type=int, default=16)
     ap.add_argument("--sweeps", type=int, default=1)
     ap.add_argument("--chi", type=int, default=1024)
@@ -57,6 +58,18 @@ def main(argv=None):
         h = 0.5 + np.array([(((i * 0x9E3779B97F4A7C15) >> 11) % 1000003) / 1000003.0 for i in range(1, a.L + 1)])
         r = hb.fdmrg(h, chi_max=a.chi, sweeps=a.sweeps, seed=2)
         print("fdmrg", r["energy"], r["num_mv"], r["t_eig"], r["t_svd"], r["t_env"])
+        return 0
+    if a.case == "svd":  # truncated SVD of a two-site theta reshaped to (2 chi) x (2 chi), graded spectrum, rank_max chi
+        n = 2 * a.chi
+        g = torch.Generator(device="cuda").manual_seed(n)
+        U, _ = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))
+        V, _ = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))
+        sv = torch.exp(-torch.arange(n, device="cuda", dtype=torch.float64) * (30.0 / n))
+        A = ((U * sv) @ V.T).T.contiguous().reshape(-1)
+        for _ in range(a.reps):
+            _, S, _, k, err = hb.svd(A, n, n, rank_max=a.chi)
+        torch.cuda.synchronize()
+        print("svd ok", k, err, float(S[0]))
         return 0
     cplx = a.dtype == "c128"
     prec = hb.PREC_MIXED if a.precision == "mixed" else hb.PREC_FP64
