@@ -25,6 +25,7 @@
 // (rows of the Gram with the conjugate coefficients); it reduces to the real rotation for e = +-1.
 #include <algorithm>
 #include <cmath>
+#include <cooperative_groups.h>
 #include <numeric>
 #include <vector>
 
@@ -104,11 +105,15 @@ __device__ __forceinline__ T rot_lo(T x, T y, T e, double sn, double tau) {
     return S::axpy(-sn, S::fma_(e, y, S::scale(x, tau)), x);
 }
 
-// One round of the block Jacobi sweep: blockIdx.x = pair index.
+// One round of the block Jacobi sweep.  A pair is handled by a cluster of CL CTAs (blockIdx.x = pair * CL + rank):
+// each forms the Gram of its share of the rows, the partials are summed through distributed shared memory in
+// rank order (so every CTA holds the same full Gram), every CTA runs the small Jacobi on it (the same Q
+// everywhere, no broadcast) and updates its share of the rows of G and V.  CL = 1: a plain launch, one CTA
+// per pair.  The two cluster barriers are reached by every CTA; the early exit comes after them.
 template<class T>
 __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, int64_t ldg, int m, T *__restrict__ V, int64_t ldv, int nv, int B,
                                                            int round, double tol, double floor_abs, const int *__restrict__ colmap,
-                                                           double *__restrict__ offmax, int *__restrict__ rotated) {
+                                                           double *__restrict__ offmax, int *__restrict__ rotated, int CL) {
     using S                = JS<T>;
     constexpr int JROWS    = S::ROWS;
     __shared__ T      sG[JP][JP + 1];
@@ -120,19 +125,22 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
     __shared__ double s_red[JTHR];
     __shared__ int    s_rot[2];
 
-    int p, q;
-    rr_pair(B, round, blockIdx.x, p, q);
+    int       p, q;
+    const int rank = (int)(blockIdx.x % CL);
+    rr_pair(B, round, (int)(blockIdx.x / CL), p, q);
     const int tid = threadIdx.x;
     if(tid < JP) s_idx[tid] = colmap[(tid < JB) ? p * JB + tid : q * JB + (tid - JB)];
     __syncthreads();
 
-    // ---- 1. Gram matrix of the 32 columns: thread owns entries (i, j) = (tid / 8, 4*(tid % 8) + 0..3)
+    // ---- 1. Gram matrix of the 32 columns over this CTA's rows [ga, gb): thread owns entries
+    //      (i, j) = (tid / 8, 4*(tid % 8) + 0..3)
     const int gi = tid / 8, gj0 = 4 * (tid % 8);
+    const int ga = (int)((int64_t)m * rank / CL), gb = (int)((int64_t)m * (rank + 1) / CL);
     T         acc[4] = {S::zero(), S::zero(), S::zero(), S::zero()};
-    for(int r0 = 0; r0 < m; r0 += JROWS) {
+    for(int r0 = ga; r0 < gb; r0 += JROWS) {
         for(int e = tid; e < JROWS * JP; e += JTHR) {
             const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
-            sT[rr][cc]   = row < m ? G[row + ldg * (int64_t)s_idx[cc]] : S::zero();
+            sT[rr][cc]   = row < gb ? G[row + ldg * (int64_t)s_idx[cc]] : S::zero();
         }
         __syncthreads();
         for(int rr = 0; rr < JROWS; rr++) {
@@ -142,9 +150,27 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
         }
         __syncthreads();
     }
+    if(CL == 1) {
 #pragma unroll
-    for(int u = 0; u < 4; u++) sG[gi][gj0 + u] = acc[u];
-    __syncthreads();
+        for(int u = 0; u < 4; u++) sG[gi][gj0 + u] = acc[u];
+        __syncthreads();
+    } else {
+        // partials in sQ (free until the Jacobi below), summed over the cluster in rank order
+        namespace cg = cooperative_groups;
+        cg::cluster_group cluster = cg::this_cluster();
+#pragma unroll
+        for(int u = 0; u < 4; u++) sQ[gi][gj0 + u] = acc[u];
+        cluster.sync();
+        T tot[4] = {S::zero(), S::zero(), S::zero(), S::zero()};
+        for(int r = 0; r < CL; r++) {
+            const T *rq = cluster.map_shared_rank(&sQ[0][0], r);
+#pragma unroll
+            for(int u = 0; u < 4; u++) tot[u] = JS<T>::axpy(1.0, rq[gi * (JP + 1) + gj0 + u], tot[u]);
+        }
+#pragma unroll
+        for(int u = 0; u < 4; u++) sG[gi][gj0 + u] = tot[u];
+        cluster.sync();  // every CTA has read the partials before any overwrites its sQ
+    }
 
     // ---- off-diagonal measure of the fresh Gram (relative to the diagonal; entries under the floor ignored)
     //      and the largest squared column norm of the pair (offmax[1], the next sweep's floor)
@@ -173,12 +199,12 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
         if(tid < w) s_red[tid] = fmax(s_red[tid], s_red[tid + w]);
         __syncthreads();
     }
-    if(tid == 0) {
+    if(tid == 0 && rank == 0) {
         atomic_max_pos(offmax, off0);
         atomic_max_pos(offmax + 1, s_red[0]);
     }
-    if(off0 <= tol) return;  // uniform across the CTA
-    if(tid == 0) atomicAdd(rotated, 1);
+    if(off0 <= tol) return;  // uniform across the CTA and the cluster (the same Gram everywhere)
+    if(tid == 0 && rank == 0) atomicAdd(rotated, 1);
 
     // ---- 2. cyclic Jacobi on sG, accumulating sQ.  Rotations are applied in Rutishauser's form
     //      x' = x - s (conj(e) y + tau x), y' = y + s (e x - tau y), tau = s / (1 + c), which keeps the
@@ -249,12 +275,13 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
         if(!rotated_this_sweep) break;
     }
 
-    // ---- 3. apply Q to the pair's columns of G (m rows) and V (nv rows)
+    // ---- 3. apply Q to this CTA's share of the pair's columns of G (m rows) and V (nv rows)
     for(int pass = 0; pass < 2; pass++) {
         T            *X    = pass == 0 ? G : V;
         const int64_t ldx  = pass == 0 ? ldg : ldv;
-        const int     rows = pass == 0 ? m : nv;
-        for(int r0 = 0; r0 < rows; r0 += JROWS) {
+        const int     all  = pass == 0 ? m : nv;
+        const int     ra = (int)((int64_t)all * rank / CL), rows = (int)((int64_t)all * (rank + 1) / CL);
+        for(int r0 = ra; r0 < rows; r0 += JROWS) {
             for(int e = tid; e < JROWS * JP; e += JTHR) {
                 const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
                 sT[rr][cc]   = row < rows ? X[row + ldx * (int64_t)s_idx[cc]] : S::zero();
@@ -388,6 +415,10 @@ static int svd_truncated_t(const T *A, int64_t lda, int64_t m, int64_t n, int64_
     // takes a 1024 x 1024 matrix from 40 sweeps without convergence to convergence in a few.
     std::vector<double> hn(npad);
     std::vector<int>    hmap(npad);
+    // CTAs per pair: enough to fill the SMs with one wave (the pairs of a round are only B / 2), when the rows
+    // are long enough to share out
+    int CL = 1;
+    while(CL < 4 && (int64_t)(B / 2) * CL * 2 <= device_sm_count() && m >= 128 * CL * 2) CL *= 2;
     for(; sweep < 40; sweep++) {
         col_norms_kernel<T><<<(npad * 32 + 255) / 256, 256, 0, s>>>(G, ldg, (int)m, npad, sig);
         HEFF_LAUNCH_CHECK();
@@ -398,8 +429,25 @@ static int svd_truncated_t(const T *A, int64_t lda, int64_t m, int64_t n, int64_
         HEFF_CUDA(cudaMemcpyAsync(cmap, hmap.data(), sizeof(int) * npad, cudaMemcpyHostToDevice, s));
         HEFF_CUDA(cudaMemsetAsync(dmax, 0, 8 * 8 + sizeof(int), s));
         for(int r = 0; r < B - 1; r++) {
-            jacobi_round_kernel<T><<<B / 2, JTHR, 0, s>>>(G, ldg, (int)m, V, npad, npad, B, r, tol, floor_abs, cmap, dmax, drot);
-            HEFF_LAUNCH_CHECK();
+            if(CL == 1) {
+                jacobi_round_kernel<T><<<B / 2, JTHR, 0, s>>>(G, ldg, (int)m, V, npad, npad, B, r, tol, floor_abs, cmap, dmax, drot, 1);
+                HEFF_LAUNCH_CHECK();
+            } else {
+                cudaLaunchConfig_t  lc = {};
+                cudaLaunchAttribute at[1];
+                at[0].id               = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = (unsigned)CL;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                lc.gridDim             = dim3((unsigned)(B / 2 * CL));
+                lc.blockDim            = dim3(JTHR);
+                lc.dynamicSmemBytes    = 0;
+                lc.stream              = s;
+                lc.attrs               = at;
+                lc.numAttrs            = 1;
+                HEFF_CUDA(cudaLaunchKernelEx(&lc, jacobi_round_kernel<T>, G, ldg, (int)m, V, (int64_t)npad, (int)npad, B, r, tol, floor_abs,
+                                             (const int *)cmap, dmax, drot, CL));
+            }
         }
         struct {
             double gmax;
