@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cooperative_groups.h>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "matvec.cuh"
@@ -100,6 +101,16 @@ __device__ inline void atomic_max_pos(double *addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
+// C += A B on the FP64 tensor pipe: mma.sync m16n8k4 (A fragment rows g, g+8 at column t; B at row t,
+// column g; C entries (g + 8 (r >> 1), 2 t + (r & 1)), g = lane / 4, t = lane % 4).
+__device__ __forceinline__ void dmma_f64(double (&c)[4], double a0, double a1, double b0) {
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a0), "d"(a1), "d"(b0));
+}
+template<class T>
+__device__ __forceinline__ void dmma_f64(T (&)[4], T, T, T) {}  // complex: not used (CUDA-core path)
+
 // x' = x - s (e y + tau x)  (one half of a Rutishauser-form rotation; e unit-modulus)
 template<class T>
 __device__ __forceinline__ T rot_lo(T x, T y, T e, double sn, double tau) {
@@ -139,38 +150,50 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
     const int gi = tid / 8, gj0 = 4 * (tid % 8);
     const int ga = (int)((int64_t)m * rank / CL), gb = (int)((int64_t)m * (rank + 1) / CL);
     T         acc[4] = {S::zero(), S::zero(), S::zero(), S::zero()};
+    // real: warp w forms the 16 x 8 tile (w / 4, w % 4) of the Gram on the FP64 tensor pipe (m16n8k4 DMMA,
+    // A = P^T, B = P from the staged rows); complex: thread-owned entries on the CUDA cores
+    const int lane = tid & 31, wg = lane >> 2, wt = lane & 3, wmt = (tid >> 5) >> 2, wnt = (tid >> 5) & 3;
     for(int r0 = ga; r0 < gb; r0 += JROWS) {
         for(int e = tid; e < JROWS * JP; e += JTHR) {
             const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
             sT[rr][cc]   = row < gb ? G[row + ldg * (int64_t)s_idx[cc]] : S::zero();
         }
         __syncthreads();
-        for(int rr = 0; rr < JROWS; rr++) {
-            const T a = sT[rr][gi];
+        if constexpr(std::is_same<T, double>::value) {
+#pragma unroll 4
+            for(int k4 = 0; k4 < JROWS; k4 += 4)
+                dmma_f64(acc, sT[k4 + wt][wmt * 16 + wg], sT[k4 + wt][wmt * 16 + wg + 8], sT[k4 + wt][wnt * 8 + wg]);
+        } else {
+            for(int rr = 0; rr < JROWS; rr++) {
+                const T a = sT[rr][gi];
 #pragma unroll
-            for(int u = 0; u < 4; u++) acc[u] = S::fma_cj(a, sT[rr][gj0 + u], acc[u]);
+                for(int u = 0; u < 4; u++) acc[u] = S::fma_cj(a, sT[rr][gj0 + u], acc[u]);
+            }
         }
         __syncthreads();
     }
+    // the Gram entry acc[u] holds: (gi, gj0 + u) on the CUDA-core path, the fragment entry u of the DMMA tile
+    auto g_row = [&](int u) { return std::is_same<T, double>::value ? wmt * 16 + wg + 8 * (u >> 1) : gi; };
+    auto g_col = [&](int u) { return std::is_same<T, double>::value ? wnt * 8 + 2 * wt + (u & 1) : gj0 + u; };
     if(CL == 1) {
 #pragma unroll
-        for(int u = 0; u < 4; u++) sG[gi][gj0 + u] = acc[u];
+        for(int u = 0; u < 4; u++) sG[g_row(u)][g_col(u)] = acc[u];
         __syncthreads();
     } else {
         // partials in sQ (free until the Jacobi below), summed over the cluster in rank order
         namespace cg = cooperative_groups;
         cg::cluster_group cluster = cg::this_cluster();
 #pragma unroll
-        for(int u = 0; u < 4; u++) sQ[gi][gj0 + u] = acc[u];
+        for(int u = 0; u < 4; u++) sQ[g_row(u)][g_col(u)] = acc[u];
         cluster.sync();
         T tot[4] = {S::zero(), S::zero(), S::zero(), S::zero()};
         for(int r = 0; r < CL; r++) {
             const T *rq = cluster.map_shared_rank(&sQ[0][0], r);
 #pragma unroll
-            for(int u = 0; u < 4; u++) tot[u] = JS<T>::axpy(1.0, rq[gi * (JP + 1) + gj0 + u], tot[u]);
+            for(int u = 0; u < 4; u++) tot[u] = JS<T>::axpy(1.0, rq[g_row(u) * (JP + 1) + g_col(u)], tot[u]);
         }
 #pragma unroll
-        for(int u = 0; u < 4; u++) sG[gi][gj0 + u] = tot[u];
+        for(int u = 0; u < 4; u++) sG[g_row(u)][g_col(u)] = tot[u];
         cluster.sync();  // every CTA has read the partials before any overwrites its sQ
     }
 
@@ -290,13 +313,36 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
                 sT[rr][cc]   = row < rows ? X[row + ldx * (int64_t)s_idx[cc]] : S::zero();
             }
             __syncthreads();
-            for(int e = tid; e < JROWS * JP; e += JTHR) {
-                const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
-                if(row < rows) {
-                    T v = S::zero();
+            if constexpr(std::is_same<T, double>::value) {
+                // (64 rows x 32) Q on the tensor pipe: warp w owns row tile w / 2 and column tiles 2 (w % 2) + 0, 1;
+                // the products go back through the staged tile so the stores below stay coalesced
+                const int mt = (tid >> 5) >> 1, nt0 = 2 * ((tid >> 5) & 1);
+                double    c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+                for(int k4 = 0; k4 < JP; k4 += 4) {
+                    const double a0 = sT[mt * 16 + wg][k4 + wt], a1 = sT[mt * 16 + wg + 8][k4 + wt];
+#pragma unroll
+                    for(int j = 0; j < 2; j++) dmma_f64(c[j], a0, a1, sQ[k4 + wt][(nt0 + j) * 8 + wg]);
+                }
+                __syncthreads();
+#pragma unroll
+                for(int j = 0; j < 2; j++)
+#pragma unroll
+                    for(int u = 0; u < 4; u++) sT[mt * 16 + wg + 8 * (u >> 1)][(nt0 + j) * 8 + 2 * wt + (u & 1)] = c[j][u];
+                __syncthreads();
+                for(int e = tid; e < JROWS * JP; e += JTHR) {
+                    const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
+                    if(row < rows) X[row + ldx * (int64_t)s_idx[cc]] = sT[rr][cc];
+                }
+            } else {
+                for(int e = tid; e < JROWS * JP; e += JTHR) {
+                    const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
+                    if(row < rows) {
+                        T v = S::zero();
 #pragma unroll 8
-                    for(int k = 0; k < JP; k++) v = S::fma_(sT[rr][k], sQ[k][cc], v);
-                    X[row + ldx * (int64_t)s_idx[cc]] = v;
+                        for(int k = 0; k < JP; k++) v = S::fma_(sT[rr][k], sQ[k][cc], v);
+                        X[row + ldx * (int64_t)s_idx[cc]] = v;
+                    }
                 }
             }
             __syncthreads();
