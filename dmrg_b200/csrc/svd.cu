@@ -108,8 +108,6 @@ __device__ __forceinline__ void dmma_f64(double (&c)[4], double a0, double a1, d
                  : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
                  : "d"(a0), "d"(a1), "d"(b0));
 }
-template<class T>
-__device__ __forceinline__ void dmma_f64(T (&)[4], T, T, T) {}  // complex: not used (CUDA-core path)
 
 // x' = x - s (e y + tau x)  (one half of a Rutishauser-form rotation; e unit-modulus)
 template<class T>
@@ -145,36 +143,43 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
     if(tid < JP) s_idx[tid] = colmap[(tid < JB) ? p * JB + tid : q * JB + (tid - JB)];
     __syncthreads();
 
-    // ---- 1. Gram matrix of the 32 columns over this CTA's rows [ga, gb): thread owns entries
-    //      (i, j) = (tid / 8, 4*(tid % 8) + 0..3)
-    const int gi = tid / 8, gj0 = 4 * (tid % 8);
+    // ---- 1. Gram matrix of the 32 columns over this CTA's rows [ga, gb)
     const int ga = (int)((int64_t)m * rank / CL), gb = (int)((int64_t)m * (rank + 1) / CL);
-    T         acc[4] = {S::zero(), S::zero(), S::zero(), S::zero()};
-    // real: warp w forms the 16 x 8 tile (w / 4, w % 4) of the Gram on the FP64 tensor pipe (m16n8k4 DMMA,
-    // A = P^T, B = P from the staged rows); complex: thread-owned entries on the CUDA cores
+    // warp w forms the 16 x 8 tile (w / 4, w % 4) of the Gram on the FP64 tensor pipe (m16n8k4 DMMA,
+    // A = P^H, B = P from the staged rows); complex: Re = Pr^T Pr + Pi^T Pi, Im = Pr^T Pi - Pi^T Pr
     const int lane = tid & 31, wg = lane >> 2, wt = lane & 3, wmt = (tid >> 5) >> 2, wnt = (tid >> 5) & 3;
+    double    accr[4] = {0, 0, 0, 0}, acci[4] = {0, 0, 0, 0};
     for(int r0 = ga; r0 < gb; r0 += JROWS) {
         for(int e = tid; e < JROWS * JP; e += JTHR) {
             const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
             sT[rr][cc]   = row < gb ? G[row + ldg * (int64_t)s_idx[cc]] : S::zero();
         }
         __syncthreads();
-        if constexpr(std::is_same<T, double>::value) {
 #pragma unroll 4
-            for(int k4 = 0; k4 < JROWS; k4 += 4)
-                dmma_f64(acc, sT[k4 + wt][wmt * 16 + wg], sT[k4 + wt][wmt * 16 + wg + 8], sT[k4 + wt][wnt * 8 + wg]);
-        } else {
-            for(int rr = 0; rr < JROWS; rr++) {
-                const T a = sT[rr][gi];
-#pragma unroll
-                for(int u = 0; u < 4; u++) acc[u] = S::fma_cj(a, sT[rr][gj0 + u], acc[u]);
+        for(int k4 = 0; k4 < JROWS; k4 += 4) {
+            const T a0 = sT[k4 + wt][wmt * 16 + wg], a1 = sT[k4 + wt][wmt * 16 + wg + 8], b = sT[k4 + wt][wnt * 8 + wg];
+            if constexpr(std::is_same<T, double>::value) {
+                dmma_f64(accr, a0, a1, b);
+            } else {
+                dmma_f64(accr, a0.x, a1.x, b.x);
+                dmma_f64(accr, a0.y, a1.y, b.y);
+                dmma_f64(acci, a0.x, a1.x, b.y);
+                dmma_f64(acci, -a0.y, -a1.y, b.x);
             }
         }
         __syncthreads();
     }
-    // the Gram entry acc[u] holds: (gi, gj0 + u) on the CUDA-core path, the fragment entry u of the DMMA tile
-    auto g_row = [&](int u) { return std::is_same<T, double>::value ? wmt * 16 + wg + 8 * (u >> 1) : gi; };
-    auto g_col = [&](int u) { return std::is_same<T, double>::value ? wnt * 8 + 2 * wt + (u & 1) : gj0 + u; };
+    T acc[4];
+#pragma unroll
+    for(int u = 0; u < 4; u++) {
+        if constexpr(std::is_same<T, double>::value)
+            acc[u] = accr[u];
+        else
+            acc[u] = make_double2(accr[u], acci[u]);
+    }
+    // the Gram entry acc[u] holds: the fragment entry u of the warp's DMMA tile
+    auto g_row = [&](int u) { return wmt * 16 + wg + 8 * (u >> 1); };
+    auto g_col = [&](int u) { return wnt * 8 + 2 * wt + (u & 1); };
     if(CL == 1) {
 #pragma unroll
         for(int u = 0; u < 4; u++) sG[g_row(u)][g_col(u)] = acc[u];
@@ -335,14 +340,33 @@ __global__ void __launch_bounds__(JTHR) jacobi_round_kernel(T *__restrict__ G, i
                     if(row < rows) X[row + ldx * (int64_t)s_idx[cc]] = sT[rr][cc];
                 }
             } else {
+                // (16 rows x 32) Q, complex: warp w owns column tile w % 4 and the real (w < 4) or imaginary part
+                const int nt = (tid >> 5) & 3, im = (tid >> 5) >> 2;
+                double    c[4] = {0, 0, 0, 0};
+#pragma unroll
+                for(int k4 = 0; k4 < JP; k4 += 4) {
+                    const T a0 = sT[wg][k4 + wt], a1 = sT[wg + 8][k4 + wt], qv = sQ[k4 + wt][nt * 8 + wg];
+                    if(im == 0) {  // Re = Tr Qr - Ti Qi
+                        dmma_f64(c, a0.x, a1.x, qv.x);
+                        dmma_f64(c, -a0.y, -a1.y, qv.y);
+                    } else {       // Im = Tr Qi + Ti Qr
+                        dmma_f64(c, a0.x, a1.x, qv.y);
+                        dmma_f64(c, a0.y, a1.y, qv.x);
+                    }
+                }
+                __syncthreads();
+#pragma unroll
+                for(int u = 0; u < 4; u++) {
+                    T &dst = sT[wg + 8 * (u >> 1)][nt * 8 + 2 * wt + (u & 1)];
+                    if(im == 0)
+                        dst.x = c[u];
+                    else
+                        dst.y = c[u];
+                }
+                __syncthreads();
                 for(int e = tid; e < JROWS * JP; e += JTHR) {
                     const int rr = e % JROWS, cc = e / JROWS, row = r0 + rr;
-                    if(row < rows) {
-                        T v = S::zero();
-#pragma unroll 8
-                        for(int k = 0; k < JP; k++) v = S::fma_(sT[rr][k], sQ[k][cc], v);
-                        X[row + ldx * (int64_t)s_idx[cc]] = v;
-                    }
+                    if(row < rows) X[row + ldx * (int64_t)s_idx[cc]] = sT[rr][cc];
                 }
             }
             __syncthreads();
