@@ -3,13 +3,14 @@
 // schmidt_multisite (source/math/svd.h:189-220), for real (double) and complex (double2) matrices.
 //
 // Algorithm: one-sided (Hestenes) block Jacobi in FP64.  The columns of the work matrix G (= A, m x n,
-// column-major, n padded to a multiple of 32 with zero columns) are grouped into blocks of 16.  A sweep
-// pairs every block with every other block once (round-robin tournament, B-1 rounds of B/2 disjoint
-// pairs).  For one pair, a CTA
-//   1. forms the 32 x 32 Gram matrix P^H P of the pair's 32 columns (streamed through shared memory),
-//   2. diagonalises it with a cyclic two-sided Jacobi eigensolver in shared memory (16 disjoint
+// column-major, n padded to a multiple of 32 with zero columns) are ordered by norm before every sweep and
+// grouped into blocks of 16 neighbours.  A sweep pairs every block with every other block once
+// (round-robin tournament, B-1 rounds of B/2 disjoint pairs).  For one pair, a cluster of 1-4 CTAs
+//   1. forms the 32 x 32 Gram matrix P^H P of the pair's 32 columns (rows streamed through shared memory,
+//      DMMA products, row shares summed across the cluster),
+//   2. runs one sweep of a cyclic two-sided Jacobi eigensolver on it in shared memory (16 disjoint
 //      rotations per step), accumulating the unitary Q,
-//   3. applies P <- P Q and V[:, pair] <- V[:, pair] Q.
+//   3. applies P <- P Q and V[:, pair] <- V[:, pair] Q (DMMA, row shares).
 // A pair whose Gram is already diagonal to |g_ij| <= max(tol*sqrt(g_ii g_jj), floor) is skipped; the
 // sweep loop stops when every pair was skipped.  The relative criterion, evaluated on freshly computed
 // Gram entries, is what lets one-sided Jacobi resolve small singular values to high relative accuracy
