@@ -83,8 +83,8 @@ __global__ void z_rowmax_fin_kernel(unsigned long long *rmax, int64_t rows, doub
 }
 
 // Digits of 16 scaled values y (|y| <= 64) for slice t: byte j of w = rint(y_j); y_j <- 128 (y_j - rint(y_j)).
-// Both steps are exact in FP64 (|y - rint y| <= 1/2 lies on y's own grid), so the digits of all slices
-// reproduce the value to 2^-(7 s) of the leading digit's unit.
+// Both steps are exact in FP64 (|y - rint y| <= 1/2 lies on y's own grid), so after s slices the value is
+// reproduced to half a unit of the last digit, 2^-7s of the row scale.
 __device__ __forceinline__ void z_digits16(double (&y)[16], uint32_t (&w)[4], uint32_t (&wn)[4]) {
 #pragma unroll
     for(int q = 0; q < 4; q++) {

@@ -3,7 +3,8 @@
 // (2012); integer form: Ootomo/Ozaki/Yokota, IJHPCA 2024):
 //
 //   every row r of an operand is scaled by a power of two sigma_r > max_k |v[r,k]| and written as signed
-//   digits  v[r,k] = sigma_r * 2^-6 * sum_t d_t[r,k] 2^(-7t)  (+ a remainder below 2^-(6+7s) sigma_r),
+//   digits  v[r,k] = sigma_r * 2^-6 * sum_t d_t[r,k] 2^(-7t)  (+ a remainder of at most 2^-7s sigma_r, half a
+//   unit of the last digit),
 //   d_0 = rint(64 x), d_t = rint(128 * remainder): |d_t| <= 64 fits int8 and every step is exact in FP64.
 //
 //   C[m,n] = fa[m] fb[n] sum_{g < s} 2^(-7g) S_g[m,n],   S_g = sum_{t+u=g} D^A_t (D^B_u)^T   (INT32, exact)
