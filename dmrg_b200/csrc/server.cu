@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "eig.cuh"
+#include "gemm_i8.cuh"
 #include "op.cuh"
 #include "runtime.cuh"
 
@@ -66,7 +67,7 @@ size_t request_bytes(const heff_request &r, int max_basis) {
         b += 2 * (S * cL) * nseg * r64(cR * DR) + 2 * cf * cR * nseg * r64(cR * DR);   // A2, B2
         b += 4 * (cL * DL) * cf * (S * cR);                                            // T1 (fp32)
     }
-    if(r.fp64_engine == HEFF_FP64_INT8) b += (int64_t)emu_bytes(S, cL, cR, DL, DR, r.dtype == HEFF_C128, 7);  // digit planes
+    if(r.fp64_engine == HEFF_FP64_INT8) b += (int64_t)emu_bytes(S, cL, cR, DL, DR, r.dtype == HEFF_C128, Z_DEFAULT_SLICES);  // digit planes
     const int64_t vec = (es * n + 255) / 256 * 256;
     b += vec * (2 * (max_basis + 1) + 2 * max_basis + 4 + (mixed ? 5 : 0)) + (int64_t)(es * 128 * 131) + 8 * 512 * 128 * 4;
     return (size_t)b + (size_t)(4 << 20);
