@@ -53,3 +53,18 @@ def test_mixed_and_int8_requests_budget_their_buffers():
 
 def test_null_request_is_zero():
     assert hb.lib().heff_request_bytes(None, 24) == 0
+
+
+def test_int8_tile_width_knob():
+    """heff_i8_set_tile_width accepts 0 (automatic), 128, 192 or 256, returns the previous setting, rejects the rest."""
+    L = hb.lib()
+    prev = L.heff_i8_set_tile_width(0)
+    try:
+        assert prev in (0, 128, 192, 256)
+        assert L.heff_i8_set_tile_width(192) == 0
+        assert L.heff_i8_set_tile_width(128) == 192
+        assert L.heff_i8_set_tile_width(100) == -1
+        assert L.heff_i8_set_tile_width(160) == -1
+        assert L.heff_i8_set_tile_width(0) == 128
+    finally:
+        L.heff_i8_set_tile_width(prev)
