@@ -506,6 +506,13 @@ class MatVecMPOS:
         """Jacobi preconditioner y = x / (diag - shift) (MultPc, matvec_mpos.cpp:1349-1364); device tensors."""
         check(lib().heff_op_multpc(self.handle, ptr(x), ptr(y), float(shift)), "heff_op_multpc")
 
+    def device_error(self):
+        """Device-side status of the tensor-core pipeline (heff_op_device_error): 0 when every bounded wait completed,
+        5 after a non-finite input on the INT8 engine, other nonzero codes after a timed-out wait."""
+        code = ctypes.c_int(0)
+        check(lib().heff_op_device_error(self.handle, ctypes.byref(code)), "heff_op_device_error")
+        return int(code.value)
+
     @property
     def num_mv(self):
         return int(lib().heff_op_num_mv(self.handle))

@@ -3,7 +3,12 @@
 //
 // Real symmetric: Householder reduction to tridiagonal form followed by the implicit QL algorithm with
 // Wilkinson-type shifts (Golub & Van Loan, "Matrix Computations", sections 8.3 and 8.5), eigenvectors
-// accumulated.  Complex Hermitian H = A + iB is solved through its real symmetric 2k x 2k form
+// accumulated.  The code follows the published EISPACK routines TRED2 (Householder tridiagonalisation
+// with accumulated transforms) and TQL2 (implicit QL on the tridiagonal matrix): Martin, Reinsch and
+// Wilkinson, Numer. Math. 11 (1968) 181-195 and Bowdler, Martin, Reinsch and Wilkinson, Numer. Math. 11
+// (1968) 293-306, as collected in the Handbook for Automatic Computation, vol. II (1971), and the EISPACK
+// Guide (Smith et al., Lecture Notes in Computer Science 6, 1976): the same row scaling, the h / f / g
+// Householder quantities and the off-diagonal vector e[] of those routines.  Complex Hermitian H = A + iB is solved through its real symmetric 2k x 2k form
 // [[A, -B], [B, A]], whose eigenvectors [x; y] give eigenvectors x + iy of H; each eigenvalue appears
 // twice there, and the duplicate (i times the same complex vector) is removed by Gram-Schmidt.
 #pragma once

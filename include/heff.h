@@ -79,10 +79,13 @@ int heff_matvec_multi_z(heff_z *res, const heff_z *mps, const int64_t mps_dims[3
  * among its own pools, or that cannot afford the device-wide synchronisation a
  * cudaMalloc/cudaFree implies).  Scratch comes from one fixed 32 MiB array
  * inside the library (held on every GPU that loads the library until exit);
- * calls needing more return HEFF_BAD_SHAPE (real two-site D=3 fits up to about
- * chi=360).  All calls on a device share that array: calls that may overlap on
+ * calls needing more return HEFF_BAD_SHAPE (real two-site D=3 fits up to
+ * chi=367).  All calls on a device share that array: calls that may overlap on
  * the GPU race, so serialise them.  The first call on a device looks up the
- * array's device address; make it before any stream capture. */
+ * array's device address and keeps it for the life of the process; make it
+ * before any stream capture.  A cudaDeviceReset of that device makes the kept
+ * address (and heff_matvec_d's kept workspaces) stale: do not call the library
+ * on a device again after resetting it in the same process. */
 int heff_matvec_d_noalloc(double *res, const double *mps, const int64_t mps_dims[3], const double *mpo, const int64_t mpo_dims[4],
                           const double *envL, const int64_t envL_dims[3], const double *envR, const int64_t envR_dims[3], void *stream);
 

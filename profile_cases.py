@@ -1,10 +1,10 @@
 """Small fixed workloads for profiler captures (ncu) of single kernels of the hot path.
 
-    python -m dmrg_b200.profile_cases matvec --chi 1024 --dtype c128 --precision mixed --reps 3
-    python -m dmrg_b200.profile_cases eigs --chi 1024 --dtype f64 --precision fp64
-    python -m dmrg_b200.profile_cases matvec --chi 1024 --dtype c128 --engine int8 --reps 2
-    python -m dmrg_b200.profile_cases fdmrg --L 16 --chi 32 --sweeps 1
-    python -m dmrg_b200.profile_cases svd --chi 512 --reps 1
+    python profile_cases.py matvec --chi 1024 --dtype c128 --precision mixed --reps 3
+    python profile_cases.py eigs --chi 1024 --dtype f64 --precision fp64
+    python profile_cases.py matvec --chi 1024 --dtype c128 --engine int8 --reps 2
+    python profile_cases.py fdmrg --L 16 --chi 32 --sweeps 1
+    python profile_cases.py svd --chi 512 --reps 1
 
 The matvec case builds the standalone two-site workload (theta[4,chi,chi], Hermitian-slice environments
 generated on the device, merged two-site Ising MPO) and applies H_eff `reps` times after one warm-up
