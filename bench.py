@@ -133,7 +133,29 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_sample(chi, D, cplx, budget_s, seed=5, one_thread_s=0.0):
+SEED = 1  # seed of the headline workload's inputs (both arms)
+
+
+def bench_config(ws):
+    """The workload description both arms print (the reference arm times the same workload on the host cores)."""
+    return {"workload": "standalone two-site H_eff matvec, theta[4,1024,1024] complex128, envs [1024,1024,3], Ising MPO D=3",
+            "chi": CHI, "D": D, "spin": SPIN, "parallelism": "replicas" if ws > 1 else "none",
+            "l2": "working set (theta 64 MB, envs 2 x 50 MB, intermediates 2 x 200 MB) larger than the 126 MB L2; the GPU arm "
+                  "also writes a 256 MB buffer between timed steps"}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference_sample(chi, D, cplx, budget_s, seed=SEED, one_thread_s=0.0):
     """Time the reference's contraction sequence (BLAS restatement, oracle/ref_numpy.py) on the host."""
     from oracle import ref_numpy as rn
 
@@ -167,6 +189,7 @@ def cpu_reference_sample(chi, D, cplx, budget_s, seed=5, one_thread_s=0.0):
     except ImportError:
         threads = os.cpu_count()
     return {"value": F * n / el / 1e12, "unit": UNIT, "cores": int(threads), "kind": "port", "matvecs": n, "seconds": el,
+            "cpu_model": cpu_model(), "host_cpus": os.cpu_count(),
             "sample": f"{n} complex128 matvecs at chi={chi}, D={D} (full workload size), BLAS restatement of contraction_tblis.cpp:277-290",
             "one_thread": one}
 
@@ -277,6 +300,132 @@ def two_site_mpo(D, cplx):
     X = np.einsum("mcst,cnuv->mnsutv", WA, WB)
     W = X.reshape(WA.shape[0], WB.shape[1], 4, 4, order="F")
     return np.asfortranarray(W.astype(np.complex128 if cplx else np.float64))
+
+
+def host_matvec(th, W, L, R):
+    """y = H_eff theta on the host in the reference's contraction order (contraction_tblis.cpp:277-290, chiL >= chiR):
+    theta . envL over a, then . W over (m, s), then . envR over (b, n); numpy tensordot (BLAS)."""
+    T1 = np.tensordot(th, L, axes=([1], [0]))  # [s, b, a', m]
+    T2 = np.tensordot(T1, W, axes=([0, 3], [2, 0]))  # [b, a', n, s']
+    y = np.tensordot(T2, R, axes=([0, 2], [0, 2]))  # [a', s', b']
+    return np.asfortranarray(y.transpose(1, 0, 2))
+
+
+def truncation_rank(S, rank_max, trunc_lim):
+    """Rank rule of svd.cpp:257-280: keep singular values while the 2-norm of the discarded tail stays >= trunc_lim,
+    at most rank_max; returns (rank, truncation error = norm of the discarded tail)."""
+    S = np.asarray(S)
+    tail = np.sqrt(np.cumsum((S[::-1] ** 2))[::-1])  # tail[k] = ||S[k:]||
+    k = int(np.count_nonzero(tail >= trunc_lim))
+    if rank_max > 0:
+        k = min(k, rank_max)
+    err = float(np.linalg.norm(S[k:])) if k < len(S) else 0.0
+    return k, err
+
+
+def measure_grid(hb, torch, stream, flush, chis=(256, 512, 1024, 2048), Ds=(3, 9), reps=5):
+    """The precision-microbenchmark grid: the standalone two-site matvec (theta Gaussian, Hermitian-slice envs generated
+    on the device, W = merged two-site Ising MPO for D=3 or its uncompressed square for D=9) at every chi and D, complex128
+    and float64; FP64 on the DMMA engine, FP64 on the INT8 engine and mixed split-BF16, each CUDA-event timed over `reps`
+    applications with the L2 flushed between them, and each compared with the host product in the reference's
+    contraction order (host_matvec; rel. error ||y - y_host|| / ||y_host||)."""
+    out = {}
+    for cplx in (True, False):
+        tag = "c128" if cplx else "f64"
+        rows = {}
+        for chi in chis:
+            for D in Ds:
+                W = two_site_mpo(D, cplx)
+                sb = 3 if D == 9 else 0
+                Ld = hb.make_env(chi, D, cplx, seed=1000 + chi + D, swap_base=sb)
+                Rd = hb.make_env(chi, D, cplx, seed=2000 + chi + D, swap_base=sb)
+                L = hb.to_host(Ld, (chi, chi, D))
+                R = hb.to_host(Rd, (chi, chi, D))
+                x = hb.make_vector(SPIN * chi * chi, cplx, seed=3000 + chi + D)
+                th = hb.to_host(x, (SPIN, chi, chi))
+                del Ld, Rd
+                y_ref = host_matvec(th, W, L, R).ravel(order="F")
+                nref = float(np.linalg.norm(y_ref))
+                F = matvec_flops(SPIN, chi, chi, D, D, cplx)
+                row = {"flops": F}
+
+                def timed(op, name):
+                    y = torch.empty_like(x)
+                    with torch.cuda.stream(stream):
+                        for _ in range(2):
+                            op.MultAx(x, y)
+                        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+                        for k, (a, b) in enumerate(evs):
+                            flush.fill_(float(k))
+                            a.record(stream)
+                            op.MultAx(x, y)
+                            b.record(stream)
+                        stream.synchronize()
+                    ms = sum(a.elapsed_time(b) for a, b in evs) / reps
+                    err = float(np.linalg.norm(y.cpu().numpy() - y_ref) / nref)
+                    row[name] = {"ms": ms, "tflops": F / (ms / 1e3) / 1e12, "rel_err_vs_host": err}
+                    return y
+
+                op = hb.MatVecMPOS([W], L, R, cplx=cplx, stream=stream)
+                op.set_profiling(True)
+                op.stage_times(reset=True)
+                timed(op, "fp64_dmma")
+                st, cnt = op.stage_times(reset=True)
+                op.set_profiling(False)
+                row["fp64_dmma"]["stage_ms"] = [v / max(cnt, 1) for v in st]
+                row["fp64_dmma"]["frac_of_nominal_40"] = row["fp64_dmma"]["tflops"] / 40.0
+                op.set_fp64_engine(hb.FP64_INT8)
+                timed(op, "fp64_int8")
+                op.close()
+                opm = hb.MatVecMPOS([W], L, R, cplx=cplx, precision=hb.PREC_MIXED, stream=stream)
+                timed(opm, "mixed")
+                opm.close()
+                rows[f"chi{chi}_D{D}"] = row
+                del x, L, R, th, y_ref
+                torch.cuda.empty_cache()
+        out[tag] = rows
+    out["workload"] = ("two-site H_eff matvec theta[4,chi,chi] Gaussian, envs [chi,chi,D] Hermitian per slice (D=9: MPO-squared swap "
+                       "symmetry), W = merged two-site Ising MPO (D=3) or its square (D=9); FLOPs are the dense algorithmic count; "
+                       "rel_err_vs_host: against host_matvec, the contraction sequence of contraction_tblis.cpp:277-290 in numpy")
+    return out
+
+
+def measure_svd(hb, torch, chis=(512, 1024), reps=3):
+    """Two-site SVD truncation at the split shape (2 chi) x (2 chi): a matrix with a Schmidt-like graded spectrum
+    (singular values 1 .. 1e-13, geometric, random orthogonal factors), rank_max = chi, truncation limit 1e-12.
+    Device one-sided Jacobi (heff_svd_d) vs LAPACK gesdd through numpy on all host cores (the routine the reference's
+    svd::solver resolves to for this shape); singular values compared with gesdd's."""
+    out = {}
+    rng = np.random.default_rng(41)
+    for chi in chis:
+        n = 2 * chi
+        Q1, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        Q2, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        sv = np.geomspace(1.0, 1e-13, n)
+        A = np.asfortranarray((Q1 * sv) @ Q2.T)
+        Ad = hb.to_device(A)
+        hb.svd(Ad, n, n, rank_max=chi, trunc_lim=1e-12)
+        torch.cuda.synchronize()
+        tg = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            U, S, VT, k, terr = hb.svd(Ad, n, n, rank_max=chi, trunc_lim=1e-12)
+            torch.cuda.synchronize()
+            tg.append(time.perf_counter() - t0)
+        tc = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            Uc, Sc, VTc = np.linalg.svd(A, full_matrices=False)  # LAPACK ?gesdd
+            kc, errc = truncation_rank(Sc, chi, 1e-12)
+            tc.append(time.perf_counter() - t0)
+        Sg = S.cpu().numpy()
+        m = min(len(Sg), len(Sc))
+        out[f"{n}x{n}"] = {"gpu_ms": 1e3 * statistics.median(tg), "cpu_gesdd_ms": 1e3 * min(tc), "speedup_vs_cpu": min(tc) / statistics.median(tg),
+                           "rank_gpu": k, "rank_gesdd": kc, "max_sigma_err_rel_sigma_max": float(np.max(np.abs(Sg[:m] - Sc[:m])) / Sc[0]),
+                           "trunc_err_gpu": terr, "trunc_err_gesdd": errc}
+        del Ad, U, S, VT
+    out["workload"] = "real (2chi)x(2chi), singular values geometric 1..1e-13, rank_max=chi, truncation limit 1e-12 (svd.cpp:257-280)"
+    return out
 
 
 def measure_eigs_folded(hb, torch, chi=512):
@@ -425,9 +574,8 @@ def run_reference(args):
     sec = sum(x["seconds"] for x in vals)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sec / mv, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-            "data": "synthetic", "config": {"workload": "standalone two-site H_eff matvec, theta[4,1024,1024] complex128, Ising MPO D=3",
-                                            "chi": CHI, "D": D, "spin": SPIN},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"], "kind": "port",
+            "data": "synthetic (seeded Gaussian theta, Hermitian-slice envs, Ising two-site MPO)", "config": bench_config(ws),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"], "kind": "port", "cpu_model": vals[0]["cpu_model"],
                              "sample": f"{mv} matvecs in {sec:.1f} s (each step ~{budget:.0f} s of BLAS restatement)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -448,6 +596,7 @@ def main():
     ap.add_argument("--serving-chi-max", type=int, default=1024)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--ensemble-n", type=int, default=32, help="realisations in the ensemble sample")
+    ap.add_argument("--no-grid", action="store_true", help="skip the chi x D precision grid and the SVD timing")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -496,7 +645,7 @@ def main():
 
     peak = zgemm_peak()
 
-    theta, mpos, L, R = make_inputs(CHI, D, True, seed=1 + rank)
+    theta, mpos, L, R = make_inputs(CHI, D, True, seed=SEED + rank)
     stream = torch.cuda.Stream()
     op = hb.MatVecMPOS(mpos, L, R, cplx=True, stream=stream)
     n = op.rows()
@@ -559,6 +708,23 @@ def main():
         extras["serving"] = sv
         extras["ensemble"] = measure_ensemble(hb, args.ensemble_n, 4, 32)  # 32 workers: 21 /s vs 18.6 /s with 16 (32 realisations)
         extras["eigensolves_folded"] = measure_eigs_folded(hb, torch)
+    if not args.no_extras and not args.no_grid:
+        torch.cuda.empty_cache()
+        gstream = torch.cuda.Stream()
+        gflush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        grid = measure_grid(hb, torch, gstream, gflush)
+        extras["precision_grid"] = grid
+        r = grid["f64"]["chi1024_D3"]["fp64_dmma"]
+        FGr = gemm_flops(SPIN, CHI, CHI, D, D, False)
+        gemm_ms_r = r["stage_ms"][1] + r["stage_ms"][3]
+        extras["real_fp64_matvec"] = {
+            "workload": "the same matvec in float64 (real Gaussian theta, real symmetric-slice envs), chi=1024, D=3",
+            "ms": r["ms"], "tflops": r["tflops"], "frac_of_nominal_40": r["tflops"] / 40.0, "stage_ms": r["stage_ms"],
+            "gemm_tflops": FGr / (gemm_ms_r / 1e3) / 1e12, "gemm_frac_of_nominal_40": FGr / (gemm_ms_r / 1e3) / 1e12 / 40.0,
+            "rel_err_vs_host": r["rel_err_vs_host"]}
+        del gflush
+        torch.cuda.empty_cache()
+        extras["svd"] = measure_svd(hb, torch)
 
     tot_ms, e2e_t = reduce_max_over_ranks([sum(step_ms), statistics.median(t_e2e)], dist)
     ms_per_step = tot_ms / args.steps
@@ -577,9 +743,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (seeded Gaussian theta, Hermitian-slice envs, Ising two-site MPO)",
-        "config": {"workload": "standalone two-site H_eff matvec, theta[4,1024,1024] complex128, envs [1024,1024,3], Ising MPO D=3",
-                   "chi": CHI, "D": D, "spin": SPIN, "parallelism": "replicas" if ws > 1 else "single GPU",
-                   "l2": "256 MB buffer written between timed steps (L2 flush)"},
+        "config": bench_config(ws),
         "roofline": {"bound": "tensor", "kernel": "gemm_f64_kernel (DMMA m16n8k4, 2 launches per matvec)", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": "cuBLAS ZGEMM 4096^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",

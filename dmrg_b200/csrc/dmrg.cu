@@ -31,9 +31,11 @@
 
 namespace heff {
 
+// The environment updates of a sweep run on the operator's stream between its matvecs, so they share the operator's
+// tail-split scratch.
 static int env_update_d(int side, double *out, const double *E, const int64_t ed[3], const double *M, const int64_t md[3], const double *W,
-                        const int64_t wd[4], double *scratch, cudaStream_t s) {
-    return env_update<false>(side, out, E, ed, M, md, W, wd, scratch, s);
+                        const int64_t wd[4], double *scratch, cudaStream_t s, void *split_ws, size_t split_bytes) {
+    return env_update<false>(side, out, E, ed, M, md, W, wd, scratch, s, split_ws, split_bytes);
 }
 
 // splitmix64 -> uniform [0, 1): the generator shared with oracle/physics.py
@@ -237,7 +239,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     // R environments: Renv[i] = env of sites > i, dims [chi_{i+1}, chi_{i+1}, wd[i][1]]
     for(int i = L - 2; i >= 0; i--) {
         const int64_t ed[3] = {chi[i + 2], chi[i + 2], wd[i + 1][1]}, mdd[3] = {d, chi[i + 1], chi[i + 2]};
-        HEFF_TRY(env_update_d(1, ws.Renv[i], ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), ws.scr, s));
+        HEFF_TRY(env_update_d(1, ws.Renv[i], ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), ws.scr, s, ws.op->split_ws, ws.op->split_bytes));
     }
     heff_eig_config ecfg;
     heff_eig_config_default(&ecfg);
@@ -285,7 +287,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
                 auto    ts0 = now();
                 int64_t k   = 0;
                 double  te  = 0;
-                HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_max, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s));
+                HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_max, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s, ws.op->split_ws, ws.op->split_bytes));
                 res.trunc_err_max = std::max(res.trunc_err_max, te);
                 res.svd_sweeps_max = std::max(res.svd_sweeps_max, last_svd_sweeps());
                 if(i + 1 == L / 2 && sweep == cfg.sweeps - 1) {
@@ -307,14 +309,14 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
                     HEFF_LAUNCH_CHECK();
                     HEFF_CUDA(cudaMemcpyAsync(ws.M[i + 1], ws.V, sizeof(double) * d * k * cb, cudaMemcpyDeviceToDevice, s));
                     const int64_t ed[3] = {ca, ca, wd[i][0]}, mdd[3] = {d, ca, k};
-                    HEFF_TRY(env_update_d(0, ws.Lenv[i + 1], ws.Lenv[i], ed, ws.M[i], mdd, ws.W[i], wd[i].data(), ws.scr, s));
+                    HEFF_TRY(env_update_d(0, ws.Lenv[i + 1], ws.Lenv[i], ed, ws.M[i], mdd, ws.W[i], wd[i].data(), ws.scr, s, ws.op->split_ws, ws.op->split_bytes));
                 } else {
                     HEFF_CUDA(cudaMemcpyAsync(ws.M[i + 1], ws.V, sizeof(double) * d * k * cb, cudaMemcpyDeviceToDevice, s));
                     scale_bond_kernel<<<g1(d * ca * k), 256, 0, s>>>(ws.U, ws.S, d, ca, k, 0);
                     HEFF_LAUNCH_CHECK();
                     HEFF_CUDA(cudaMemcpyAsync(ws.M[i], ws.U, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
                     const int64_t ed[3] = {cb, cb, wd[i + 1][1]}, mdd[3] = {d, k, cb};
-                    HEFF_TRY(env_update_d(1, ws.Renv[i], ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), ws.scr, s));
+                    HEFF_TRY(env_update_d(1, ws.Renv[i], ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), ws.scr, s, ws.op->split_ws, ws.op->split_bytes));
                 }
                 t_env += secs(tv0, now());
             }
@@ -338,7 +340,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
         HEFF_CUDA(cudaMemcpyAsync(ws.Lenv[L - 1], &one, sizeof(double), cudaMemcpyHostToDevice, s));
         for(int i = L - 2; i >= 1; i--) {
             const int64_t ed[3] = {chi[i + 2], chi[i + 2], w3[i + 1][1]}, mdd[3] = {d, chi[i + 1], chi[i + 2]};
-            HEFF_TRY(env_update_d(1, ws.Lenv[i], ws.Lenv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], w3[i + 1].data(), ws.scr, s));
+            HEFF_TRY(env_update_d(1, ws.Lenv[i], ws.Lenv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], w3[i + 1].data(), ws.scr, s, ws.op->split_ws, ws.op->split_bytes));
         }
         const int64_t ca = chi[0], cc = chi[1], cb = chi[2];
         perm_sc_kernel<<<g1(d * cc * cb), 256, 0, s>>>(ws.M[1], ws.P2, d, cc, cb);

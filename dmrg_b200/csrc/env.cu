@@ -112,7 +112,8 @@ int64_t env_scratch_elems(const int64_t md[3], const int64_t wd[4]) {
 // out = build_block(env, M, W); scratch holds env_scratch_elems() elements.
 template<bool CPLX>
 int env_update(int side, typename Scalar<CPLX>::T *out, const typename Scalar<CPLX>::T *E, const int64_t ed[3], const typename Scalar<CPLX>::T *M,
-               const int64_t md[3], const typename Scalar<CPLX>::T *W, const int64_t wd[4], typename Scalar<CPLX>::T *scratch, cudaStream_t s) {
+               const int64_t md[3], const typename Scalar<CPLX>::T *W, const int64_t wd[4], typename Scalar<CPLX>::T *scratch, cudaStream_t s,
+               void *split_ws, size_t split_bytes) {
     using T = typename Scalar<CPLX>::T;
     HEFF_TRY(check_env_dims(side, ed, md, wd));
     auto          pad = [](int64_t n) { return (n + 31) / 32 * 32; };
@@ -141,6 +142,7 @@ int env_update(int side, typename Scalar<CPLX>::T *out, const typename Scalar<CP
         h.M = (int)cR, h.N = (int)(cR * DR), h.K = (int)(d * cL), h.batch = 1;
         h.A = M, h.lda = d * cL, h.B = Y, h.ldb = d * cL, h.C = out, h.ldc = cR;
         h.alpha = make_double2(1, 0), h.beta = make_double2(0, 0);
+        h.split_ws = split_ws, h.split_ws_bytes = split_bytes;
         HEFF_TRY(gemm_f64<CPLX>(true, false, false, h, s));
     } else {
         env_prep_R<<<grid1(nM), 256, 0, s>>>(M, Mc, M2, d, cL, cR, nM);
@@ -160,15 +162,16 @@ int env_update(int side, typename Scalar<CPLX>::T *out, const typename Scalar<CP
         h.M = (int)cL, h.N = (int)(cL * DL), h.K = (int)(d * cR), h.batch = 1;
         h.A = M2, h.lda = d * cR, h.B = Y, h.ldb = d * cR, h.C = out, h.ldc = cL;
         h.alpha = make_double2(1, 0), h.beta = make_double2(0, 0);
+        h.split_ws = split_ws, h.split_ws_bytes = split_bytes;
         HEFF_TRY(gemm_f64<CPLX>(true, false, false, h, s));
     }
     return HEFF_OK;
 }
 
 template int env_update<false>(int, double *, const double *, const int64_t *, const double *, const int64_t *, const double *, const int64_t *,
-                               double *, cudaStream_t);
+                               double *, cudaStream_t, void *, size_t);
 template int env_update<true>(int, double2 *, const double2 *, const int64_t *, const double2 *, const int64_t *, const double2 *,
-                              const int64_t *, double2 *, cudaStream_t);
+                              const int64_t *, double2 *, cudaStream_t, void *, size_t);
 
 template<bool CPLX>
 static int env_stateless(int side, void *out, const void *env, const int64_t ed[3], const void *mps, const int64_t md[3], const void *mpo,
@@ -180,10 +183,13 @@ static int env_stateless(int side, void *out, const void *env, const int64_t ed[
         return HEFF_BAD_ARG;
     }
     HEFF_TRY(check_env_dims(side, ed, md, wd));
-    void *base = nullptr;
-    HEFF_TRY(stream_workspace(s, (size_t)env_scratch_elems(md, wd) * sizeof(T), &base));
+    void        *base  = nullptr;
+    const size_t bytes = (size_t)env_scratch_elems(md, wd) * sizeof(T);
+    const size_t split = matvec_split_bytes(bytes);
+    HEFF_TRY(stream_workspace(s, bytes + split, &base));
     return env_update<CPLX>(side, reinterpret_cast<T *>(out), reinterpret_cast<const T *>(env), ed, reinterpret_cast<const T *>(mps), md,
-                            reinterpret_cast<const T *>(mpo), wd, reinterpret_cast<T *>(base), s);
+                            reinterpret_cast<const T *>(mpo), wd, reinterpret_cast<T *>(base), s, reinterpret_cast<unsigned char *>(base) + bytes,
+                            split);
 }
 
 }  // namespace heff

@@ -26,6 +26,14 @@ struct GemmArgs {
     void       *C;
     int64_t     ldc, sC;
     double2     alpha, beta;  // real GEMMs use .x
+    // Optional scratch for the tail split (set by the caller; nullptr or too small: no split).  When the
+    // tiles do not fill whole waves of the device, the tiles of the last partial wave are split along K
+    // into `split` pieces that write partial tiles to `part`; a second kernel sums the pieces in piece
+    // order (deterministic) and applies alpha/beta.  Set by the launcher: split, nfull, part.
+    void       *split_ws;
+    size_t      split_ws_bytes;
+    int         split, nfull;
+    void       *part;
 };
 
 template<bool CPLX>
@@ -56,6 +64,18 @@ struct GemmSmem {
 };
 
 constexpr int GROUP_M = 16;  // row panels per rasterisation group
+
+// Grouped rasterisation: consecutive tile ids walk GROUP_M row panels for every column panel, so the
+// CTAs resident at one time share their A and B panels in L2 instead of re-reading them from HBM.
+template<int BM, int BN>
+__device__ __forceinline__ void gemm_raster(int pid, int M, int N, int &tile_m, int &tile_n) {
+    const int num_m = (M + BM - 1) / BM, num_n = (N + BN - 1) / BN;
+    const int per_group = GROUP_M * num_n;
+    const int first_m   = (pid / per_group) * GROUP_M;
+    const int gsize     = min(num_m - first_m, GROUP_M);
+    tile_m              = first_m + (pid % per_group) % gsize;
+    tile_n              = (pid % per_group) / gsize;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -95,24 +115,24 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const GemmArgs p) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wm0 = (warp % (BM / WM)) * WM, wn0 = (warp / (BM / WM)) * WN;
-    // Grouped rasterisation: consecutive CTAs walk GROUP_M row panels for every column panel, so the
-    // CTAs resident at one time share their A and B panels in L2 instead of re-reading them from HBM.
-    int tile_m, tile_n;
-    {
-        const int num_m = (p.M + BM - 1) / BM, num_n = (p.N + BN - 1) / BN;
-        const int pid = blockIdx.x, per_group = GROUP_M * num_n;
-        const int first_m = (pid / per_group) * GROUP_M;
-        const int gsize   = min(num_m - first_m, GROUP_M);
-        tile_m            = first_m + (pid % per_group) % gsize;
-        tile_n            = (pid % per_group) / gsize;
+    const int M = p.M, N = p.N, K = p.K;
+    const int KT = (K + BK - 1) / BK;
+    // Tail split: CTAs past the first nfull tiles each take one K-range piece of a tail tile.
+    int tile_id = blockIdx.x, kt0 = 0, kt1 = KT, unit = -1;
+    if(p.split > 1 && tile_id >= p.nfull) {
+        unit            = tile_id - p.nfull;
+        const int piece = unit % p.split;
+        tile_id         = p.nfull + unit / p.split;
+        kt0             = (int)((int64_t)KT * piece / p.split);
+        kt1             = (int)((int64_t)KT * (piece + 1) / p.split);
     }
+    int tile_m, tile_n;
+    gemm_raster<BM, BN>(tile_id, M, N, tile_m, tile_n);
     const int m0 = tile_m * BM, n0 = tile_n * BN;
     const int bz = blockIdx.z;
     const T  *A  = reinterpret_cast<const T *>(p.A) + (int64_t)bz * p.sA;
     const T  *B  = reinterpret_cast<const T *>(p.B) + (int64_t)bz * p.sB;
     T        *C  = reinterpret_cast<T *>(p.C) + (int64_t)bz * p.sC;
-    const int M = p.M, N = p.N, K = p.K;
-    const int KT = (K + BK - 1) / BK;
 
     auto load_stage = [&](int stage, int kt) {
         T        *As = smem + stage * SM::STAGE;
@@ -167,19 +187,20 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const GemmArgs p) {
 
 #pragma unroll
     for(int s = 0; s < ST - 1; s++) {
-        if(s < KT) load_stage(s, s);
+        if(kt0 + s < kt1) load_stage(s, kt0 + s);
         cp_async_commit();
     }
 
-    for(int kt = 0; kt < KT; kt++) {
+    for(int kt = kt0; kt < kt1; kt++) {
+        const int it = kt - kt0;  // pipeline slot counter
         cp_async_wait<ST - 2>();
         __syncthreads();
         {
             const int nk = kt + ST - 1;
-            if(nk < KT) load_stage(nk % ST, nk);
+            if(nk < kt1) load_stage((it + ST - 1) % ST, nk);
             cp_async_commit();
         }
-        const T *As = smem + (kt % ST) * SM::STAGE;
+        const T *As = smem + (it % ST) * SM::STAGE;
         const T *Bs = As + SM::A_ELEMS;
 #pragma unroll
         for(int k4 = 0; k4 < BK; k4 += 4) {
@@ -220,6 +241,27 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const GemmArgs p) {
     }
     cp_async_wait<0>();
 
+    if(unit >= 0) {
+        // Tail piece: the raw partial tile, element (i, j, r) of thread tid at [(i NT + j) 4 + r] * 256 + tid
+        // (coalesced), summed by gemm_split_reduce_kernel.
+        T *P = reinterpret_cast<T *>(p.part) + (size_t)unit * (BM * BN);
+#pragma unroll
+        for(int i = 0; i < MT; i++)
+#pragma unroll
+            for(int j = 0; j < NT; j++)
+#pragma unroll
+                for(int r = 0; r < 4; r++) {
+                    const int e = (i * NT + j) * 4 + r;
+                    if constexpr(!CPLX) {
+                        P[e * 256 + tid] = acc[i][j][0][r];
+                    } else {
+                        const double t1 = acc[i][j][0][r], t2 = acc[i][j][1][r], t3 = acc[i][j][2][r];
+                        P[e * 256 + tid] = make_double2(t1 - t2, t3 - t1 - t2);
+                    }
+                }
+        return;
+    }
+
     // Epilogue: C = alpha*acc + beta*C (C is not read when beta == 0).
     const bool use_beta = (p.beta.x != 0.0) || (p.beta.y != 0.0);
 #pragma unroll
@@ -245,6 +287,83 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const GemmArgs p) {
                 }
             }
 }
+
+// Second pass of the tail split: sums each tail tile's `split` partial pieces in piece order (the same order on
+// every run) and writes C = alpha * sum + beta * C with the GEMM kernel's thread mapping.  Grid: (tail tiles,
+// EPT / EPB); each thread takes EPB of its tile elements and issues all EPB * split loads before any addition,
+// so the pass runs at memory bandwidth instead of one load latency per partial.
+constexpr int SPLIT_MAX = 16;
+template<bool CPLX>
+struct SplitReduce {
+    using G                 = GemmTile<CPLX>;
+    static constexpr int MT = G::WM / 16, NT = G::WN / 8;
+    static constexpr int EPT = MT * NT * 4;   // tile elements per thread
+    static constexpr int EPB = CPLX ? 2 : 4;  // elements per thread per CTA of the reduction
+};
+template<bool CPLX>
+__global__ void __launch_bounds__(256) gemm_split_reduce_kernel(const GemmArgs p) {
+    using G  = GemmTile<CPLX>;
+    using T  = typename Scalar<CPLX>::T;
+    using SR = SplitReduce<CPLX>;
+    constexpr int BM = G::BM, BN = G::BN, WM = G::WM, WN = G::WN, NT = SR::NT, EPB = SR::EPB;
+    const int     tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int     g = lane >> 2, t = lane & 3;
+    const int     wm0 = (warp % (BM / WM)) * WM, wn0 = (warp / (BM / WM)) * WN;
+    const int     tail = blockIdx.x, e0 = blockIdx.y * EPB;
+    int           tile_m, tile_n;
+    gemm_raster<BM, BN>(p.nfull + tail, p.M, p.N, tile_m, tile_n);
+    const int     m0 = tile_m * BM, n0 = tile_n * BN;
+    const T      *P  = reinterpret_cast<const T *>(p.part) + (size_t)tail * p.split * (BM * BN);
+    T            *C  = reinterpret_cast<T *>(p.C);
+    const bool    use_beta = (p.beta.x != 0.0) || (p.beta.y != 0.0);
+    const int     ns = p.split < SPLIT_MAX ? p.split : SPLIT_MAX;
+    T             w[EPB][SPLIT_MAX];
+#pragma unroll
+    for(int q = 0; q < SPLIT_MAX; q++)
+#pragma unroll
+        for(int u = 0; u < EPB; u++)
+            if(q < ns) w[u][q] = P[(size_t)q * (BM * BN) + (e0 + u) * 256 + tid];
+#pragma unroll
+    for(int u = 0; u < EPB; u++) {
+        const int e = e0 + u, r = e & 3, j = (e >> 2) % NT, i = (e >> 2) / NT;
+        T         v = w[u][0];
+#pragma unroll
+        for(int q = 1; q < SPLIT_MAX; q++)
+            if(q < ns) {
+                if constexpr(!CPLX)
+                    v += w[u][q];
+                else
+                    v = cadd(v, w[u][q]);
+            }
+        const int gm = m0 + wm0 + i * 16 + g + ((r >> 1) << 3);
+        const int gn = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+        if(gm < p.M && gn < p.N) {
+            T *cp = C + gm + (int64_t)gn * p.ldc;
+            if constexpr(!CPLX) {
+                double o = p.alpha.x * v;
+                if(use_beta) o += p.beta.x * (*cp);
+                *cp = o;
+            } else {
+                double2 o = cmul(p.alpha, v);
+                if(use_beta) o = cadd(o, cmul(p.beta, *cp));
+                *cp = o;
+            }
+        }
+    }
+}
+
+// Tail-split plan for a GEMM of `tiles` tiles of KT k-tiles on `slots` co-resident CTAs: the number of K pieces
+// (1 = no split) that minimises (whole waves + the pieces' rounds / split) plus the split's own cost, the
+// reduction launch and the partial tiles' HBM round trip measured against one tile's time `tile_s`; pieces
+// keep >= 4 k-tiles and their partials (unit_bytes each) fit `max_units`.
+struct SplitPlan {
+    int split = 1, nfull = 0;
+};
+SplitPlan gemm_split_plan(int64_t tiles, int KT, int64_t slots, int64_t max_units, double tile_s, double unit_bytes);
+
+// Bytes of tail-split scratch that let every GEMM of a matvec-sized problem pick its best split: at most
+// 4 * (co-resident CTAs) partial tiles of the larger (real) tile.
+size_t gemm_split_ws_bytes();
 
 // Host launcher.  Returns HEFF_OK or a status code; never synchronises.
 template<bool CPLX>

@@ -175,6 +175,8 @@ int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename
     g1.ldc   = d.cL * d.DL;
     g1.alpha = make_double2(1.0, 0.0);
     g1.beta  = make_double2(0.0, 0.0);
+    g1.split_ws       = ws.split_ws;
+    g1.split_ws_bytes = ws.split_bytes;
     HEFF_TRY(gemm_f64<CPLX>(/*ta=*/true, /*tb=*/false, false, g1, s));
     if(ev) HEFF_CUDA(cudaEventRecord(ev[2], s));
     HEFF_TRY(launch_mix<CPLX>(d, ws.T1, ws.T2, W, s));
@@ -192,6 +194,8 @@ int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename
     g2.ldc   = d.S * d.cL;
     g2.alpha = make_double2(1.0, 0.0);
     g2.beta  = make_double2(0.0, 0.0);
+    g2.split_ws       = ws.split_ws;
+    g2.split_ws_bytes = ws.split_bytes;
     HEFF_TRY(gemm_f64<CPLX>(false, false, false, g2, s));
     if(ev) HEFF_CUDA(cudaEventRecord(ev[4], s));
     return HEFF_OK;
@@ -401,11 +405,14 @@ static int matvec_stateless(void *res, const void *mps, const int64_t md[3], con
         set_last_error_msg("matvec: res must not alias mps");
         return HEFF_BAD_ARG;
     }
-    const int64_t elems = MatvecScratch<CPLX>::elems(d) + d.size_Rp();
+    const int64_t elems = MatvecScratch<CPLX>::elems(d) + MatvecScratch<CPLX>::pad(d.size_Rp());
+    const size_t  split = matvec_split_bytes((size_t)elems * sizeof(T));
     void         *base  = nullptr;
-    HEFF_TRY(stream_workspace(s, (size_t)elems * sizeof(T), &base));
+    HEFF_TRY(stream_workspace(s, (size_t)elems * sizeof(T) + split, &base));
     MatvecScratch<CPLX> ws;
     T                  *Rp = ws.carve(reinterpret_cast<T *>(base), d);
+    ws.split_ws           = reinterpret_cast<unsigned char *>(base) + (size_t)elems * sizeof(T);
+    ws.split_bytes        = split;
     HEFF_TRY(permute_R<CPLX>(reinterpret_cast<const T *>(envR), Rp, d, s));
     return matvec_fp64<CPLX>(d, reinterpret_cast<const T *>(mps), reinterpret_cast<T *>(res), reinterpret_cast<const T *>(envL), Rp,
                              reinterpret_cast<const T *>(mpo), ws, s);

@@ -32,6 +32,9 @@ template<bool CPLX>
 struct MatvecScratch {
     using T = typename Scalar<CPLX>::T;
     T *xp = nullptr, *T1 = nullptr, *T2 = nullptr;
+    // optional tail-split scratch of the two GEMMs (nullptr: every tile runs whole; see GemmArgs)
+    void  *split_ws    = nullptr;
+    size_t split_bytes = 0;
     // sub-buffers start on 256-byte boundaries so the GEMMs can use 16-byte copies
     static int64_t pad(int64_t n) { return (n + 31) / 32 * 32; }
     static int64_t elems(const MatvecDims &d) { return pad(d.size_mps()) + pad(d.size_T1()) + pad(d.size_T2()); }
@@ -42,6 +45,14 @@ struct MatvecScratch {
         return T2 + pad(d.size_T2());
     }
 };
+
+// Tail-split scratch to reserve beside a matvec scratch of `scratch_bytes`: enough partial tiles for the best
+// split of large GEMMs (gemm_split_ws_bytes), at least 16 MB so small-bond GEMMs with few tiles can split finely.
+inline size_t matvec_split_bytes(size_t scratch_bytes) {
+    const size_t cap = gemm_split_ws_bytes();
+    const size_t want = scratch_bytes > ((size_t)16 << 20) ? scratch_bytes : ((size_t)16 << 20);
+    return want < cap ? want : cap;
+}
 
 // Streams and events of the host-buffer matvec pipeline (matvec_fp64_host), owned by the operator.
 struct HostPipe {

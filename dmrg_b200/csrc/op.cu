@@ -197,6 +197,8 @@ static int create_impl(heff_op **out, int nsites, const void *const *mpos, const
     const int64_t nscr = MatvecScratch<CPLX>::elems(d);
     if(cudaMalloc(&op->scratch, nscr * es) != cudaSuccess) return fail(HEFF_OOM);
     op->scratch_bytes = (size_t)nscr * es;
+    op->split_bytes   = matvec_split_bytes(op->scratch_bytes);
+    if(cudaMalloc(&op->split_ws, op->split_bytes) != cudaSuccess) return fail(HEFF_OOM);
     void *Rtmp        = nullptr;
     if(cudaMalloc(&Rtmp, nR * es) != cudaSuccess) return fail(HEFF_OOM);
     (void)where;  // source location of each buffer is inferred from its address (unified addressing)
@@ -245,6 +247,8 @@ int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_
     if(cudaMalloc(&op->W, op->cap_W * es) != cudaSuccess) return fail(HEFF_OOM);
     if(cudaMalloc(&op->scratch, op->cap_scratch * es) != cudaSuccess) return fail(HEFF_OOM);
     op->scratch_bytes = (size_t)op->cap_scratch * es;
+    op->split_bytes   = matvec_split_bytes(op->scratch_bytes);
+    if(cudaMalloc(&op->split_ws, op->split_bytes) != cudaSuccess) return fail(HEFF_OOM);
     op->diag_cap      = S * cmax * cmax;
     if(cudaMalloc(&op->diag, op->diag_cap * es) != cudaSuccess) return fail(HEFF_OOM);
     *out              = op;
@@ -345,6 +349,8 @@ static int apply_impl(heff_op *op, const void *x, void *y) {
     }
     MatvecScratch<CPLX> ws;
     ws.carve(reinterpret_cast<T *>(op->scratch), op->d);
+    ws.split_ws    = op->split_ws;
+    ws.split_bytes = op->split_bytes;
     HEFF_TRY(matvec_fp64<CPLX>(op->d, reinterpret_cast<const T *>(x), reinterpret_cast<T *>(y), reinterpret_cast<const T *>(op->L),
                                reinterpret_cast<const T *>(op->Rp), reinterpret_cast<const T *>(op->W), ws, op->stream, op_prof_slot(op)));
     op->num_mv++;
@@ -381,6 +387,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->Rp) cudaFree(op->Rp);
     if(op->W) cudaFree(op->W);
     if(op->scratch) cudaFree(op->scratch);
+    if(op->split_ws) cudaFree(op->split_ws);
     if(op->stage_x) cudaFree(op->stage_x);
     if(op->eig_ws) cudaFree(op->eig_ws);
     if(op->Rtmp) cudaFree(op->Rtmp);

@@ -19,6 +19,8 @@ struct heff_op {
     std::vector<void *> seq_W;
     void              *scratch       = nullptr;                    // x' | T1 | T2
     size_t             scratch_bytes = 0;
+    void              *split_ws      = nullptr;  // tail-split partial tiles of the matvec GEMMs (matvec_split_bytes)
+    size_t             split_bytes   = 0;
     void              *stage_x       = nullptr;  // device staging for MultAx with host buffers
     size_t             stage_bytes   = 0;
     heff::HostPipe    *pipe          = nullptr;  // streams/events of the overlapped host-buffer matvec (created on first use)

@@ -60,6 +60,7 @@ size_t request_bytes(const heff_request &r, int max_basis) {
     auto          pad = [](int64_t v) { return (v + 31) / 32 * 32; };
     int64_t       b   = es * (cL * cL * DL + 2 * cR * cR * DR + DL * DR * S * S);  // L, R' (+ transient R), W
     b += es * (pad(n) + pad(DL * n) + pad(DR * n));                                 // x', T1, T2
+    b += (int64_t)matvec_split_bytes((size_t)(es * (pad(n) + pad(DL * n) + pad(DR * n))));  // GEMM tail-split partials
     const bool mixed = r.precision == HEFF_PREC_MIXED;
     if(mixed) {
         const int64_t nseg = r.dtype == HEFF_C128 ? 6 : 3;

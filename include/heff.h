@@ -272,6 +272,17 @@ int heff_gemm_i8_emu(int dtype, const void *A, const void *B, void *C, int64_t M
  * counterpart in the reference. */
 int heff_i8_set_tile_width(int bn);
 
+/* Tail split of the FP64 (DMMA) GEMMs of the matvec: when a GEMM's tiles leave
+ * the last wave of the device partly empty, the tiles of that wave are split
+ * along K into pieces whose partial tiles a second kernel sums in piece order.
+ * mode 0 = off, 1 = automatic (a cost model of waves, partial traffic and the
+ * extra launch; default), 2..16 = that many pieces whenever a wave is partial.
+ * The initial value comes from the environment variable HEFF_GEMM_SPLIT.  Results
+ * are deterministic for a given mode and device but differ from the unsplit
+ * product at the rounding level.  Returns the previous mode, or -1 for an invalid
+ * one.  Process-wide tuning knob; no counterpart in the reference. */
+int heff_gemm_set_tail_split(int mode);
+
 /* ---------------------------------------------------------------------------
  * Eigensolver (the caller side of MultAx: eig::solver, source/math/eig/solver.h:15-88)
  * ------------------------------------------------------------------------- */

@@ -157,7 +157,9 @@ def test_matvec_rejects_bad_shapes(cuda):
 @pytest.mark.parametrize("chiL,chiR,c", [(512, 512, False), (400, 371, True), (1400, 200, False)])
 def test_host_buffer_matvec_overlapped_path(cuda, chiL, chiR, c):
     """MultAx with host buffers of >= 8 MB takes the overlapped path (slabbed copies on a copy stream, two compute
-    streams): bit-identical to the device-pointer MultAx, with pageable and pinned buffers, call after call."""
+    streams).  Its slab GEMMs run every tile whole, while the device-pointer MultAx may split the tiles of a last
+    partial wave along K, so the two agree to rounding (1e-14 relative); each path is bit-identical call after call,
+    with pageable and pinned buffers."""
     th, W, L, R = ph.heff_inputs(chiL, D=3, cplx=c, seed=chiL + chiR, chiR=chiR)
     assert th.nbytes >= 8 << 20
     op = hb.MatVecMPOS([W], L, R, cplx=c)
@@ -166,14 +168,20 @@ def test_host_buffer_matvec_overlapped_path(cuda, chiL, chiR, c):
     op.MultAx(x, y)
     torch.cuda.synchronize()
     y_dev = y.cpu().numpy()
+    y_first = None
     for _ in range(2):
         y_host = op.MultAx_host(th).ravel(order="F")
-        assert np.array_equal(y_host, y_dev)
+        if y_first is None:
+            y_first = y_host
+        assert np.array_equal(y_host, y_first)
+        assert relerr(y_host, y_dev) < 1e-14
         op.MultAx(x, y)  # interleaved device-pointer call on the same operator
+        torch.cuda.synchronize()
+        assert np.array_equal(y.cpu().numpy(), y_dev)
     # pinned buffers through the C ABI
     xp = torch.from_numpy(np.ascontiguousarray(th.ravel(order="F"))).pin_memory()
     yp = torch.empty_like(xp).pin_memory()
     hb.check(hb.lib().heff_op_multax_host(op.handle, hb.ptr(xp), hb.ptr(yp)), "multax_host")
-    assert np.array_equal(yp.numpy(), y_dev)
+    assert np.array_equal(yp.numpy(), y_first)
     assert relerr(y_dev.reshape(th.shape, order="F"), rn.matvec_blas(th, W, L, R)) < TOL
     op.close()

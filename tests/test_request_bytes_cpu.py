@@ -68,3 +68,19 @@ def test_int8_tile_width_knob():
         assert L.heff_i8_set_tile_width(0) == 128
     finally:
         L.heff_i8_set_tile_width(prev)
+
+
+def test_gemm_tail_split_knob():
+    """heff_gemm_set_tail_split accepts 0 (off), 1 (automatic) or a piece count 2..16, returns the previous mode,
+    rejects the rest."""
+    L = hb.lib()
+    prev = L.heff_gemm_set_tail_split(1)
+    try:
+        assert 0 <= prev <= 16
+        assert L.heff_gemm_set_tail_split(0) == 1
+        assert L.heff_gemm_set_tail_split(4) == 0
+        assert L.heff_gemm_set_tail_split(17) == -1
+        assert L.heff_gemm_set_tail_split(-1) == -1
+        assert L.heff_gemm_set_tail_split(1) == 4
+    finally:
+        L.heff_gemm_set_tail_split(prev)
