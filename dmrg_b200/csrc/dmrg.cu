@@ -287,7 +287,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
                 auto    ts0 = now();
                 int64_t k   = 0;
                 double  te  = 0;
-                HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_max, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s, ws.op->split_ws, ws.op->split_bytes));
+                HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_max, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s));
                 res.trunc_err_max = std::max(res.trunc_err_max, te);
                 res.svd_sweeps_max = std::max(res.svd_sweeps_max, last_svd_sweeps());
                 if(i + 1 == L / 2 && sweep == cfg.sweeps - 1) {
