@@ -402,6 +402,73 @@ class EigServer:
             pass
 
 
+def two_site_ising_mpo(D, cplx, h1=0.8, h2=1.2, J=1.0):
+    """Merged two-site random-field Ising MPO (D=3; IsingRandomField.cpp:122-129, merged as matvec_mpos.cpp:104-119)
+    or the merged uncompressed MPO squared (D=9; MpoSite.cpp:57-70), Fortran-ordered [D, D, 4, 4] numpy."""
+    def site(h):
+        W = np.zeros((3, 3, 2, 2))
+        sx = np.array([[0.0, 1.0], [1.0, 0.0]])
+        sz = np.array([[1.0, 0.0], [0.0, -1.0]])
+        W[0, 0] = np.eye(2)
+        W[1, 0] = sz
+        W[2, 0] = -h * sx
+        W[2, 1] = -J * sz
+        W[2, 2] = np.eye(2)
+        return W
+
+    def square(W):
+        return np.einsum("mnsp,MNpt->mMnNst", W, W).reshape(9, 9, 2, 2, order="F")
+
+    if D not in (3, 9):
+        raise ValueError("D must be 3 (H) or 9 (H squared)")
+    WA, WB = site(h1), site(h2)
+    if D == 9:
+        WA, WB = square(WA), square(WB)
+    X = np.einsum("mcst,cnuv->mnsutv", WA, WB)
+    W = X.reshape(WA.shape[0], WB.shape[1], 4, 4, order="F")
+    return np.asfortranarray(W.astype(np.complex128 if cplx else np.float64))
+
+
+def serve_specs(specs, hbm_budget_bytes=None, max_inflight=8, max_basis=24, wait_timeout=3600.0):
+    """Runs a stream of synthetic eigensolve requests through one EigServer on this process's GPU.
+
+    specs: list of dicts with chi, D (3: H, lowest eigenpair; 9: H squared, lowest eigenpair of the folded
+    operator), cplx, seed and optionally precision (PREC_FP64), tol (1e-10), arrival (seconds after the first
+    submit; requests are submitted in list order, each not before its arrival time).  Environments (Hermitian
+    slices, seeded) and start vectors are generated on the device before the stream starts.  Returns
+    (list of response dicts, list of status codes, wall seconds of the stream, server stats)."""
+    import time
+
+    torch = _torch()
+    reqs = []
+    for sp in specs:
+        chi, D, cplx, seed = int(sp["chi"]), int(sp["D"]), bool(sp["cplx"]), int(sp["seed"])
+        envL = make_env(chi, D, cplx, seed=2 * seed, swap_base=3 if D == 9 else 0)
+        envR = make_env(chi, D, cplx, seed=2 * seed + 1, swap_base=3 if D == 9 else 0)
+        th0 = make_vector(4 * chi * chi, cplx, seed=7 * seed + 3)
+        reqs.append(EigServer.request(two_site_ising_mpo(D, cplx), envL, envR, 4, chi, chi, cplx, theta0=th0,
+                                      tol=float(sp.get("tol", 1e-10)), precision=int(sp.get("precision", PREC_FP64))))
+    torch.cuda.synchronize()
+    if hbm_budget_bytes is None:
+        free, _ = torch.cuda.mem_get_info()
+        hbm_budget_bytes = int(0.8 * free)
+    srv = EigServer(hbm_budget_bytes=hbm_budget_bytes, max_inflight=max_inflight, max_basis=max_basis)
+    try:
+        t0 = time.perf_counter()
+        ids = []
+        for sp, r in zip(specs, reqs):
+            dt = float(sp.get("arrival", 0.0)) - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(srv.submit(r))
+        resp = [srv.wait(i, timeout=wait_timeout) for i in ids]
+        secs = time.perf_counter() - t0
+        st = srv.stats()
+    finally:
+        srv.close()
+    return resp, [r["status"] for r in resp], secs, st
+
+
 class MatVecMPOS:
     """MatVecMPOS<T> (matvec_mpos.h:23-180): operator object handed to an eigensolver.
 
