@@ -464,43 +464,34 @@ def measure_eigs_folded(hb, torch, chi=512):
     return out
 
 
-def measure_serving(hb, torch, n_req, chi_lo, chi_hi, rate, precision, seed=2024):
-    """Bounded sample of the serving stream: Poisson arrivals at `rate`/s, chi log-uniform in [chi_lo, chi_hi],
-    70% float64 / 30% complex128, D=3 requests target the lowest eigenpair, D=9 requests (MPO squared) the
-    lowest eigenpair of the folded operator; envs Hermitian (seeded Gaussians, generated on the device),
-    resident on the device; tol 1e-10.  Returns p50/p99 latency, solves/s and the server's peak concurrency."""
+def serving_specs(n_req, chi_lo, chi_hi, rate, precision, seed=2024):
+    """The serving stream's requests: Poisson arrivals at `rate`/s, chi log-uniform in [chi_lo, chi_hi], 70% float64 /
+    30% complex128, D=3 (H, lowest eigenpair) or D=9 (MPO squared: lowest eigenpair of the folded operator) with equal
+    probability, tol 1e-10, each request's environments and start vector seeded by its index."""
     rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     specs = []
     for i in range(n_req):
         chi = int(round(np.exp(rng.uniform(np.log(chi_lo), np.log(chi_hi)))))
         D = 3 if rng.uniform() < 0.5 else 9
-        cplx = rng.uniform() < 0.3
-        specs.append((chi, D, cplx))
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-    reqs = []
-    for i, (chi, D, cplx) in enumerate(specs):
-        envL = hb.make_env(chi, D, cplx, seed=seed * 1000 + 2 * i, swap_base=3 if D == 9 else 0)
-        envR = hb.make_env(chi, D, cplx, seed=seed * 1000 + 2 * i + 1, swap_base=3 if D == 9 else 0)
-        th0 = hb.make_vector(4 * chi * chi, cplx, seed=seed * 1000 + 7 * i)
-        reqs.append(hb.EigServer.request(two_site_mpo(D, cplx), envL, envR, 4, chi, chi, cplx, theta0=th0, tol=1e-10, precision=precision))
-    torch.cuda.synchronize()
-    free, total = torch.cuda.mem_get_info()
-    srv = hb.EigServer(hbm_budget_bytes=int(0.8 * free), max_inflight=8)
-    t0 = time.perf_counter()
-    ids = []
-    for a, r in zip(arrivals, reqs):
-        dt = a - (time.perf_counter() - t0)
-        if dt > 0:
-            time.sleep(dt)
-        ids.append(srv.submit(r))
-    resp = [srv.wait(i, timeout=600) for i in ids]
-    st = srv.stats()
-    srv.close()
-    ok = sum(1 for r in resp if r["status"] == 0)
+        cplx = bool(rng.uniform() < 0.3)
+        specs.append({"chi": chi, "D": D, "cplx": cplx, "seed": seed * 100003 + i, "precision": precision, "tol": 1e-10,
+                      "arrival": float(arrivals[i] - arrivals[0])})
+    return specs
+
+
+def measure_serving(hb, torch, n_req, chi_lo, chi_hi, rate, precision, seed=2024, max_inflight=8):
+    """The serving stream through one EigServer (hb.serve_specs): p50/p99 latency, solves/s, the server's peak
+    concurrency and what its slot arenas hold."""
+    specs = serving_specs(n_req, chi_lo, chi_hi, rate, precision, seed)
+    resp, st_codes, secs, st = hb.serve_specs(specs, max_inflight=max_inflight, wait_timeout=1800)
+    ok = sum(1 for c in st_codes if c == 0)
     return {"requests": n_req, "answered_ok": ok, "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
-            "max_latency_s": st["max_latency_s"], "solves_per_s": st["solves_per_s"], "peak_inflight": st["peak_inflight"],
-            "peak_device_bytes": st["peak_bytes"], "arrival_rate_per_s": rate, "chi_range": [chi_lo, chi_hi],
-            "eigvals_head": [r["eigval"] for r in resp[:4]]}
+            "max_latency_s": st["max_latency_s"], "solves_per_s": st["solves_per_s"], "stream_seconds": secs,
+            "p50_latency_from_arrival_s": st.get("p50_latency_from_arrival_s"), "p99_latency_from_arrival_s": st.get("p99_latency_from_arrival_s"),
+            "peak_inflight": st["peak_inflight"], "peak_device_bytes": st["peak_bytes"], "arena_bytes": st["arena_bytes"],
+            "arena_grows": st["arena_grows"], "arrival_rate_per_s": rate, "chi_range": [chi_lo, chi_hi],
+            "chi_max_served": max(s["chi"] for s in specs), "eigvals_head": [r["eigval"] for r in resp[:4]]}
 
 
 def splitmix_fields(seed, L, lo=0.5, hi=1.5):

@@ -429,43 +429,68 @@ def two_site_ising_mpo(D, cplx, h1=0.8, h2=1.2, J=1.0):
     return np.asfortranarray(W.astype(np.complex128 if cplx else np.float64))
 
 
-def serve_specs(specs, hbm_budget_bytes=None, max_inflight=8, max_basis=24, wait_timeout=3600.0):
+def serve_specs(specs, hbm_budget_bytes=None, max_inflight=8, max_basis=24, wait_timeout=3600.0, max_pending_bytes=16 << 30):
     """Runs a stream of synthetic eigensolve requests through one EigServer on this process's GPU.
 
     specs: list of dicts with chi, D (3: H, lowest eigenpair; 9: H squared, lowest eigenpair of the folded
-    operator), cplx, seed and optionally precision (PREC_FP64), tol (1e-10), arrival (seconds after the first
-    submit; requests are submitted in list order, each not before its arrival time).  Environments (Hermitian
-    slices, seeded) and start vectors are generated on the device before the stream starts.  Returns
-    (list of response dicts, list of status codes, wall seconds of the stream, server stats)."""
+    operator), cplx, seed and optionally precision (PREC_FP64), tol (1e-10), arrival (seconds after the stream
+    starts; requests are submitted in list order, each not before its arrival time).  A request's environments
+    (Hermitian slices, seeded) and start vector are generated on the device when it arrives and released once it is
+    answered; while the generated inputs of unanswered requests exceed `max_pending_bytes`, the next arrival waits
+    for the oldest answer (its latency from arrival then includes that wait).  Returns (list of response dicts,
+    list of status codes, wall seconds of the stream, server stats plus the latency percentiles measured from each
+    request's arrival time)."""
+    import collections
     import time
 
     torch = _torch()
-    reqs = []
-    for sp in specs:
-        chi, D, cplx, seed = int(sp["chi"]), int(sp["D"]), bool(sp["cplx"]), int(sp["seed"])
-        envL = make_env(chi, D, cplx, seed=2 * seed, swap_base=3 if D == 9 else 0)
-        envR = make_env(chi, D, cplx, seed=2 * seed + 1, swap_base=3 if D == 9 else 0)
-        th0 = make_vector(4 * chi * chi, cplx, seed=7 * seed + 3)
-        reqs.append(EigServer.request(two_site_ising_mpo(D, cplx), envL, envR, 4, chi, chi, cplx, theta0=th0,
-                                      tol=float(sp.get("tol", 1e-10)), precision=int(sp.get("precision", PREC_FP64))))
+    n = len(specs)
     torch.cuda.synchronize()
     if hbm_budget_bytes is None:
+        torch.cuda.empty_cache()
         free, _ = torch.cuda.mem_get_info()
-        hbm_budget_bytes = int(0.8 * free)
+        hbm_budget_bytes = max(int(0.85 * free) - int(max_pending_bytes), 1 << 30)
     srv = EigServer(hbm_budget_bytes=hbm_budget_bytes, max_inflight=max_inflight, max_basis=max_basis)
+    resp = [None] * n
+    pending = collections.deque()
+    pend_bytes = 0
+
+    def settle_oldest():
+        nonlocal pend_bytes
+        j, rid, keep, nb = pending.popleft()
+        resp[j] = srv.wait(rid, timeout=wait_timeout)
+        pend_bytes -= nb
+        del keep
+
     try:
         t0 = time.perf_counter()
-        ids = []
-        for sp, r in zip(specs, reqs):
+        for i, sp in enumerate(specs):
+            chi, D, cplx, seed = int(sp["chi"]), int(sp["D"]), bool(sp["cplx"]), int(sp["seed"])
+            nb = (2 * chi * chi * D + 4 * chi * chi) * (16 if cplx else 8)
+            while pending and pend_bytes + nb > max_pending_bytes:
+                settle_oldest()
             dt = float(sp.get("arrival", 0.0)) - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            ids.append(srv.submit(r))
-        resp = [srv.wait(i, timeout=wait_timeout) for i in ids]
+            envL = make_env(chi, D, cplx, seed=2 * seed, swap_base=3 if D == 9 else 0)
+            envR = make_env(chi, D, cplx, seed=2 * seed + 1, swap_base=3 if D == 9 else 0)
+            th0 = make_vector(4 * chi * chi, cplx, seed=7 * seed + 3)
+            req = EigServer.request(two_site_ising_mpo(D, cplx), envL, envR, 4, chi, chi, cplx, theta0=th0,
+                                    tol=float(sp.get("tol", 1e-10)), precision=int(sp.get("precision", PREC_FP64)))
+            torch.cuda.current_stream().synchronize()  # the inputs are complete before the server reads them
+            pending.append((i, srv.submit(req), req, nb))
+            pend_bytes += nb
+        while pending:
+            settle_oldest()
         secs = time.perf_counter() - t0
         st = srv.stats()
     finally:
         srv.close()
+    start = min(r["t_submit"] for r in resp) if resp else 0.0
+    lat = sorted(r["t_done"] - (start + float(sp.get("arrival", 0.0))) for r, sp in zip(resp, specs))
+    if lat:
+        st["p50_latency_from_arrival_s"] = lat[min(len(lat) - 1, int(0.50 * (len(lat) - 1) + 0.5))]
+        st["p99_latency_from_arrival_s"] = lat[min(len(lat) - 1, int(0.99 * (len(lat) - 1) + 0.5))]
     return resp, [r["status"] for r in resp], secs, st
 
 

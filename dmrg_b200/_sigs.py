@@ -73,7 +73,8 @@ class Response(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("queued", ctypes.c_int64), ("inflight", ctypes.c_int),
                 ("peak_inflight", ctypes.c_int), ("peak_bytes", ctypes.c_size_t), ("p50_latency_s", ctypes.c_double),
-                ("p99_latency_s", ctypes.c_double), ("max_latency_s", ctypes.c_double), ("solves_per_s", ctypes.c_double)]
+                ("p99_latency_s", ctypes.c_double), ("max_latency_s", ctypes.c_double), ("solves_per_s", ctypes.c_double),
+                ("arena_bytes", ctypes.c_size_t), ("arena_grows", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -189,6 +189,7 @@ struct DmrgWorkspace {
             op->fp64_engine = HEFF_FP64_INT8;
             HEFF_TRY(emu_reserve(op, d * d, chi, Dmax));  // digit planes for the largest bond, once
         }
+        if(prec == HEFF_PREC_MIXED) HEFF_TRY(mixed_reserve(op, mixed_bytes(d * d, chi, chi, Dmax, Dmax, false)));  // split operands, once
         heff_eig_config ec;
         heff_eig_config_default(&ec);
         return eig_reserve(op, d * d * chi * chi, ec.max_basis, prec == HEFF_PREC_MIXED);

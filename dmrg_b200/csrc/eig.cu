@@ -577,6 +577,11 @@ static int eigs_impl(heff_op *op, const heff_eig_config &cfg, const void *x0, vo
     return conv ? HEFF_OK : HEFF_NOT_CONVERGED;
 }
 
+size_t eig_workspace_bytes(int64_t n, int max_basis, bool mixed, bool cplx) {
+    const int maxb = std::max(4, std::min(max_basis > 0 ? max_basis : 32, (int)MD_MAXK - 1));
+    return cplx ? Davidson<true>::workspace_bytes(n, maxb, mixed) : Davidson<false>::workspace_bytes(n, maxb, mixed);
+}
+
 // Pre-sizes the operator's eigensolver workspace for problems up to n_max elements (so that solves on a
 // rebound operator never allocate).
 int eig_reserve(heff_op *op, int64_t n_max, int max_basis, bool mixed) {

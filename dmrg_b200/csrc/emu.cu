@@ -138,6 +138,8 @@ int emu_reserve(heff_op *op, int64_t S, int64_t cmax, int64_t Dmax) {
     return emu_alloc(op, st, z.total(), e.M2);
 }
 
+size_t emu_held_bytes(const heff_op *op) { return op->emu ? reinterpret_cast<const EmuState *>(op->emu)->cap : 0; }
+
 size_t emu_bytes(int64_t S, int64_t cL, int64_t cR, int64_t DL, int64_t DR, bool cplx, int nslices) {
     EmuDims e;
     e.cf = cplx ? 2 : 1;

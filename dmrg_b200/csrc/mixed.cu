@@ -34,6 +34,10 @@ struct MixedState {
     unsigned char *wl  = nullptr;  // the MPO's nonzero list (wlist.cuh layout)
     int            wl_bytes = 0;
     CUtensorMap    tA1, tB1, tA2, tB2;
+    // every buffer above is carved from one pooled allocation that persists across rebinds (grown, never shrunk)
+    void          *pool  = nullptr;
+    size_t         cap   = 0;
+    bool           stale = true;  // the split operands belong to other environments (set by a rebind)
 };
 
 __device__ __forceinline__ void split2(double v, __nv_bfloat16 &h, __nv_bfloat16 &m) {
@@ -275,27 +279,86 @@ static int g1(int64_t n) {
 }
 static int64_t r64(int64_t v) { return (v + 63) / 64 * 64; }
 
+// Byte sizes of the split operands, the FP32 T1 and the flags of one operator shape, each rounded to 256 bytes
+// (in carve order: A1, B1, A2, B2, T1, err, wl).
+struct MixedSizes {
+    size_t b[7];
+    size_t total() const {
+        size_t t = 0;
+        for(size_t v : b) t += v;
+        return t;
+    }
+};
+static size_t up256m(size_t v) { return (v + 255) / 256 * 256; }
+static MixedSizes mixed_sizes(int64_t S, int64_t cL, int64_t cR, int64_t DL, int64_t DR, bool cplx) {
+    const int64_t nseg = cplx ? 6 : 3, cf = cplx ? 2 : 1;
+    const int64_t M1 = cL * DL, N1 = S * cR, Kx1 = nseg * r64(cL);
+    const int64_t M2 = S * cL, N2 = cR, Kx2 = nseg * r64(cR * DR);
+    MixedSizes    z;
+    z.b[0] = up256m(2 * (size_t)M1 * Kx1);
+    z.b[1] = up256m(2 * (size_t)(cf * N1) * Kx1);
+    z.b[2] = up256m(2 * (size_t)M2 * Kx2);
+    z.b[3] = up256m(2 * (size_t)(cf * N2) * Kx2);
+    z.b[4] = up256m(4 * (size_t)M1 * (cf * N1));
+    z.b[5] = 256;
+    z.b[6] = up256m(wlist_bytes((int)DL, (int)DR, (int)S, cplx ? 16 : 8));
+    return z;
+}
+
+size_t mixed_bytes(int64_t S, int64_t cL, int64_t cR, int64_t DL, int64_t DR, bool cplx) { return mixed_sizes(S, cL, cR, DL, DR, cplx).total(); }
+
 static void mixed_destroy(heff_op *op) {
     MixedState *m = reinterpret_cast<MixedState *>(op->mixed);
     if(!m) return;
-    if(m->A1) cudaFree(m->A1);
-    if(m->B1) cudaFree(m->B1);
-    if(m->A2) cudaFree(m->A2);
-    if(m->B2) cudaFree(m->B2);
-    if(m->T1) cudaFree(m->T1);
-    if(m->err) cudaFree(m->err);
-    if(m->wl) cudaFree(m->wl);
+    if(m->pool) cudaFree(m->pool);
     delete m;
     op->mixed = nullptr;
 }
 
+void mixed_invalidate(heff_op *op) {
+    if(op->mixed) reinterpret_cast<MixedState *>(op->mixed)->stale = true;
+}
+
+size_t mixed_held_bytes(const heff_op *op) { return op->mixed ? reinterpret_cast<const MixedState *>(op->mixed)->cap : 0; }
+
+static MixedState *mixed_state(heff_op *op) {
+    if(!op->mixed) {
+        op->mixed        = new MixedState();
+        op->destroy_hook = mixed_destroy;
+    }
+    return reinterpret_cast<MixedState *>(op->mixed);
+}
+
+// Grows the pooled buffer to at least `bytes` (stream-synchronised free of the old one; nothing when it is
+// large enough already).
+static int mixed_grow(heff_op *op, MixedState *m, size_t bytes) {
+    if(m->cap >= bytes) return HEFF_OK;
+    if(m->pool) {
+        HEFF_CUDA(cudaStreamSynchronize(op->stream));
+        cudaFree(m->pool);
+        m->pool = nullptr;
+        m->cap  = 0;
+    }
+    cudaError_t e = cudaMalloc(&m->pool, bytes);
+    if(e != cudaSuccess) {
+        m->pool = nullptr;
+        set_last_cuda_error(e, "mixed-precision buffers", __FILE__, __LINE__);
+        return HEFF_OOM;
+    }
+    m->cap   = bytes;
+    m->stale = true;
+    return HEFF_OK;
+}
+
+int mixed_reserve(heff_op *op, size_t bytes) { return mixed_grow(op, mixed_state(op), bytes); }
+
+// Lays the split operands of the operator's current shape out in the pooled buffer (grown when needed), splits
+// L and R' into them and builds the tensor maps.  Runs on the first mixed matvec after a create or a rebind.
 template<bool CPLX>
 static int mixed_setup(heff_op *op) {
     using T         = typename Scalar<CPLX>::T;
     const auto &d   = op->d;
-    MixedState *m   = new MixedState();
-    op->mixed       = m;
-    op->destroy_hook = mixed_destroy;
+    MixedState *m   = mixed_state(op);
     m->cplx         = CPLX;
     m->nseg         = CPLX ? 6 : 3;
     const int cf    = CPLX ? 2 : 1;
@@ -309,29 +372,18 @@ static int mixed_setup(heff_op *op) {
     m->K2           = d.cR * d.DR;
     m->Kp2          = r64(m->K2);
     m->Kx2          = m->nseg * m->Kp2;
-    const size_t bA1 = 2 * (size_t)m->M1 * m->Kx1, bB1 = 2 * (size_t)(cf * m->N1) * m->Kx1;
-    const size_t bA2 = 2 * (size_t)m->M2 * m->Kx2, bB2 = 2 * (size_t)(cf * m->N2) * m->Kx2;
-    const size_t bT1 = 4 * (size_t)m->M1 * (cf * m->N1);
-    auto         al  = [&](void **p, size_t b) -> int {
-        cudaError_t e = cudaMalloc(p, b);
-        if(e != cudaSuccess) {
-            set_last_cuda_error(e, "mixed-precision buffers", __FILE__, __LINE__);
-            return HEFF_OOM;
-        }
-        return HEFF_OK;
-    };
-    HEFF_TRY(al((void **)&m->A1, bA1));
-    HEFF_TRY(al((void **)&m->B1, bB1));
-    HEFF_TRY(al((void **)&m->A2, bA2));
-    HEFF_TRY(al((void **)&m->B2, bB2));
-    HEFF_TRY(al((void **)&m->T1, bT1));
-    HEFF_TRY(al((void **)&m->err, sizeof(int)));
+    const MixedSizes z = mixed_sizes(d.S, d.cL, d.cR, d.DL, d.DR, CPLX);
+    HEFF_TRY(mixed_grow(op, m, z.total()));
+    unsigned char *p = reinterpret_cast<unsigned char *>(m->pool);
+    void         **dst[7] = {(void **)&m->A1, (void **)&m->B1, (void **)&m->A2, (void **)&m->B2, (void **)&m->T1, (void **)&m->err, (void **)&m->wl};
+    for(int i = 0; i < 7; i++) {
+        *dst[i] = p;
+        p += z.b[i];
+    }
     cudaStream_t s = op->stream;
-    // K padding of every segment stays zero for the life of the buffers
-    HEFF_CUDA(cudaMemsetAsync(m->A1, 0, bA1, s));
-    HEFF_CUDA(cudaMemsetAsync(m->B1, 0, bB1, s));
-    HEFF_CUDA(cudaMemsetAsync(m->A2, 0, bA2, s));
-    HEFF_CUDA(cudaMemsetAsync(m->B2, 0, bB2, s));
+    // K padding of every segment must read zero: the split operands (and the padding the kernels never write) are
+    // cleared whenever the layout is (re)built, since the pool may hold another shape's values
+    HEFF_CUDA(cudaMemsetAsync(m->pool, 0, z.b[0] + z.b[1] + z.b[2] + z.b[3], s));
     HEFF_CUDA(cudaMemsetAsync(m->err, 0, sizeof(int), s));
     split_L_kernel<CPLX><<<g1(m->K1 * m->M1), 256, 0, s>>>(reinterpret_cast<const T *>(op->L), m->A1, d.cL, m->M1, m->Kp1, m->Kx1);
     HEFF_LAUNCH_CHECK();
@@ -343,7 +395,6 @@ static int mixed_setup(heff_op *op) {
     HEFF_TRY(make_tmap_bf16(&m->tB2, m->B2, cf * m->N2, m->Kx2, m->Kx2, X_BN));
 
     m->wl_bytes = (int)wlist_bytes((int)d.DL, (int)d.DR, (int)d.S, sizeof(T));
-    HEFF_TRY(al((void **)&m->wl, (size_t)m->wl_bytes));
     wlist_global_kernel<T><<<1, 32, 0, s>>>(reinterpret_cast<const T *>(op->W), (int)d.DL, (int)d.DR, (int)d.S, m->wl);
     HEFF_LAUNCH_CHECK();
     const int    ta       = mx_ta(d.DL * d.S, cf);
@@ -351,14 +402,14 @@ static int mixed_setup(heff_op *op) {
     if(mix_smem > 200 * 1024) return HEFF_BAD_SHAPE;
     HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     HEFF_CUDA(cudaFuncSetAttribute(mix_mixed_kernel<CPLX, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    HEFF_CUDA(cudaStreamSynchronize(s));
+    m->stale = false;
     return HEFF_OK;
 }
 
 template<bool CPLX>
 static int mixed_apply_impl(heff_op *op, const void *x, void *y) {
     using T = typename Scalar<CPLX>::T;
-    if(!op->mixed) HEFF_TRY(mixed_setup<CPLX>(op));
+    if(!op->mixed || reinterpret_cast<MixedState *>(op->mixed)->stale) HEFF_TRY(mixed_setup<CPLX>(op));
     MixedState  *m  = reinterpret_cast<MixedState *>(op->mixed);
     const auto  &d  = op->d;
     cudaStream_t s  = op->stream;

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "matvec.cuh"
+#include "eig.cuh"
 #include "gemm_i8.cuh"
 #include "op.cuh"
 #include "runtime.cuh"
@@ -262,7 +263,7 @@ static int rebind_impl(heff_op *op, int nsites, const void *const *mpos_host, co
                        const void *envR, const int64_t rd[3]) {
     using T  = typename Scalar<CPLX>::T;
     using HT = typename std::conditional<CPLX, HostC, double>::type;
-    if(op->mixed && op->destroy_hook) op->destroy_hook(op);  // split operands belong to the old environments
+    mixed_invalidate(op);                                      // split operands belong to the old environments (re-split in place)
     op->emu_stale  = true;                                     // so do the digit planes of L and R' (rebuilt in place)
     op->diag_ready = false;
     std::vector<HT> W;
@@ -308,6 +309,125 @@ int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64
     if(op->cap_env == 0) return HEFF_BAD_ARG;
     return op->cplx ? rebind_impl<true>(op, nsites, mpos_host, mdims, envL, ld, envR, rd)
                     : rebind_impl<false>(op, nsites, mpos_host, mdims, envL, ld, envR, rd);
+}
+
+ArenaBytes ArenaBytes::max_with(const ArenaBytes &o) const {
+    ArenaBytes m;
+    m.env     = std::max(env, o.env);
+    m.W       = std::max(W, o.W);
+    m.scratch = std::max(scratch, o.scratch);
+    m.split   = std::max(split, o.split);
+    m.diag    = std::max(diag, o.diag);
+    m.mixed   = std::max(mixed, o.mixed);
+    m.emu     = std::max(emu, o.emu);
+    m.eig     = std::max(eig, o.eig);
+    m.vec     = std::max(vec, o.vec);
+    return m;
+}
+
+ArenaBytes arena_need(const heff_request &r, int max_basis) {
+    const bool       cplx = r.dtype == HEFF_C128;
+    const size_t     es   = cplx ? 16 : 8;
+    const MatvecDims d{r.spin, r.chiL, r.chiR, r.mpoL, r.mpoR};
+    ArenaBytes       a;
+    a.env     = es * (size_t)std::max(d.cL * d.cL * d.DL, d.size_Rp());
+    a.W       = es * (size_t)(d.DL * d.DR * d.S * d.S);
+    a.scratch = es * (size_t)(cplx ? MatvecScratch<true>::elems(d) : MatvecScratch<false>::elems(d));
+    a.split   = matvec_split_bytes(a.scratch);
+    a.diag    = es * (size_t)d.size_mps();
+    const bool mixed = r.precision == HEFF_PREC_MIXED;
+    if(mixed) a.mixed = mixed_bytes(d.S, d.cL, d.cR, d.DL, d.DR, cplx);
+    if(r.fp64_engine == HEFF_FP64_INT8) a.emu = emu_bytes(d.S, d.cL, d.cR, d.DL, d.DR, cplx, Z_DEFAULT_SLICES);
+    a.eig = eig_workspace_bytes(d.size_mps(), max_basis, mixed, cplx);
+    a.vec = 2 * es * (size_t)d.size_mps();
+    return a;
+}
+
+ArenaBytes arena_held(const heff_op *op) {
+    ArenaBytes a;
+    a.env     = op->cap_env_b;
+    a.W       = op->cap_W_b;
+    a.scratch = op->cap_scratch_b;
+    a.split   = op->cap_split_b;
+    a.diag    = op->cap_diag_b;
+    a.mixed   = mixed_held_bytes(op);
+    a.emu     = emu_held_bytes(op);
+    a.eig     = op->eig_ws_bytes;
+    a.vec     = op->arena_vec_b;
+    return a;
+}
+
+int op_create_arena(heff_op **out, cudaStream_t stream) {
+    if(!out) return HEFF_BAD_ARG;
+    heff_op *op     = new heff_op();
+    op->arena       = true;
+    op->stream      = stream;
+    op->mixed_apply = mixed_apply;
+    *out            = op;
+    return HEFF_OK;
+}
+
+// Replaces *p by a buffer of `need` bytes when *cap is smaller (stream-synchronised free of the old buffer).
+static int arena_grow(heff_op *op, void **p, size_t *cap, size_t need, const char *what) {
+    if(*cap >= need) return HEFF_OK;
+    if(*p) {
+        HEFF_CUDA(cudaStreamSynchronize(op->stream));
+        cudaFree(*p);
+        *p   = nullptr;
+        *cap = 0;
+    }
+    cudaError_t e = cudaMalloc(p, need);
+    if(e != cudaSuccess) {
+        *p = nullptr;
+        set_last_cuda_error(e, what, __FILE__, __LINE__);
+        return HEFF_OOM;
+    }
+    *cap = need;
+    return HEFF_OK;
+}
+
+int op_arena_bind(heff_op *op, const heff_request &r, int max_basis, void **vec) {
+    if(!op || !op->arena || !vec || !r.mpo || !r.envL || !r.envR) return HEFF_BAD_ARG;
+    if(r.dtype != HEFF_F64 && r.dtype != HEFF_C128) return HEFF_BAD_ARG;
+    const bool       cplx = r.dtype == HEFF_C128;
+    const ArenaBytes need = arena_need(r, max_basis);
+    size_t           env_cap = op->cap_env_b;
+    // L, R' and the R staging share one capacity
+    if(env_cap < need.env) {
+        size_t c = env_cap;
+        HEFF_TRY(arena_grow(op, &op->L, &c, need.env, "arena envL"));
+        c = env_cap;
+        HEFF_TRY(arena_grow(op, &op->Rp, &c, need.env, "arena envR"));
+        c = env_cap;
+        HEFF_TRY(arena_grow(op, &op->Rtmp, &c, need.env, "arena envR staging"));
+        op->cap_env_b = need.env;
+    }
+    HEFF_TRY(arena_grow(op, &op->W, &op->cap_W_b, need.W, "arena MPO"));
+    HEFF_TRY(arena_grow(op, &op->scratch, &op->cap_scratch_b, need.scratch, "arena matvec scratch"));
+    HEFF_TRY(arena_grow(op, &op->split_ws, &op->cap_split_b, need.split, "arena tail-split partials"));
+    op->split_bytes = need.split;  // this request's own share: the GEMMs' split plans (and rounding) do not depend on the arena's history
+    HEFF_TRY(arena_grow(op, &op->diag, &op->cap_diag_b, need.diag, "arena preconditioner diagonal"));
+    HEFF_TRY(arena_grow(op, &op->arena_vec, &op->arena_vec_b, need.vec, "arena start/result vectors"));
+    if(cplx != op->cplx) op->emu_stale = true;
+    op->cplx          = cplx;
+    const size_t es   = cplx ? 16 : 8;
+    op->cap_env       = (int64_t)(op->cap_env_b / es);
+    op->cap_W         = (int64_t)(op->cap_W_b / es);
+    op->cap_scratch   = (int64_t)(op->cap_scratch_b / es);
+    op->scratch_bytes = op->cap_scratch_b;
+    op->diag_cap      = (int64_t)(op->cap_diag_b / es);
+    op->precision     = r.precision == HEFF_PREC_MIXED ? HEFF_PREC_MIXED : HEFF_PREC_FP64;
+    if(need.mixed) HEFF_TRY(mixed_reserve(op, need.mixed));
+    HEFF_TRY(heff_op_set_fp64_engine(op, r.fp64_engine == HEFF_FP64_INT8 ? HEFF_FP64_INT8 : HEFF_FP64_DMMA, 0));
+    if(need.emu) HEFF_TRY(emu_reserve(op, r.spin, std::max(r.chiL, r.chiR), std::max(r.mpoL, r.mpoR)));
+    const void   *mp[1] = {r.mpo};
+    const int64_t md[4] = {r.mpoL, r.mpoR, r.spin, r.spin};
+    const int64_t ld[3] = {r.chiL, r.chiL, r.mpoL};
+    const int64_t rd[3] = {r.chiR, r.chiR, r.mpoR};
+    HEFF_TRY(op_rebind(op, 1, mp, md, r.envL, ld, r.envR, rd));
+    HEFF_TRY(eig_reserve(op, op->d.size_mps(), max_basis, r.precision == HEFF_PREC_MIXED));
+    *vec = op->arena_vec;
+    return HEFF_OK;
 }
 
 int op_prof_flush(heff_op *op) {
@@ -391,6 +511,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->stage_x) cudaFree(op->stage_x);
     if(op->eig_ws) cudaFree(op->eig_ws);
     if(op->Rtmp) cudaFree(op->Rtmp);
+    if(op->arena_vec) cudaFree(op->arena_vec);
     for(void *p : op->seq_W) cudaFree(p);
     if(op->pipe) {
         if(op->pipe->aux) cudaStreamDestroy(op->pipe->aux);

@@ -29,6 +29,12 @@ struct heff_op {
     int64_t            cap_env = 0, cap_W = 0, cap_scratch = 0;
     void              *Rtmp    = nullptr;
     std::vector<unsigned char> w_host;
+    // arena operators (server slots, op_create_arena): byte capacities of the buffers above and of the
+    // start/result vector pair; cap_env/cap_W/cap_scratch/diag_cap follow from them for the bound dtype
+    bool               arena = false;
+    size_t             cap_env_b = 0, cap_W_b = 0, cap_scratch_b = 0, cap_diag_b = 0, cap_split_b = 0;
+    void              *arena_vec   = nullptr;
+    size_t             arena_vec_b = 0;
     // eigensolver workspace, kept across heff_eigs calls on this operator (grown on demand)
     void              *eig_ws       = nullptr;
     size_t             eig_ws_bytes = 0;
@@ -60,6 +66,11 @@ namespace heff {
 int op_apply(heff_op *op, const void *x, void *y);
 int mixed_apply(heff_op *op, const void *x, void *y);     // mixed.cu
 int mixed_error_flag(heff_op *op, int *flag);              // mixed.cu
+void mixed_invalidate(heff_op *op);                        // mixed.cu: split operands are rebuilt on the next mixed matvec
+int mixed_reserve(heff_op *op, size_t bytes);              // mixed.cu: pooled split-operand buffer of at least `bytes`
+size_t mixed_bytes(int64_t S, int64_t cL, int64_t cR, int64_t DL, int64_t DR, bool cplx);  // mixed.cu: pool bytes of one shape
+size_t mixed_held_bytes(const heff_op *op);                // mixed.cu
+size_t eig_workspace_bytes(int64_t n, int max_basis, bool mixed, bool cplx);  // eig.cu: Davidson workspace of one solve
 bool emu_supported(const heff_op *op);                     // emu.cu: both GEMMs within the exact-INT32 range
 int emu_apply(heff_op *op, const void *x, void *y);        // emu.cu
 int emu_error_flag(heff_op *op, int *flag);                // emu.cu
@@ -67,6 +78,22 @@ void emu_destroy(heff_op *op);                             // emu.cu
 int emu_reserve(heff_op *op, int64_t S, int64_t cmax, int64_t Dmax);  // emu.cu: digit-plane buffer for the largest bond
 size_t emu_bytes(int64_t S, int64_t cL, int64_t cR, int64_t DL, int64_t DR, bool cplx, int nslices);  // emu.cu
 int op_create_capacity(heff_op **out, bool cplx, int64_t S, int64_t cmax, int64_t Dmax, heff_precision prec, cudaStream_t stream);
+size_t emu_held_bytes(const heff_op *op);  // emu.cu: bytes of the digit-plane buffer
+
+// Arena operators (one per eigensolve-server slot): every device buffer is kept across requests and grown only when
+// a request needs more, so a request costs no cudaMalloc/cudaFree (which synchronise the whole device) once the
+// arena has grown to the stream's sizes.  Byte capacities, so one arena serves real and complex requests.
+struct ArenaBytes {
+    size_t env = 0, W = 0, scratch = 0, split = 0, diag = 0, mixed = 0, emu = 0, eig = 0, vec = 0;
+    size_t total() const { return 3 * env + W + scratch + split + diag + mixed + emu + eig + vec; }
+    ArenaBytes max_with(const ArenaBytes &o) const;
+};
+ArenaBytes arena_need(const heff_request &r, int max_basis);  // bytes each buffer needs for this request
+ArenaBytes arena_held(const heff_op *op);                      // bytes each buffer holds now
+int op_create_arena(heff_op **out, cudaStream_t stream);
+// Grows the arena to cover `r`, binds its MPO and environments (copied onto the device, stream-ordered) and sets its
+// dtype, precision and FP64 engine.  *vec receives a device buffer of 2 * rows elements (start vector and result).
+int op_arena_bind(heff_op *op, const heff_request &r, int max_basis, void **vec);
 int op_rebind(heff_op *op, int nsites, const void *const *mpos_host, const int64_t *mdims, const void *envL, const int64_t ld[3], const void *envR,
               const int64_t rd[3]);
 int eig_host_ready(heff_op *op);     // eig.cu: pinned coefficient buffer + event of the Krylov loop

@@ -1,13 +1,18 @@
 // Site-optimisation eigensolve server: continuous batching of H_eff eigensolves on one GPU.
 //
 // No counterpart in the reference (DMRG++ solves one site problem at a time on the calling thread,
-// solver_primme.cpp:298-517).  Requests are queued; `max_inflight` worker threads, each with its own
-// CUDA stream, take the first queued request that fits into the remaining device-memory budget
-// (first-fit admission, so a small request is not stuck behind one that does not fit yet), build its
-// operator (environments resident on the device for the whole solve), run the eigensolver and copy
-// the result out.  Requests that arrive while others are on the GPU are admitted as soon as a slot
-// and memory free up; their kernels overlap on the device.  Every kernel on the path reduces in a
-// fixed order, so a request's result does not depend on what else is running.
+// solver_primme.cpp:298-517).  Requests are queued; `max_inflight` worker threads (slots), each with its
+// own CUDA stream and its own arena operator, take the first queued request that fits into the remaining
+// device-memory budget (first-fit admission, so a small request is not stuck behind one that does not fit
+// yet), bind it to the arena (environments copied onto the device, resident for the whole solve), run the
+// eigensolver and copy the result out.  The arena keeps every device buffer from one request to the next
+// and grows only when a request needs more, so once it has grown to the stream's sizes a request costs no
+// cudaMalloc or cudaFree: those synchronise the whole device and would stall every other slot's stream.
+// The budget counts what the arenas hold (idle ones included); an idle slot gives its arena back when a
+// queued request does not fit otherwise.  Requests that arrive while others are on the GPU are admitted
+// as soon as a slot and memory free up; their kernels overlap on the device.  Every kernel on the path
+// reduces in a fixed order, so a request's result does not depend on what else is running or on which
+// slot ran it.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -28,18 +33,23 @@ struct heff_server {
     std::mutex                        mu;
     std::condition_variable           cv_work, cv_done;
     struct Item {
-        int64_t      id;
-        heff_request req;
-        size_t       bytes;
-        double       t_submit;
+        int64_t          id;
+        heff_request     req;
+        heff::ArenaBytes need;  // per-buffer bytes this request needs in an arena
+        double           t_submit;
     };
+    struct Slot {
+        heff_op *op   = nullptr;  // arena operator (op_create_arena), owned by the slot's worker thread
+        size_t   held = 0;        // bytes its arena holds (counted in `used`)
+    };
+    std::vector<Slot>                 slots;
     std::deque<Item>                  queue;
     std::map<int64_t, heff_response>  done;
     std::vector<double>               latencies;
     std::vector<std::thread>          workers;
     size_t                            used = 0, peak_used = 0;
     int                               inflight = 0, peak_inflight = 0;
-    int64_t                           next_id = 1, completed = 0, failed = 0;
+    int64_t                           next_id = 1, completed = 0, failed = 0, arena_grows = 0;
     double                            t_first = -1, t_last = 0, busy_overlap = 0;
     bool                              stop = false;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -48,61 +58,45 @@ struct heff_server {
 
 namespace heff {
 
-static int64_t r64(int64_t v) { return (v + 63) / 64 * 64; }
+// Slack per arena for the few small buffers the estimate does not itemise (row maxima of the INT8 engine's
+// accumulators, flags).
+static constexpr size_t kArenaSlack = (size_t)4 << 20;
+
+static bool request_dims_ok(const heff_request &r) { return r.spin > 0 && r.chiL > 0 && r.chiR > 0 && r.mpoL > 0 && r.mpoR > 0; }
 
 // Device memory one request holds while it runs (operator copies + matvec scratch + mixed-precision
-// split operands or INT8-engine digit planes + eigensolver basis), matching the allocations in op.cu,
-// mixed.cu, emu.cu and eig.cu.
+// split operands or INT8-engine digit planes + eigensolver basis + start/result vectors): the per-buffer sizes
+// the arena allocates for it (arena_need, computed by the same functions that size the buffers).
 size_t request_bytes(const heff_request &r, int max_basis) {
-    const int64_t es = r.dtype == HEFF_C128 ? 16 : 8, cf = r.dtype == HEFF_C128 ? 2 : 1;
-    const int64_t S = r.spin, cL = r.chiL, cR = r.chiR, DL = r.mpoL, DR = r.mpoR;
-    const int64_t n = S * cL * cR;
-    auto          pad = [](int64_t v) { return (v + 31) / 32 * 32; };
-    int64_t       b   = es * (cL * cL * DL + 2 * cR * cR * DR + DL * DR * S * S);  // L, R' (+ transient R), W
-    b += es * (pad(n) + pad(DL * n) + pad(DR * n));                                 // x', T1, T2
-    b += (int64_t)matvec_split_bytes((size_t)(es * (pad(n) + pad(DL * n) + pad(DR * n))));  // GEMM tail-split partials
-    const bool mixed = r.precision == HEFF_PREC_MIXED;
-    if(mixed) {
-        const int64_t nseg = r.dtype == HEFF_C128 ? 6 : 3;
-        b += 2 * (cL * DL) * nseg * r64(cL) + 2 * cf * (S * cR) * nseg * r64(cL);      // A1, B1
-        b += 2 * (S * cL) * nseg * r64(cR * DR) + 2 * cf * cR * nseg * r64(cR * DR);   // A2, B2
-        b += 4 * (cL * DL) * cf * (S * cR);                                            // T1 (fp32)
-    }
-    if(r.fp64_engine == HEFF_FP64_INT8) b += (int64_t)emu_bytes(S, cL, cR, DL, DR, r.dtype == HEFF_C128, Z_DEFAULT_SLICES);  // digit planes
-    const int64_t vec = (es * n + 255) / 256 * 256;
-    b += vec * (2 * (max_basis + 1) + 2 * max_basis + 4 + (mixed ? 5 : 0)) + (int64_t)(es * 128 * 131) + 8 * 512 * 128 * 4;
-    return (size_t)b + (size_t)(4 << 20);
+    if(!request_dims_ok(r)) return 0;
+    return arena_need(r, max_basis).total() + kArenaSlack;
 }
 
-static void run_request(heff_server *srv, heff_server::Item &it, cudaStream_t stream, heff_response &out) {
-    const heff_request &r = it.req;
-    out.id                = it.id;
-    out.t_submit          = it.t_submit;
-    out.t_start           = srv->now();
-    const void   *mp[1]   = {r.mpo};
-    const int64_t md[4]   = {r.mpoL, r.mpoR, r.spin, r.spin};
-    const int64_t ld[3]   = {r.chiL, r.chiL, r.mpoL};
-    const int64_t rd[3]   = {r.chiR, r.chiR, r.mpoR};
-    heff_op      *op      = nullptr;
-    int rc = heff_op_create(&op, (heff_dtype)r.dtype, 1, mp, md, r.envL, ld, r.envR, rd, (heff_mem)r.env_where, (heff_precision)r.precision, stream);
-    if(rc == HEFF_OK && r.fp64_engine != HEFF_FP64_DMMA) rc = heff_op_set_fp64_engine(op, r.fp64_engine, 0);
+static int server_basis(const heff_server *srv) { return srv->cfg.max_basis > 0 ? srv->cfg.max_basis : 24; }
+
+static void run_request(heff_server *srv, heff_server::Item &it, heff_op *op, heff_response &out) {
+    const heff_request &r      = it.req;
+    cudaStream_t        stream = op->stream;
+    out.id                     = it.id;
+    out.t_submit               = it.t_submit;
+    out.t_start                = srv->now();
+    void *vec                  = nullptr;
+    int   rc                   = op_arena_bind(op, r, server_basis(srv), &vec);
     if(rc == HEFF_OK) {
         heff_eig_config cfg;
         heff_eig_config_default(&cfg);
-        cfg.ritz   = r.ritz;
-        cfg.target = r.target;
-        cfg.tol    = r.tol > 0 ? r.tol : 1e-10;
-        cfg.mixed  = r.precision == HEFF_PREC_MIXED;
-        cfg.max_basis = srv->cfg.max_basis > 0 ? srv->cfg.max_basis : 24;
+        cfg.ritz      = r.ritz;
+        cfg.target    = r.target;
+        cfg.tol       = r.tol > 0 ? r.tol : 1e-10;
+        cfg.mixed     = r.precision == HEFF_PREC_MIXED;
+        cfg.max_basis = server_basis(srv);
         const size_t es   = r.dtype == HEFF_C128 ? 16 : 8;
         const size_t nb   = (size_t)op->d.size_mps() * es;
+        void        *xout = vec;
         void        *x0   = nullptr;
-        void        *xout = nullptr;
-        if(cudaMalloc(&xout, 2 * nb) != cudaSuccess) rc = HEFF_OOM;
-        if(rc == HEFF_OK && r.theta0) {
-            x0 = reinterpret_cast<char *>(xout) + nb;
-            if(cudaMemcpyAsync(x0, r.theta0, nb, cudaMemcpyDefault, stream) != cudaSuccess)
-                rc = HEFF_CUDA_ERROR;
+        if(r.theta0) {
+            x0 = reinterpret_cast<char *>(vec) + nb;
+            if(cudaMemcpyAsync(x0, r.theta0, nb, cudaMemcpyDefault, stream) != cudaSuccess) rc = HEFF_CUDA_ERROR;
         }
         heff_eig_result er;
         std::memset(&er, 0, sizeof(er));
@@ -115,42 +109,68 @@ static void run_request(heff_server *srv, heff_server::Item &it, cudaStream_t st
         out.num_mv       = er.num_mv;
         out.num_mv_mixed = er.num_mv_mixed;
         out.converged    = er.converged;
-        if(xout) cudaFree(xout);
-        heff_op_destroy(op);
     }
     out.status = rc;
     out.t_done = srv->now();
 }
 
-static void worker_main(heff_server *srv) {
+static void worker_main(heff_server *srv, int k) {
     cudaSetDevice(srv->cfg.device);
     cudaStream_t stream = nullptr;
     cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    heff_server::Slot &slot = srv->slots[k];
+    op_create_arena(&slot.op, stream);
     std::unique_lock<std::mutex> lock(srv->mu);
     while(true) {
-        auto fit = srv->queue.end();
-        for(auto itq = srv->queue.begin(); itq != srv->queue.end(); ++itq)
-            if(srv->used + itq->bytes <= srv->cfg.hbm_budget_bytes) {
-                fit = itq;
+        auto   fit      = srv->queue.end();
+        size_t new_held = 0;
+        for(auto itq = srv->queue.begin(); itq != srv->queue.end(); ++itq) {
+            const size_t t = arena_held(slot.op).max_with(itq->need).total() + kArenaSlack;
+            if(srv->used - slot.held + t <= srv->cfg.hbm_budget_bytes) {
+                fit      = itq;
+                new_held = t;
                 break;
             }
+        }
         if(fit == srv->queue.end()) {
             if(srv->stop && srv->queue.empty()) break;
+            if(!srv->queue.empty() && slot.held > 0) {
+                // memory pressure: nothing queued fits next to what the arenas hold, so this idle slot gives its arena back
+                heff_op *old = slot.op;
+                srv->used -= slot.held;
+                slot.held = 0;
+                slot.op   = nullptr;
+                lock.unlock();
+                heff_op_destroy(old);
+                op_create_arena(&slot.op, stream);
+                lock.lock();
+                srv->cv_work.notify_all();
+                continue;
+            }
             srv->cv_work.wait(lock);
             continue;
         }
         heff_server::Item it = *fit;
         srv->queue.erase(fit);
-        srv->used += it.bytes;
+        srv->used += new_held - slot.held;
+        slot.held = new_held;
         srv->inflight++;
         srv->peak_used     = std::max(srv->peak_used, srv->used);
         srv->peak_inflight = std::max(srv->peak_inflight, srv->inflight);
+        const size_t before = arena_held(slot.op).total();
         lock.unlock();
         heff_response resp;
         std::memset(&resp, 0, sizeof(resp));
-        run_request(srv, it, stream, resp);
+        run_request(srv, it, slot.op, resp);
+        const size_t after  = arena_held(slot.op).total();
+        const size_t actual = after + kArenaSlack;
         lock.lock();
-        srv->used -= it.bytes;
+        if(after > before) srv->arena_grows++;
+        if(actual > slot.held) {  // the estimate missed a buffer: count what the arena really holds
+            srv->used += actual - slot.held;
+            slot.held      = actual;
+            srv->peak_used = std::max(srv->peak_used, srv->used);
+        }
         srv->inflight--;
         if(resp.status == HEFF_OK || resp.status == HEFF_NOT_CONVERGED) {
             srv->completed++;
@@ -163,7 +183,11 @@ static void worker_main(heff_server *srv) {
         srv->cv_done.notify_all();
         srv->cv_work.notify_all();
     }
+    srv->used -= slot.held;
+    slot.held = 0;
     lock.unlock();
+    heff_op_destroy(slot.op);
+    slot.op = nullptr;
     cudaStreamDestroy(stream);
 }
 
@@ -189,7 +213,8 @@ extern "C" int heff_server_create(const heff_server_config *cfg, heff_server **o
         delete srv;
         return HEFF_BAD_ARG;
     }
-    for(int i = 0; i < srv->cfg.max_inflight; i++) srv->workers.emplace_back(worker_main, srv);
+    srv->slots.resize(srv->cfg.max_inflight);
+    for(int i = 0; i < srv->cfg.max_inflight; i++) srv->workers.emplace_back(worker_main, srv, i);
     *out = srv;
     return HEFF_OK;
 }
@@ -198,8 +223,10 @@ extern "C" size_t heff_request_bytes(const heff_request *req, int max_basis) { r
 
 extern "C" int heff_server_submit(heff_server *srv, const heff_request *req, int64_t *id) {
     if(!srv || !req || !id || !req->mpo || !req->envL || !req->envR) return HEFF_BAD_ARG;
-    if(req->spin <= 0 || req->chiL <= 0 || req->chiR <= 0 || req->mpoL <= 0 || req->mpoR <= 0) return HEFF_BAD_SHAPE;
-    const size_t bytes = request_bytes(*req, srv->cfg.max_basis > 0 ? srv->cfg.max_basis : 24);
+    if(!request_dims_ok(*req)) return HEFF_BAD_SHAPE;
+    if(req->dtype != HEFF_F64 && req->dtype != HEFF_C128) return HEFF_BAD_ARG;
+    const ArenaBytes need  = arena_need(*req, server_basis(srv));
+    const size_t     bytes = need.total() + kArenaSlack;
     std::lock_guard<std::mutex> lock(srv->mu);
     if(srv->stop) return HEFF_BAD_ARG;
     *id = srv->next_id++;
@@ -214,7 +241,7 @@ extern "C" int heff_server_submit(heff_server *srv, const heff_request *req, int
         srv->cv_done.notify_all();
         return HEFF_OK;  // the request is answered (status HEFF_OOM), the server stays up
     }
-    heff_server::Item it{*id, *req, bytes, srv->now()};
+    heff_server::Item it{*id, *req, need, srv->now()};
     if(srv->t_first < 0) srv->t_first = it.t_submit;
     srv->queue.push_back(it);
     srv->cv_work.notify_one();
@@ -242,6 +269,8 @@ extern "C" int heff_server_get_stats(heff_server *srv, heff_server_stats *st) {
     st->inflight      = srv->inflight;
     st->peak_inflight = srv->peak_inflight;
     st->peak_bytes    = srv->peak_used;
+    st->arena_bytes   = srv->used;
+    st->arena_grows   = srv->arena_grows;
     std::vector<double> l = srv->latencies;
     std::sort(l.begin(), l.end());
     auto pct = [&](double p) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)(p * (l.size() - 1) + 0.5))]; };

@@ -416,6 +416,10 @@ typedef struct {
     int     inflight, peak_inflight;
     size_t  peak_bytes;
     double  p50_latency_s, p99_latency_s, max_latency_s, solves_per_s;
+    /* slot arenas: device bytes they hold now, and how many requests had to grow one (a growth frees and
+     * reallocates buffers, which synchronises the device; a stream of sizes seen before grows none) */
+    size_t  arena_bytes;
+    int64_t arena_grows;
 } heff_server_stats;
 
 void   heff_server_config_default(heff_server_config *cfg);
