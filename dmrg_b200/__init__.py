@@ -242,14 +242,16 @@ def schmidt_multisite(theta, dL, dR, chiL, chiR, rank_max=0, trunc_lim=1e-12, st
     return U[: m * k], S[:k], V[: k * n], k, float(err.value)
 
 
-def xdmrg(h, energy_target, **kw):
-    """Excited-state DMRG (folded spectrum): the eigenstate closest to energy_target (heff_dmrg_run, algorithm 1)."""
-    return fdmrg(h, energy_shift_per_site=energy_target / len(h), algorithm=1, **kw)
+def xdmrg(h, energy_target, one_site=False, **kw):
+    """Excited-state DMRG (folded spectrum): the eigenstate closest to energy_target (heff_dmrg_run, algorithm 1, or 3:
+    one-site with subspace expansion)."""
+    return fdmrg(h, energy_shift_per_site=energy_target / len(h), algorithm=3 if one_site else 1, **kw)
 
 
 def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, precision=PREC_FP64, seed=0, ritz="SA", target=0.0,
-          energy_shift_per_site=0.0, algorithm=0, precond=-1, fp64_engine=FP64_DMMA, stream=None):
-    """Two-site DMRG of the random-field Ising chain on the device (heff_dmrg_run); returns the result dict."""
+          energy_shift_per_site=0.0, algorithm=0, precond=-1, fp64_engine=FP64_DMMA, expansion_alpha=0.0, stream=None):
+    """DMRG of the random-field Ising chain on the device (heff_dmrg_run); returns the result dict.  algorithm 0: two-site
+    ground state, 1: two-site folded spectrum, 2 / 3: the same with one-site DMRG and forward subspace expansion."""
     from ._sigs import DmrgConfig, DmrgResult
 
     hs = np.ascontiguousarray(np.asarray(h, dtype=np.float64))
@@ -270,6 +272,7 @@ def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, preci
     cfg.algorithm = int(algorithm)
     cfg.precond = int(precond)
     cfg.fp64_engine = int(fp64_engine)
+    cfg.expansion_alpha = float(expansion_alpha)
     res = DmrgResult()
     check(lib().heff_dmrg_run(ctypes.byref(cfg), ctypes.byref(res), _stream_handle(stream)), "heff_dmrg_run")
     return res.as_dict()
@@ -594,8 +597,19 @@ class MatVecMPOS:
         check(lib().heff_op_diagonal(self.handle, ptr(out)), "heff_op_diagonal")
         return out
 
+    def set_jacobi_blocksize(self, block_size):
+        """Block size of the Jacobi preconditioner (set_jcbMaxBlockSize, matvec_mpos.h:147): 1 = diagonal."""
+        check(lib().heff_op_set_jacobi_blocksize(self.handle, int(block_size)), "heff_op_set_jacobi_blocksize")
+
+    def jacobi_singular(self):
+        """Pivots of the block-Jacobi inversion that were floored (0 for a well-conditioned preconditioner)."""
+        c = ctypes.c_int(0)
+        check(lib().heff_op_jacobi_singular(self.handle, ctypes.byref(c)), "heff_op_jacobi_singular")
+        return int(c.value)
+
     def MultPc(self, x, y, shift):
-        """Jacobi preconditioner y = x / (diag - shift) (MultPc, matvec_mpos.cpp:1349-1364); device tensors."""
+        """Jacobi preconditioner (MultPc, matvec_mpos.cpp:1349-1416); device tensors.  Block size 1: y = x / (diag - shift);
+        block size > 1: y_blk = (H[blk, blk] - shift0 I)^-1 x_blk with shift0 the shift of the first call."""
         check(lib().heff_op_multpc(self.handle, ptr(x), ptr(y), float(shift)), "heff_op_multpc")
 
     def device_error(self):

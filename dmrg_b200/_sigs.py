@@ -33,7 +33,7 @@ class DmrgConfig(ctypes.Structure):
     _fields_ = [("L", ctypes.c_int), ("J", ctypes.c_double), ("h", _DP), ("chi_max", ctypes.c_int64), ("sweeps", ctypes.c_int),
                 ("trunc_lim", ctypes.c_double), ("eig_tol", ctypes.c_double), ("ritz", ctypes.c_int), ("target", ctypes.c_double),
                 ("precision", ctypes.c_int), ("seed", ctypes.c_int64), ("energy_shift_per_site", ctypes.c_double), ("algorithm", ctypes.c_int),
-                ("precond", ctypes.c_int), ("fp64_engine", ctypes.c_int)]
+                ("precond", ctypes.c_int), ("fp64_engine", ctypes.c_int), ("expansion_alpha", ctypes.c_double)]
 
 
 class DmrgResult(ctypes.Structure):
@@ -97,6 +97,8 @@ def declare(L, sig):
         sig(L, n, _I, [_P, _P, _I64P, _I, ctypes.POINTER(_P), _I64P, _P, _I64P, _P, _I64P, _P])
     sig(L, "heff_dense_eig", _I, [_I, _I64, _P, _I64, _P, _P, _P])
     sig(L, "heff_op_multpc", _I, [_P, _P, _P, ctypes.c_double])
+    sig(L, "heff_op_set_jacobi_blocksize", _I, [_P, _I64])
+    sig(L, "heff_op_jacobi_singular", _I, [_P, ctypes.POINTER(ctypes.c_int)])
     sig(L, "heff_gemm_bf16_f32", _I, [_P, _P, _P, _I64, _I64, _I64, _P])
     sig(L, "heff_gemm_i8_emu", _I, [_I, _P, _P, _P, _I64, _I64, _I64, _I, _P])
     sig(L, "heff_i8_set_tile_width", _I, [_I])

@@ -31,6 +31,10 @@
 
 namespace heff {
 
+template<bool CPLX>
+int expansion_term(int side, typename Scalar<CPLX>::T *P, const typename Scalar<CPLX>::T *B, const int64_t ed[3], const typename Scalar<CPLX>::T *M,
+                   const int64_t md[3], const typename Scalar<CPLX>::T *W, const int64_t wd[4], double alpha, cudaStream_t s);  // expansion.cu
+
 // The environment updates of a sweep run on the operator's stream between its matvecs, so they share the operator's
 // tail-split scratch.
 static int env_update_d(int side, double *out, const double *E, const int64_t ed[3], const double *M, const int64_t md[3], const double *W,
@@ -142,6 +146,20 @@ struct DmrgWorkspace {
     std::vector<double *> M, Lenv, Renv, W;
     double *theta = nullptr, *Cbuf = nullptr, *P2 = nullptr, *U = nullptr, *S = nullptr, *V = nullptr, *scr = nullptr, *red = nullptr;
     heff_op *op = nullptr;
+    // one-site DMRG with subspace expansion (algorithms 2 and 3): expansion term, enlarged-bond matrix and its
+    // transpose, SVD factors and GEMM temporaries, each d (1 + Dmax) chi^2 elements, and the SVD scratch
+    double *eP = nullptr, *eX = nullptr, *eT = nullptr, *eU = nullptr, *eV = nullptr, *eY = nullptr, *eZ = nullptr, *escr = nullptr;
+    bool    onesite = false;
+    int init_onesite() {
+        if(onesite) return HEFF_OK;
+        const int64_t d = 2, chi = chicap;
+        const size_t  big = (size_t)(d * (1 + Dcap) * chi * chi) + 64;
+        for(double **p : {&eP, &eX, &eT, &eU, &eV, &eY, &eZ}) HEFF_TRY(get(p, big));
+        const int64_t m = (1 + Dcap) * chi, n = d * chi;
+        HEFF_TRY(get(&escr, (size_t)(svd_scratch_bytes(m, n, 8) / 8) + 64));
+        onesite = true;
+        return HEFF_OK;
+    }
     ~DmrgWorkspace() {
         if(op) heff_op_destroy(op);
         for(void *p : ptrs) cudaFree(p);
@@ -383,11 +401,357 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     return HEFF_OK;
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// One-site DMRG with forward subspace expansion (algorithm 2: ground state of H; algorithm 3: lowest eigenpair of
+// the energy-shifted (H - E_t)^2, the folded spectrum of xDMRG).  The reference's default single-site strategy
+// (settings.h:225) with expand_environment_1site (tools/finite/env/env.cpp:1034-1262) before each local
+// optimisation: moving right at site i, the next site B(i+1) is enriched with the expansion term of the
+// operator being optimised, P = alpha * (env_R . B(i+1) . W(i+1)) (EnvBase::get_expansion_term), the rows
+// [B(i+1); P] of the enlarged left bond are decomposed as U S V (rank <= min(d chi_i, d chi_{i+2}, chi_max),
+// trunc_lim), B(i+1) <- V and the centre AC(i) <- [AC(i), 0] U S (merge_expansion_term_PR, case [AC, B]); the
+// state is unchanged up to that truncation, but the optimisation of AC(i) now sees the enriched environment.
+// Moving left mirrors it with [A(i-1), P_L] (merge_expansion_term_PL, case [A, AC]).  The R-side term is read
+// by its index meaning [s', b', (a, m)]: heff_expansion_term_* reproduces the reference's bytes, whose final
+// reshape to [spin, chiL*DL, chiR] reinterprets that order when chiR > 1.
+// Mixing factor: the DMRG3S schedule (Hubig, McCulloch, Schollwoeck, Wolf, PRB 91, 155115 (2015)) in place of the
+// reference's optimally mixed block (get_optimally_mixed_block_1site): alpha = expansion_alpha (default 1e-3)
+// halved every sweep and switched off for the last two sweeps, so the final sweeps converge the fixed basis.
+// ---------------------------------------------------------------------------------------------------------------
+
+// X[a2 + c2 (s + d b)] (c2 = c (1 + DL)): rows a2 < c are B[s + d (a2 + c b)], rows c + (a + c m) the R-side
+// expansion term P[s + d (b + cb (a + c m))]
+__global__ void ex_rows_R_kernel(const double *__restrict__ B, const double *__restrict__ P, double *__restrict__ X, int64_t d, int64_t c, int64_t DL,
+                                 int64_t cb) {
+    const int64_t c2 = c * (1 + DL), tot = c2 * d * cb;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a2 = e % c2, col = e / c2, s = col % d, b = col / d;
+        X[e]             = a2 < c ? B[s + d * (a2 + c * b)] : P[s + d * (b + cb * (a2 - c))];
+    }
+}
+// site tensor [s, a, b] -> its left-bond rows X[a + c (s + d b)]
+__global__ void site_rows_kernel(const double *__restrict__ M, double *__restrict__ X, int64_t d, int64_t c, int64_t cb) {
+    const int64_t tot = d * c * cb;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = e % c, col = e / c, s = col % d, b = col / d;
+        X[e]            = M[s + d * (a + c * b)];
+    }
+}
+// rows X[a + ldx (s + d b)] (a < c) -> site tensor M[s + d (a + c b)]
+__global__ void rows_site_kernel(const double *__restrict__ X, int64_t ldx, double *__restrict__ M, int64_t d, int64_t c, int64_t cb) {
+    const int64_t tot = d * c * cb;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = e % d, r = e / d, a = r % c, b = r / c;
+        M[e]            = X[a + ldx * (s + d * b)];
+    }
+}
+// which 0: X[r + ld k] *= S[k] (columns); which 1: X[k + ld j] *= S[k] (rows); rows x cols of X
+__global__ void scale_mat_kernel(double *__restrict__ X, int64_t ld, int64_t rows, int64_t cols, const double *__restrict__ S, int which) {
+    const int64_t tot = rows * cols;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e % rows, c = e / rows;
+        X[r + ld * c] *= S[which == 0 ? c : r];
+    }
+}
+// Y[j + ldy i] = X[i + ldx j] for i < rows, j < cols
+__global__ void transpose_kernel(const double *__restrict__ X, int64_t ldx, int64_t rows, int64_t cols, double *__restrict__ Y, int64_t ldy) {
+    const int64_t tot = rows * cols;
+    for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % rows, j = e / rows;
+        Y[j + ldy * i]  = X[i + ldx * j];
+    }
+}
+
+// C (M x N, ldc) = A (M x K, lda) B (K x N, ldb), FP64 DMMA
+static int gemm_nn(const double *A, int64_t lda, const double *B, int64_t ldb, double *C, int64_t ldc, int64_t M, int64_t N, int64_t K, cudaStream_t s) {
+    GemmArgs g{};
+    g.M = (int)M, g.N = (int)N, g.K = (int)K, g.batch = 1;
+    g.A = A, g.lda = lda, g.B = B, g.ldb = ldb, g.C = C, g.ldc = ldc;
+    g.alpha = make_double2(1, 0), g.beta = make_double2(0, 0);
+    return gemm_f64<false>(false, false, false, g, s);
+}
+
+// A (m x n, lda) = U S VT with U m x k (ld m), VT k x n (ld k); the one-sided Jacobi always runs on the taller
+// orientation (a wide matrix is transposed first and the factors swapped back).
+static int svd_oriented(DmrgWorkspace &ws, const double *A, int64_t lda, int64_t m, int64_t n, int64_t rank_max, double trunc, double *U, double *S,
+                        double *VT, int64_t *k, double *err, cudaStream_t s) {
+    if(m >= n) return svd_truncated(A, lda, m, n, rank_max, trunc, U, S, VT, k, err, ws.escr, nullptr, s);
+    transpose_kernel<<<g1(m * n), 256, 0, s>>>(A, lda, m, n, ws.eT, n);
+    HEFF_LAUNCH_CHECK();
+    HEFF_TRY(svd_truncated(ws.eT, n, n, m, rank_max, trunc, ws.eY, S, ws.eZ, k, err, ws.escr, nullptr, s));
+    // A^T = U' S VT'  ->  A = VT'^T S U'^T
+    transpose_kernel<<<g1(*k * m), 256, 0, s>>>(ws.eZ, *k, *k, m, U, m);
+    HEFF_LAUNCH_CHECK();
+    transpose_kernel<<<g1(n * *k), 256, 0, s>>>(ws.eY, n, n, *k, VT, *k);
+    HEFF_LAUNCH_CHECK();
+    return HEFF_OK;
+}
+
+// S <- S / ||S|| (the split keeps the state normalised, svd.h:172); returns ||S||^2 before and the values on the host
+static int normalise_S(double *S, int64_t k, std::vector<double> &hs, cudaStream_t s) {
+    hs.resize(k);
+    HEFF_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+    HEFF_CUDA(cudaStreamSynchronize(s));
+    double nrm = 0;
+    for(double v : hs) nrm += v * v;
+    nrm = std::sqrt(nrm);
+    if(nrm > 0 && std::fabs(nrm - 1.0) > 0) {
+        for(double &v : hs) v /= nrm;
+        HEFF_CUDA(cudaMemcpyAsync(S, hs.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+        HEFF_CUDA(cudaStreamSynchronize(s));  // hs is a host vector reused by the caller
+    }
+    return HEFF_OK;
+}
+
+static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgWorkspace &ws) {
+    auto      t0 = std::chrono::steady_clock::now();
+    const int L  = cfg.L;
+    if(L < 2 || L > ws.Lcap || !cfg.h || cfg.chi_max < 1 || cfg.chi_max > ws.chicap) return HEFF_BAD_ARG;
+    const bool folded = cfg.algorithm == 3;
+    if(folded && ws.Dcap < 9) return HEFF_BAD_ARG;
+    HEFF_TRY(ws.init_onesite());
+    const int64_t d = 2, chi_max = cfg.chi_max;
+    cudaStream_t  s = ws.s;
+    std::memset(&res, 0, sizeof(res));
+    ws.op->precision = (heff_precision)cfg.precision;
+    if(cfg.fp64_engine != HEFF_FP64_DMMA && cfg.fp64_engine != HEFF_FP64_INT8) return HEFF_BAD_ARG;
+    ws.op->fp64_engine = cfg.fp64_engine;
+    std::vector<std::vector<double>>    Wh(L);
+    std::vector<std::array<int64_t, 4>> wd(L);
+    for(int i = 0; i < L; i++) {
+        int64_t dd[4];
+        if(folded)
+            ising_site_mpo2(Wh[i], dd, i, L, cfg.J, cfg.h[i], cfg.energy_shift_per_site);
+        else
+            ising_site_mpo(Wh[i], dd, i, L, cfg.J, cfg.h[i], cfg.energy_shift_per_site);
+        for(int k = 0; k < 4; k++) wd[i][k] = dd[k];
+        HEFF_CUDA(cudaMemcpyAsync(ws.W[i], Wh[i].data(), Wh[i].size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    std::vector<int64_t> chi(L + 1, 1);
+    std::vector<double>  init(2 * L);
+    uint64_t             st = (uint64_t)cfg.seed * 0x2545F4914F6CDD1Dull + 17;
+    for(int i = 0; i < L; i++) {
+        double a = uniform01(st) - 0.5, b = uniform01(st) - 0.5, nn = std::sqrt(a * a + b * b);
+        init[2 * i]     = a / nn;
+        init[2 * i + 1] = b / nn;
+        HEFF_CUDA(cudaMemcpyAsync(ws.M[i], init.data() + 2 * i, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    const double one = 1.0;
+    HEFF_CUDA(cudaMemcpyAsync(ws.Lenv[0], &one, sizeof(double), cudaMemcpyHostToDevice, s));
+    HEFF_CUDA(cudaMemcpyAsync(ws.Renv[L - 1], &one, sizeof(double), cudaMemcpyHostToDevice, s));
+    HEFF_CUDA(cudaStreamSynchronize(s));
+    void  *sw = ws.op->split_ws;
+    size_t sb = ws.op->split_bytes;
+    // Renv[i] = environment of the sites > i, dims [chi_{i+1}, chi_{i+1}, wd[i][1]]
+    auto renv = [&](int i) {  // from Renv[i+1] and M[i+1]
+        const int64_t ed[3] = {chi[i + 2], chi[i + 2], wd[i + 1][1]}, mdd[3] = {d, chi[i + 1], chi[i + 2]};
+        return env_update_d(1, ws.Renv[i], ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), ws.scr, s, sw, sb);
+    };
+    // Lenv[i] = environment of the sites < i, dims [chi_i, chi_i, wd[i][0]]
+    auto lenv = [&](int i) {  // Lenv[i + 1] from Lenv[i] and M[i]
+        const int64_t ed[3] = {chi[i], chi[i], wd[i][0]}, mdd[3] = {d, chi[i], chi[i + 1]};
+        return env_update_d(0, ws.Lenv[i + 1], ws.Lenv[i], ed, ws.M[i], mdd, ws.W[i], wd[i].data(), ws.scr, s, sw, sb);
+    };
+    for(int i = L - 2; i >= 0; i--) HEFF_TRY(renv(i));
+    heff_eig_config ecfg;
+    heff_eig_config_default(&ecfg);
+    ecfg.tol         = cfg.eig_tol > 0 ? cfg.eig_tol : 1e-12;
+    ecfg.ritz        = cfg.ritz;
+    ecfg.target      = cfg.target;
+    ecfg.mixed       = cfg.precision == HEFF_PREC_MIXED;
+    ecfg.precond     = cfg.precond >= 0 ? cfg.precond : (folded ? 1 : 0);
+    ecfg.max_matvecs = 4000;
+    double              energy = 0, t_env = 0, t_eig = 0, t_svd = 0;
+    auto                now  = [] { return std::chrono::steady_clock::now(); };
+    auto                secs = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+    std::vector<double> hs;
+    const double        alpha0 = cfg.expansion_alpha > 0 ? cfg.expansion_alpha : 1e-3;
+    auto optimise = [&](int i) -> int {
+        auto          te0   = now();
+        const void   *mp[1] = {Wh[i].data()};
+        const int64_t ld[3] = {chi[i], chi[i], wd[i][0]}, rd[3] = {chi[i + 1], chi[i + 1], wd[i][1]};
+        HEFF_TRY(op_rebind(ws.op, 1, mp, wd[i].data(), ws.Lenv[i], ld, ws.Renv[i], rd));
+        heff_eig_result er;
+        int             rc = eigs(ws.op, &ecfg, ws.M[i], ws.M[i], &er);
+        if(rc != HEFF_OK && rc != HEFF_NOT_CONVERGED) return rc;
+        res.num_mv += er.num_mv;
+        res.num_mv_mixed += er.num_mv_mixed;
+        if(!er.converged) res.unconverged_solves++;
+        energy = er.eigval;
+        t_eig += secs(te0, now());
+        return HEFF_OK;
+    };
+    auto record_mid = [&](int bond, int sweep) {  // entanglement entropy at the middle bond, last sweep
+        if(bond != L / 2 || sweep != cfg.sweeps - 1) return;
+        double ent = 0;
+        for(double v : hs)
+            if(v > 0) ent -= v * v * std::log(v * v);
+        res.entropy_mid = std::fabs(ent);
+        res.chi_mid     = (int64_t)hs.size();
+    };
+    for(int sweep = 0; sweep < cfg.sweeps; sweep++) {
+        const double alpha = (sweep + 2 < cfg.sweeps) ? alpha0 * std::ldexp(1.0, -sweep) : 0.0;
+        // ---- left to right: sites 0 .. L-2, centre AC(i), B(i+1) enriched
+        for(int i = 0; i + 1 < L; i++) {
+            auto ts0 = now();
+            if(alpha > 0) {
+                const int64_t ca = chi[i], c = chi[i + 1], cb = chi[i + 2], DL = wd[i + 1][0];
+                const int64_t ed[3] = {cb, cb, wd[i + 1][1]}, mdd[3] = {d, c, cb};
+                HEFF_TRY(expansion_term<false>(1, ws.eP, ws.Renv[i + 1], ed, ws.M[i + 1], mdd, ws.W[i + 1], wd[i + 1].data(), alpha, s));
+                const int64_t c2 = c * (1 + DL);
+                ex_rows_R_kernel<<<g1(c2 * d * cb), 256, 0, s>>>(ws.M[i + 1], ws.eP, ws.eX, d, c, DL, cb);
+                HEFF_LAUNCH_CHECK();
+                const int64_t rmax = std::min(std::min(d * ca, d * cb), chi_max);
+                int64_t       k    = 0;
+                double        te   = 0;
+                HEFF_TRY(svd_oriented(ws, ws.eX, c2, c2, d * cb, rmax, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
+                // AC(i) <- AC(i) U[0:c, :] S ; B(i+1) <- V
+                HEFF_TRY(gemm_nn(ws.M[i], d * ca, ws.eU, c2, ws.Cbuf, d * ca, d * ca, k, c, s));
+                scale_mat_kernel<<<g1(d * ca * k), 256, 0, s>>>(ws.Cbuf, d * ca, d * ca, k, ws.S, 0);
+                HEFF_LAUNCH_CHECK();
+                HEFF_CUDA(cudaMemcpyAsync(ws.M[i], ws.Cbuf, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
+                rows_site_kernel<<<g1(d * k * cb), 256, 0, s>>>(ws.eV, k, ws.M[i + 1], d, k, cb);
+                HEFF_LAUNCH_CHECK();
+                chi[i + 1] = k;
+                auto tv0   = now();
+                HEFF_TRY(renv(i));
+                t_env += secs(tv0, now());
+            }
+            t_svd += secs(ts0, now());
+            HEFF_TRY(optimise(i));
+            // split AC(i) = A(i) S V; AC(i+1) = S V B(i+1)
+            auto          ts1 = now();
+            const int64_t ca = chi[i], c = chi[i + 1], cb = chi[i + 2];
+            int64_t       k  = 0;
+            double        te = 0;
+            HEFF_TRY(svd_oriented(ws, ws.M[i], d * ca, d * ca, c, chi_max, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
+            HEFF_TRY(normalise_S(ws.S, k, hs, s));
+            res.trunc_err_max = std::max(res.trunc_err_max, te);
+            record_mid(i + 1, sweep);
+            HEFF_CUDA(cudaMemcpyAsync(ws.M[i], ws.eU, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
+            scale_mat_kernel<<<g1(k * c), 256, 0, s>>>(ws.eV, k, k, c, ws.S, 1);
+            HEFF_LAUNCH_CHECK();
+            site_rows_kernel<<<g1(d * c * cb), 256, 0, s>>>(ws.M[i + 1], ws.eX, d, c, cb);
+            HEFF_LAUNCH_CHECK();
+            HEFF_TRY(gemm_nn(ws.eV, k, ws.eX, c, ws.eZ, k, k, d * cb, c, s));
+            rows_site_kernel<<<g1(d * k * cb), 256, 0, s>>>(ws.eZ, k, ws.M[i + 1], d, k, cb);
+            HEFF_LAUNCH_CHECK();
+            chi[i + 1] = k;
+            t_svd += secs(ts1, now());
+            auto tv0 = now();
+            HEFF_TRY(lenv(i));
+            t_env += secs(tv0, now());
+        }
+        // ---- right to left: sites L-1 .. 1, centre AC(i), A(i-1) enriched
+        for(int i = L - 1; i >= 1; i--) {
+            auto ts0 = now();
+            if(alpha > 0) {
+                const int64_t ca = chi[i - 1], c = chi[i], cb = chi[i + 1], DR = wd[i - 1][1];
+                const int64_t ed[3] = {ca, ca, wd[i - 1][0]}, mdd[3] = {d, ca, c};
+                // [A(i-1), P_L] along the right bond: P_L's layout [s', a', (b, n)] continues A's columns
+                HEFF_CUDA(cudaMemcpyAsync(ws.eX, ws.M[i - 1], sizeof(double) * d * ca * c, cudaMemcpyDeviceToDevice, s));
+                HEFF_TRY(expansion_term<false>(0, ws.eX + d * ca * c, ws.Lenv[i - 1], ed, ws.M[i - 1], mdd, ws.W[i - 1], wd[i - 1].data(), alpha, s));
+                const int64_t c2   = c * (1 + DR);
+                const int64_t rmax = std::min(std::min(d * ca, d * cb), chi_max);
+                int64_t       k    = 0;
+                double        te   = 0;
+                HEFF_TRY(svd_oriented(ws, ws.eX, d * ca, d * ca, c2, rmax, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
+                // A(i-1) <- U ; AC(i) <- S V[:, 0:c] AC(i)
+                HEFF_CUDA(cudaMemcpyAsync(ws.M[i - 1], ws.eU, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
+                scale_mat_kernel<<<g1(k * c), 256, 0, s>>>(ws.eV, k, k, c, ws.S, 1);
+                HEFF_LAUNCH_CHECK();
+                site_rows_kernel<<<g1(d * c * cb), 256, 0, s>>>(ws.M[i], ws.eP, d, c, cb);
+                HEFF_LAUNCH_CHECK();
+                HEFF_TRY(gemm_nn(ws.eV, k, ws.eP, c, ws.eZ, k, k, d * cb, c, s));
+                rows_site_kernel<<<g1(d * k * cb), 256, 0, s>>>(ws.eZ, k, ws.M[i], d, k, cb);
+                HEFF_LAUNCH_CHECK();
+                chi[i] = k;
+                auto tv0 = now();
+                HEFF_TRY(lenv(i - 1));
+                t_env += secs(tv0, now());
+            }
+            t_svd += secs(ts0, now());
+            HEFF_TRY(optimise(i));
+            // split AC(i) = U S B(i); AC(i-1) = A(i-1) U S
+            auto          ts1 = now();
+            const int64_t ca = chi[i - 1], c = chi[i], cb = chi[i + 1];
+            site_rows_kernel<<<g1(d * c * cb), 256, 0, s>>>(ws.M[i], ws.eX, d, c, cb);
+            HEFF_LAUNCH_CHECK();
+            int64_t k  = 0;
+            double  te = 0;
+            HEFF_TRY(svd_oriented(ws, ws.eX, c, c, d * cb, chi_max, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
+            HEFF_TRY(normalise_S(ws.S, k, hs, s));
+            res.trunc_err_max = std::max(res.trunc_err_max, te);
+            record_mid(i, sweep);
+            rows_site_kernel<<<g1(d * k * cb), 256, 0, s>>>(ws.eV, k, ws.M[i], d, k, cb);
+            HEFF_LAUNCH_CHECK();
+            HEFF_TRY(gemm_nn(ws.M[i - 1], d * ca, ws.eU, c, ws.Cbuf, d * ca, d * ca, k, c, s));
+            scale_mat_kernel<<<g1(d * ca * k), 256, 0, s>>>(ws.Cbuf, d * ca, d * ca, k, ws.S, 0);
+            HEFF_LAUNCH_CHECK();
+            HEFF_CUDA(cudaMemcpyAsync(ws.M[i - 1], ws.Cbuf, sizeof(double) * d * ca * k, cudaMemcpyDeviceToDevice, s));
+            chi[i] = k;
+            t_svd += secs(ts1, now());
+            auto tv0 = now();
+            HEFF_TRY(renv(i - 1));
+            t_env += secs(tv0, now());
+        }
+        if(sweep < 64) res.energy_per_sweep[sweep] = energy;
+        res.sweeps_done = sweep + 1;
+    }
+    if(res.chi_mid == 0) res.chi_mid = chi[L / 2];
+    if(folded) {
+        // <H> at the final centre AC(0): right environments of the unshifted H (D = 3) from the right-normalised
+        // sites 1 .. L-1 into the (now unused) left-environment storage, Lenv[j + 1] = environment of the sites > j
+        const double E_t = cfg.energy_shift_per_site * L;
+        const double lam = energy;
+        std::vector<std::vector<double>>    W3h(L);
+        std::vector<std::array<int64_t, 4>> w3(L);
+        for(int i = 0; i < L; i++) {
+            int64_t dd[4];
+            ising_site_mpo(W3h[i], dd, i, L, cfg.J, cfg.h[i], 0.0);
+            for(int k = 0; k < 4; k++) w3[i][k] = dd[k];
+            HEFF_CUDA(cudaMemcpyAsync(ws.W[i], W3h[i].data(), W3h[i].size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
+        HEFF_CUDA(cudaMemcpyAsync(ws.Lenv[L], &one, sizeof(double), cudaMemcpyHostToDevice, s));
+        for(int j = L - 2; j >= 0; j--) {
+            const int64_t ed[3] = {chi[j + 2], chi[j + 2], w3[j + 1][1]}, mdd[3] = {d, chi[j + 1], chi[j + 2]};
+            HEFF_TRY(env_update_d(1, ws.Lenv[j + 1], ws.Lenv[j + 2], ed, ws.M[j + 1], mdd, ws.W[j + 1], w3[j + 1].data(), ws.scr, s, sw, sb));
+        }
+        const void   *mp[1] = {W3h[0].data()};
+        const int64_t ld[3] = {chi[0], chi[0], w3[0][0]}, rd[3] = {chi[1], chi[1], w3[0][1]};
+        HEFF_TRY(op_rebind(ws.op, 1, mp, w3[0].data(), ws.Lenv[0], ld, ws.Lenv[1], rd));
+        ws.op->precision = HEFF_PREC_FP64;
+        HEFF_TRY(op_apply(ws.op, ws.M[0], ws.Cbuf));
+        const int64_t n = d * chi[0] * chi[1];
+        double        hv[2];
+        HEFF_TRY(dot_device<false>(ws.M[0], ws.Cbuf, n, ws.red, ws.red + 8, s));
+        HEFF_TRY(dot_device<false>(ws.M[0], ws.M[0], n, ws.red + 1, ws.red + 8, s));
+        HEFF_CUDA(cudaMemcpyAsync(hv, ws.red, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        HEFF_CUDA(cudaStreamSynchronize(s));
+        const double Eh = hv[0] / hv[1];
+        res.variance    = lam - (Eh - E_t) * (Eh - E_t);
+        energy          = Eh;
+    }
+    HEFF_CUDA(cudaStreamSynchronize(s));
+    res.energy  = energy;
+    res.t_eig   = t_eig;
+    res.t_svd   = t_svd;
+    res.t_env   = t_env;
+    res.seconds = secs(t0, now());
+    return HEFF_OK;
+}
+
+static int dmrg_any_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgWorkspace &ws) {
+    if(cfg.algorithm == 2 || cfg.algorithm == 3) return dmrg1_run_ws(cfg, res, ws);
+    if(cfg.algorithm != 0 && cfg.algorithm != 1) return HEFF_BAD_ARG;
+    return dmrg_run_ws(cfg, res, ws);
+}
+
 int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s) {
     if(cfg.L < 2 || cfg.L > 4096 || !cfg.h || cfg.chi_max < 1) return HEFF_BAD_ARG;
     DmrgWorkspace ws;
-    HEFF_TRY(ws.init(cfg.L, cfg.chi_max, (heff_precision)cfg.precision, s, cfg.algorithm == 1 ? 9 : 3, cfg.fp64_engine));
-    return dmrg_run_ws(cfg, res, ws);
+    const bool    folded = cfg.algorithm == 1 || cfg.algorithm == 3;
+    HEFF_TRY(ws.init(cfg.L, cfg.chi_max, (heff_precision)cfg.precision, s, folded ? 9 : 3, cfg.fp64_engine));
+    return dmrg_any_ws(cfg, res, ws);
 }
 
 // Many independent realisations: nthreads workers, each with its own stream and workspace (sized for the
@@ -415,7 +779,7 @@ int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_re
         int64_t Dmax   = 3;
         int     engine = HEFF_FP64_DMMA;
         for(int i = 0; i < n; i++) {
-            if(cfgs[i].algorithm == 1) Dmax = 9;
+            if(cfgs[i].algorithm == 1 || cfgs[i].algorithm == 3) Dmax = 9;
             if(cfgs[i].fp64_engine == HEFF_FP64_INT8) engine = HEFF_FP64_INT8;
         }
         int rc = wss[t]->init(Lmax, chimax, (heff_precision)cfgs[0].precision, streams[t], Dmax, engine);
@@ -428,7 +792,7 @@ int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_re
             while(true) {
                 const int i = next.fetch_add(1);
                 if(i >= n) break;
-                status[i] = dmrg_run_ws(cfgs[i], results[i], *wss[t]);
+                status[i] = dmrg_any_ws(cfgs[i], results[i], *wss[t]);
             }
         });
     }

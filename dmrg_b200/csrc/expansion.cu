@@ -109,6 +109,11 @@ int expansion_term(int side, typename Scalar<CPLX>::T *P, const typename Scalar<
     return HEFF_OK;
 }
 
+template int expansion_term<false>(int, double *, const double *, const int64_t[3], const double *, const int64_t[3], const double *,
+                                   const int64_t[4], double, cudaStream_t);
+template int expansion_term<true>(int, double2 *, const double2 *, const int64_t[3], const double2 *, const int64_t[3], const double2 *,
+                                  const int64_t[4], double, cudaStream_t);
+
 }  // namespace heff
 
 using namespace heff;

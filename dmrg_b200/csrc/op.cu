@@ -266,6 +266,7 @@ static int rebind_impl(heff_op *op, int nsites, const void *const *mpos_host, co
     mixed_invalidate(op);                                      // split operands belong to the old environments (re-split in place)
     op->emu_stale  = true;                                     // so do the digit planes of L and R' (rebuilt in place)
     op->diag_ready = false;
+    op->jcb_ready  = false;
     std::vector<HT> W;
     int64_t         wd[4];
     for(int i = 0; i < nsites; i++) {
@@ -521,6 +522,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
         delete op->pipe;
     }
     if(op->diag) cudaFree(op->diag);
+    if(op->jcb) cudaFree(op->jcb);
     if(op->eig_host) cudaFreeHost(op->eig_host);
     if(op->eig_event) cudaEventDestroy(op->eig_event);
     delete op;

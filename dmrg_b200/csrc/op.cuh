@@ -44,6 +44,13 @@ struct heff_op {
     void              *diag         = nullptr;
     int64_t            diag_cap     = 0;
     bool               diag_ready   = false;
+    // block-Jacobi preconditioner (heff_op_set_jacobi_blocksize > 1): [0, 256) singular-pivot count, then the
+    // inverted blocks; formed at the shift of the first MultPc after a (re)bind
+    int64_t            jcb_block    = 1;
+    void              *jcb          = nullptr;
+    size_t             jcb_bytes    = 0;
+    bool               jcb_ready    = false;
+    double             jcb_shift    = 0.0;
     // stage profiling (heff_op_set_profiling): ring of 5-event sets, summed on query
     bool               profiling     = false;
     std::vector<cudaEvent_t> prof_events;  // 5 * prof_cap

@@ -234,11 +234,24 @@ int heff_op_get_matrix(heff_op *op, void *M_out);
  * orthonormal eigenvectors.  FP64 one-sided Jacobi on the Gershgorin-shifted
  * positive-definite matrix; n <= 16384.  Synchronises the stream. */
 int heff_dense_eig(heff_dtype dtype, int64_t n, const void *A, int64_t lda, double *evals, void *evecs, void *stream);
-/* Jacobi preconditioner, replacing MatVecMPOS::MultPc(T*, T*, T shift) with
- * jcbMaxBlockSize == 1 (matvec_mpos.cpp:1349-1364): y = x / (diag - shift), the
- * denominator kept >= 1e-10 max(|shift|, 1) in magnitude.  Device buffers,
- * stream-ordered. */
+/* Jacobi preconditioner, replacing MatVecMPOS::MultPc(T*, T*, T shift)
+ * (matvec_mpos.cpp:1349-1416).  Block size 1 (the default): y = x / (diag - shift),
+ * the denominator kept >= 1e-10 max(|shift|, 1) in magnitude.  Block size bs > 1
+ * (jcbMaxBlockSize, CalcPc matvec_mpos.cpp:1087-1240): the rows are cut into
+ * consecutive blocks of bs (the last one shorter), each block B = H[blk,blk] - shift I
+ * is formed and inverted on the device at the shift of the first call after a create
+ * or rebind (later shifts reuse it, like readyCalcPc), and y_blk = B^-1 x_blk.
+ * Device buffers, stream-ordered. */
 int heff_op_multpc(heff_op *op, const void *x, void *y, double shift);
+/* Block size of the Jacobi preconditioner, replacing MatVecMPOS::set_jcbMaxBlockSize
+ * (matvec_mpos.h:147): 1 = diagonal; 2 .. HEFF_JCB_MAX_BLOCK = block Jacobi (the
+ * inverted blocks take rows() * bs elements of device memory).  A change takes effect
+ * at the next MultPc. */
+#define HEFF_JCB_MAX_BLOCK 1024
+int heff_op_set_jacobi_blocksize(heff_op *op, int64_t block_size);
+/* Number of block-Jacobi pivots that were below 1e-14 of their block's largest entry
+ * and floored there (0 for a well-conditioned preconditioner).  Synchronises the stream. */
+int heff_op_jacobi_singular(heff_op *op, int *count);
 
 /* ---------------------------------------------------------------------------
  * BF16 tensor-core GEMM used by the mixed-precision path (tcgen05 + TMA)
@@ -337,16 +350,22 @@ typedef struct {
     int           precision;             /* heff_precision of the matvecs */
     int64_t       seed;                  /* random product-state initialisation */
     double        energy_shift_per_site; /* MPO energy shift (IsingRandomField.cpp:127) */
-    int           algorithm;             /* 0: ground state (fDMRG, H);  1: excited state (xDMRG): lowest
-                                            eigenpair of (H - E_t)^2 with E_t = L * energy_shift_per_site,
-                                            MPO^2 uncompressed (MpoSite.cpp:57-70, D = 9), as in
-                                            optimize_folded_spectrum.cpp:236-370 */
+    int           algorithm;             /* 0: two-site ground state (fDMRG, H);  1: two-site excited state
+                                            (xDMRG): lowest eigenpair of (H - E_t)^2 with E_t = L *
+                                            energy_shift_per_site, MPO^2 uncompressed (MpoSite.cpp:57-70,
+                                            D = 9), as in optimize_folded_spectrum.cpp:236-370;  2 and 3: the
+                                            same two problems with one-site DMRG and forward subspace
+                                            expansion before each local optimisation (the reference's
+                                            single-site strategy, expand_environment_1site,
+                                            tools/finite/env/env.cpp:1034-1262) */
     int           precond;               /* eigensolver expansion (heff_eig_config.precond); default -1:
                                             Jacobi for xDMRG (as the reference's PRIMME set-up for H^2,
                                             optimize_folded_spectrum.cpp:303-304), Krylov for fDMRG */
     int           fp64_engine;           /* heff_fp64_engine of the FP64-accurate matvecs (heff_op_set_fp64_engine);
                                             default HEFF_FP64_DMMA.  With HEFF_FP64_INT8 the digit planes are
                                             reserved once for chi_max, so sweeps still allocate nothing */
+    double        expansion_alpha;       /* algorithms 2 and 3: mixing factor of the expansion term in the first
+                                            sweep (0: 1e-3), halved every sweep, off for the last two sweeps */
 } heff_dmrg_config;
 
 typedef struct {

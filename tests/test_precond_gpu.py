@@ -100,3 +100,76 @@ def test_xdmrg_with_jacobi_preconditioner(cuda):
     assert r0["variance"] < 1e-10 and r1["variance"] < 1e-10
     assert abs(r0["energy"] - r1["energy"]) < 1e-9
     print(f"xDMRG matvecs: Krylov {r0['num_mv']}, Jacobi-preconditioned {r1['num_mv']}")
+
+
+def block_inverse_apply(H, x, bs, shift):
+    """Reference for block Jacobi: y_blk = (H[blk, blk] - shift I)^-1 x_blk over consecutive blocks of bs rows
+    (CalcPc / MultPc, matvec_mpos.cpp:1087-1240, 1349-1416), by a dense solve per block."""
+    n = H.shape[0]
+    y = np.zeros_like(x)
+    for off in range(0, n, bs):
+        e = min(bs, n - off)
+        B = H[off:off + e, off:off + e] - shift * np.eye(e)
+        y[off:off + e] = np.linalg.solve(B, x[off:off + e])
+    return y
+
+
+@pytest.mark.parametrize("chi,chiR,D,c,bs", [(5, 4, 3, False, 2), (7, 9, 3, True, 7), (9, 8, 9, False, 64), (8, 9, 3, True, 128),
+                                             (10, 9, 9, False, 128), (11, 10, 3, False, 200), (9, 10, 9, True, 100)])
+def test_block_jacobi_vs_dense_solve(cuda, chi, chiR, D, c, bs):
+    """Blocks of every size class: a few rows, a shared-memory block (bs^2 entries within 200 KB) and blocks inverted
+    in global memory (real 200, complex 128/100); n = 4 chi chiR is never a multiple of bs, so the last block is short."""
+    th, W, L, R = ph.heff_inputs(chi, D=D, cplx=c, seed=chi * 31 + bs, chiR=chiR)
+    H = dense(th, W, L, R)  # the matrix MultAx applies: y = H x
+    op = hb.MatVecMPOS([W], L, R, cplx=c)
+    op.set_jacobi_blocksize(bs)
+    x = th.ravel(order="F")
+    y = torch.empty(x.size, dtype=torch.complex128 if c else torch.float64, device="cuda")
+    shift = -0.75
+    op.MultPc(hb.to_device(th), y, shift)
+    ref = block_inverse_apply(H, x, bs, shift)
+    assert np.linalg.norm(y.cpu().numpy() - ref) <= 1e-11 * np.linalg.norm(ref)
+    assert op.jacobi_singular() == 0
+    # the blocks are formed at the first shift and reused, like readyCalcPc; a rebind-free second call with another
+    # shift gives the same result
+    y2 = torch.empty_like(y)
+    op.MultPc(hb.to_device(th), y2, 5.0)
+    assert torch.equal(y, y2)
+    # a new block size takes effect at the next call (formed at that call's shift)
+    op.set_jacobi_blocksize(3)
+    op.MultPc(hb.to_device(th), y2, 1.5)
+    ref3 = block_inverse_apply(H, x, 3, 1.5)
+    assert np.linalg.norm(y2.cpu().numpy() - ref3) <= 1e-11 * np.linalg.norm(ref3)
+    op.close()
+
+
+def test_block_jacobi_of_whole_operator_is_the_inverse(cuda):
+    """One block covering every row: MultPc is the dense inverse (H - shift)^-1, so A MultPc(x) = x."""
+    th, W, L, R = ph.heff_inputs(6, D=3, cplx=False, seed=5, chiR=5)
+    n = th.size
+    H = dense(th, W, L, R)
+    op = hb.MatVecMPOS([W], L, R)
+    op.set_jacobi_blocksize(n)
+    x = hb.to_device(th)
+    y = torch.empty_like(x)
+    op.MultPc(x, y, 0.3)
+    z = (H - 0.3 * np.eye(n)) @ y.cpu().numpy()
+    assert np.linalg.norm(z - th.ravel(order="F")) <= 1e-11 * np.linalg.norm(th)
+    with pytest.raises(hb.HeffError):
+        op.set_jacobi_blocksize(0)
+    op.close()
+
+
+@pytest.mark.parametrize("c", [False, True])
+def test_block_jacobi_eigs_vs_dense(cuda, c):
+    """The preconditioned Davidson with block-Jacobi expansion vectors converges to the dense eigenvalues; the folded
+    shape (MPO squared, D=9) is where the reference's PRIMME set-up uses it (optimize_folded_spectrum.cpp:303-304)."""
+    th, W, L, R = ph.heff_inputs(8, D=3, cplx=c, seed=22, chiR=7)
+    w = np.linalg.eigvalsh(dense(th, W, L, R))
+    for bs in (1, 16, 64):
+        op = hb.MatVecMPOS([W], L, R, cplx=c)
+        op.set_jacobi_blocksize(bs)
+        e, res = op.eigs(ritz="SA", tol=1e-12, mixed=False, precond=1)
+        assert res["converged"] == 1, (bs, res)
+        assert abs(e - w[0]) < 1e-10 * max(1.0, abs(w[0])), bs
+        op.close()
