@@ -132,6 +132,20 @@ __global__ void scale_bond_kernel(double *__restrict__ X, const double *__restri
     }
 }
 
+// Warm-up schedule of both drivers: the first sweeps use the reduced bond limit and the loose eigensolver tolerance
+static int warmup_sweeps(const heff_dmrg_config &cfg) {
+    if(cfg.warmup_sweeps >= 0) return cfg.warmup_sweeps;
+    return (cfg.algorithm == 1 || cfg.algorithm == 3) ? 2 : 0;
+}
+static int64_t sweep_bond_limit(const heff_dmrg_config &cfg, int sweep) {
+    if(sweep >= warmup_sweeps(cfg)) return cfg.chi_max;
+    return std::min<int64_t>(cfg.chi_max, cfg.bond_min > 0 ? cfg.bond_min : 8);
+}
+static double sweep_eig_tol(const heff_dmrg_config &cfg, int sweep) {
+    const double tol = cfg.eig_tol > 0 ? cfg.eig_tol : 1e-12;
+    return sweep >= warmup_sweeps(cfg) ? tol : std::max(1e-8, tol);
+}
+
 static int g1(int64_t n) {
     int64_t g = (n + 255) / 256, cap = (int64_t)device_sm_count() * 8;
     return (int)(g < 1 ? 1 : (g < cap ? g : cap));
@@ -220,7 +234,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     if(L < 2 || L > ws.Lcap || !cfg.h || cfg.chi_max < 1 || cfg.chi_max > ws.chicap) return HEFF_BAD_ARG;
     const bool folded = cfg.algorithm == 1;
     if(folded && ws.Dcap < 9) return HEFF_BAD_ARG;
-    const int64_t d = 2, chi_max = cfg.chi_max;
+    const int64_t d = 2;
     cudaStream_t  s = ws.s;
     std::memset(&res, 0, sizeof(res));
     ws.op->precision = (heff_precision)cfg.precision;
@@ -270,6 +284,8 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     ecfg.max_matvecs = 4000;
     double energy    = 0;
     for(int sweep = 0; sweep < cfg.sweeps; sweep++) {
+        const int64_t chi_lim = sweep_bond_limit(cfg, sweep);
+        ecfg.tol              = sweep_eig_tol(cfg, sweep);
         for(int dir = 0; dir < 2; dir++) {
             for(int step = 0; step < L - 1; step++) {
                 const int     i  = dir == 0 ? step : (L - 2 - step);
@@ -306,7 +322,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
                 auto    ts0 = now();
                 int64_t k   = 0;
                 double  te  = 0;
-                HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_max, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s));
+                HEFF_TRY(schmidt_split(ws.theta, d, d, ca, cb, chi_lim, cfg.trunc_lim, ws.U, ws.S, ws.V, &k, &te, ws.scr, s));
                 res.trunc_err_max = std::max(res.trunc_err_max, te);
                 res.svd_sweeps_max = std::max(res.svd_sweeps_max, last_svd_sweeps());
                 if(i + 1 == L / 2 && sweep == cfg.sweeps - 1) {
@@ -509,7 +525,7 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
     const bool folded = cfg.algorithm == 3;
     if(folded && ws.Dcap < 9) return HEFF_BAD_ARG;
     HEFF_TRY(ws.init_onesite());
-    const int64_t d = 2, chi_max = cfg.chi_max;
+    const int64_t d = 2;
     cudaStream_t  s = ws.s;
     std::memset(&res, 0, sizeof(res));
     ws.op->precision = (heff_precision)cfg.precision;
@@ -589,7 +605,9 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
         res.chi_mid     = (int64_t)hs.size();
     };
     for(int sweep = 0; sweep < cfg.sweeps; sweep++) {
-        const double alpha = (sweep + 2 < cfg.sweeps) ? alpha0 * std::ldexp(1.0, -sweep) : 0.0;
+        const double  alpha   = (sweep + 2 < cfg.sweeps) ? alpha0 * std::ldexp(1.0, -sweep) : 0.0;
+        const int64_t chi_lim = sweep_bond_limit(cfg, sweep);
+        ecfg.tol              = sweep_eig_tol(cfg, sweep);
         // ---- left to right: sites 0 .. L-2, centre AC(i), B(i+1) enriched
         for(int i = 0; i + 1 < L; i++) {
             auto ts0 = now();
@@ -600,7 +618,7 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
                 const int64_t c2 = c * (1 + DL);
                 ex_rows_R_kernel<<<g1(c2 * d * cb), 256, 0, s>>>(ws.M[i + 1], ws.eP, ws.eX, d, c, DL, cb);
                 HEFF_LAUNCH_CHECK();
-                const int64_t rmax = std::min(std::min(d * ca, d * cb), chi_max);
+                const int64_t rmax = std::min(std::min(d * ca, d * cb), chi_lim);
                 int64_t       k    = 0;
                 double        te   = 0;
                 HEFF_TRY(svd_oriented(ws, ws.eX, c2, c2, d * cb, rmax, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
@@ -623,7 +641,7 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
             const int64_t ca = chi[i], c = chi[i + 1], cb = chi[i + 2];
             int64_t       k  = 0;
             double        te = 0;
-            HEFF_TRY(svd_oriented(ws, ws.M[i], d * ca, d * ca, c, chi_max, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
+            HEFF_TRY(svd_oriented(ws, ws.M[i], d * ca, d * ca, c, chi_lim, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
             HEFF_TRY(normalise_S(ws.S, k, hs, s));
             res.trunc_err_max = std::max(res.trunc_err_max, te);
             record_mid(i + 1, sweep);
@@ -651,7 +669,7 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
                 HEFF_CUDA(cudaMemcpyAsync(ws.eX, ws.M[i - 1], sizeof(double) * d * ca * c, cudaMemcpyDeviceToDevice, s));
                 HEFF_TRY(expansion_term<false>(0, ws.eX + d * ca * c, ws.Lenv[i - 1], ed, ws.M[i - 1], mdd, ws.W[i - 1], wd[i - 1].data(), alpha, s));
                 const int64_t c2   = c * (1 + DR);
-                const int64_t rmax = std::min(std::min(d * ca, d * cb), chi_max);
+                const int64_t rmax = std::min(std::min(d * ca, d * cb), chi_lim);
                 int64_t       k    = 0;
                 double        te   = 0;
                 HEFF_TRY(svd_oriented(ws, ws.eX, d * ca, d * ca, c2, rmax, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
@@ -678,7 +696,7 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
             HEFF_LAUNCH_CHECK();
             int64_t k  = 0;
             double  te = 0;
-            HEFF_TRY(svd_oriented(ws, ws.eX, c, c, d * cb, chi_max, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
+            HEFF_TRY(svd_oriented(ws, ws.eX, c, c, d * cb, chi_lim, cfg.trunc_lim, ws.eU, ws.S, ws.eV, &k, &te, s));
             HEFF_TRY(normalise_S(ws.S, k, hs, s));
             res.trunc_err_max = std::max(res.trunc_err_max, te);
             record_mid(i, sweep);
@@ -817,6 +835,7 @@ extern "C" void heff_dmrg_config_default(heff_dmrg_config *cfg) {
     cfg->eig_tol   = 1e-12;
     cfg->ritz      = HEFF_RITZ_SA;
     cfg->precision = HEFF_PREC_FP64;
+    cfg->warmup_sweeps = -1;
 }
 
 extern "C" int heff_dmrg_run(const heff_dmrg_config *cfg, heff_dmrg_result *res, void *stream) {

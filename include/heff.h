@@ -366,6 +366,12 @@ typedef struct {
                                             reserved once for chi_max, so sweeps still allocate nothing */
     double        expansion_alpha;       /* algorithms 2 and 3: mixing factor of the expansion term in the first
                                             sweep (0: 1e-3), halved every sweep, off for the last two sweeps */
+    int           warmup_sweeps;         /* first sweeps run at bond limit bond_min and eigensolver tolerance
+                                            max(1e-8, eig_tol) (the reference's warm-up iterations with bond_min and
+                                            eigs_tol_max, AlgorithmFinite.cpp:530-545, 812-822); -1 (default): 2 for
+                                            the folded-spectrum algorithms (1, 3), 0 for the ground state */
+    int64_t       bond_min;              /* bond limit of the warm-up sweeps (0: 8, the xDMRG bond_min of
+                                            settings.h:432) */
 } heff_dmrg_config;
 
 typedef struct {

@@ -113,6 +113,54 @@ def free_fermion_ground(hs, J=1.0):
     return -float(np.sum(free_fermion_levels(hs, J)))
 
 
+def free_fermion_modes(hs, J=1.0):
+    """Majorana normal modes of the open TFIM (Jordan-Wigner with sx_i = 1 - 2 n_i): H = (i/4) sum M_kl g_k g_l with
+    M[a_i, b_i] = 2 h_i, M[b_i, a_{i+1}] = 2 J; returns (eps, W) with M = W blockdiag([[0, eps_k], [-eps_k, 0]]) W^T,
+    eps_k = 2 Lambda_k >= 0 (real Schur form).  An eigenstate with mode occupations n_k has E = E0 + sum n_k eps_k."""
+    import scipy.linalg as sla
+
+    L = len(hs)
+    M = np.zeros((2 * L, 2 * L))
+    for i in range(L):
+        M[2 * i, 2 * i + 1], M[2 * i + 1, 2 * i] = 2 * hs[i], -2 * hs[i]
+        if i + 1 < L:
+            M[2 * i + 1, 2 * i + 2], M[2 * i + 2, 2 * i + 1] = 2 * J, -2 * J
+    T, W = sla.schur(M, output="real")
+    eps = np.empty(L)
+    for k in range(L):
+        e = T[2 * k, 2 * k + 1]
+        if e < 0:
+            W[:, [2 * k, 2 * k + 1]] = W[:, [2 * k + 1, 2 * k]]
+            e = -e
+        eps[k] = e
+    return eps, W
+
+
+def free_fermion_schmidt(eps, W, occ, cut, keep=1 << 17):
+    """Schmidt weights (squared singular values, descending, the largest `keep`) of the eigenstate with mode
+    occupations `occ` across the bond after site `cut` - 1 (sites [0, cut) | [cut, L)): the eigenvalues +-nu_j of the
+    restricted Majorana correlation matrix (Peschel, J. Phys. A 36, L205 (2003)) give the weights prod (1 +- nu_j)/2."""
+    L = len(eps)
+    G = np.zeros((2 * L, 2 * L))
+    for k in range(L):
+        v = 2.0 * occ[k] - 1.0
+        G[2 * k, 2 * k + 1], G[2 * k + 1, 2 * k] = v, -v
+    Gam = W @ G @ W.T
+    nu = np.sort(np.abs(np.linalg.eigvals(Gam[: 2 * cut, : 2 * cut]).imag))[::2]
+    p = np.array([1.0])
+    for x in nu:
+        p = np.concatenate([p * (1 + x) / 2, p * (1 - x) / 2])
+        if p.size > keep:
+            p = np.sort(p)[::-1][:keep]
+    return np.sort(p)[::-1]
+
+
+def bond_dimension_for_weight(p, weight):
+    """Smallest number of Schmidt weights whose discarded tail sums to at most `weight`."""
+    tail = np.cumsum(p[::-1])[::-1]
+    return int(np.count_nonzero(tail > weight))
+
+
 def hermitian_env(rng, chi, D, cplx):
     """[chi,chi,D] environment with every D-slice Hermitian: (X + X^dagger)/2, X Gaussian."""
     if cplx:
