@@ -448,7 +448,10 @@ def measure_eigs_folded(hb, torch, chi=512):
         return e, r, time.perf_counter() - t0
 
     out = {}
-    for name, op, kw in (("fp64", op64, {"mixed": False}), ("fp64_jacobi", op64, {"mixed": False, "precond": 1}), ("mixed", opm, {"mixed": True})):
+    opb = hb.MatVecMPOS([W], L, R, cplx=False)
+    opb.set_jacobi_blocksize(128)  # the reference's starting block size (eigs_jcb_min_blocksize, settings.h:261)
+    for name, op, kw in (("fp64", op64, {"mixed": False}), ("fp64_jacobi", op64, {"mixed": False, "precond": 1}),
+                         ("fp64_block_jacobi_128", opb, {"mixed": False, "precond": 1}), ("mixed", opm, {"mixed": True})):
         solve(op, **kw)
         runs = [solve(op, **kw) for _ in range(2)]
         t = statistics.median(r[2] for r in runs)
@@ -457,10 +460,12 @@ def measure_eigs_folded(hb, torch, chi=512):
                      "converged": r["converged"]}
     op64.close()
     opm.close()
+    opb.close()
     out["workload"] = "lowest eigenpair, real H_eff, two-site MPO squared D=9, chi=512, tol 1e-12 (the folded-spectrum solve's shape)"
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     out["abs_dE_mixed_vs_fp64"] = abs(out["mixed"]["E"] - out["fp64"]["E"])
     out["abs_dE_jacobi_vs_fp64"] = abs(out["fp64_jacobi"]["E"] - out["fp64"]["E"])
+    out["abs_dE_block_jacobi_vs_fp64"] = abs(out["fp64_block_jacobi_128"]["E"] - out["fp64"]["E"])
     return out
 
 
@@ -583,9 +588,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision, eigensolve and serving measurements")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
-    ap.add_argument("--serving-requests", type=int, default=40)
-    ap.add_argument("--serving-chi-max", type=int, default=1024)
-    ap.add_argument("--serving-rate", type=float, default=6.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serving-requests", type=int, default=120, help="requests of the mixed-precision serving stream")
+    ap.add_argument("--serving-requests-fp64", type=int, default=60, help="requests of the FP64 serving stream (its first ones)")
+    ap.add_argument("--serving-chi-max", type=int, default=2048)
+    ap.add_argument("--serving-rate", type=float, default=4.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serving-only", action="store_true", help="run only the serving streams (after the headline matvec)")
     ap.add_argument("--ensemble-n", type=int, default=32, help="realisations in the ensemble sample")
     ap.add_argument("--no-grid", action="store_true", help="skip the chi x D precision grid and the SVD timing")
     args = ap.parse_args()
@@ -684,22 +691,24 @@ def main():
             hb.check(hb.lib().heff_op_multax_host(op.handle, hb.ptr(xh), hb.ptr(yh)), "multax_host")
             t_e2e.append(time.perf_counter() - t0)
         clk = clocks.stop()
-        extras = {} if args.no_extras else measure_mixed_and_eigs(hb, torch, op, mpos, L, R, x, y, flush, stream, F)
+        extras = {} if (args.no_extras or args.serving_only) else measure_mixed_and_eigs(hb, torch, op, mpos, L, R, x, y, flush, stream, F)
     if not args.no_extras and not args.no_serving:
         op.close()
         del x, y, flush
         torch.cuda.empty_cache()
         sv = {}
-        for name, prec in (("mixed", hb.PREC_MIXED), ("fp64", hb.PREC_FP64)):
-            sv[name] = measure_serving(hb, torch, args.serving_requests, 64, args.serving_chi_max, args.serving_rate, prec)
+        for name, prec, nreq in (("mixed", hb.PREC_MIXED, args.serving_requests), ("fp64", hb.PREC_FP64, args.serving_requests_fp64)):
+            if nreq > 0:
+                sv[name] = measure_serving(hb, torch, nreq, 64, args.serving_chi_max, args.serving_rate, prec)
         sv["workload"] = ("bounded sample of the serving stream: Poisson arrivals, chi log-uniform, 70% f64 / 30% c128, D in {3, 9} "
                           "(D=9: MPO squared, folded-spectrum target), Hermitian seeded envs resident on the device, tol 1e-10")
-        if sv["fp64"]["solves_per_s"] > 0:
+        if "fp64" in sv and "mixed" in sv and sv["fp64"]["solves_per_s"] > 0:
             sv["mixed_vs_fp64_solves_per_s"] = sv["mixed"]["solves_per_s"] / sv["fp64"]["solves_per_s"]
         extras["serving"] = sv
-        extras["ensemble"] = measure_ensemble(hb, args.ensemble_n, 4, 32)  # 32 workers: 21 /s vs 18.6 /s with 16 (32 realisations)
-        extras["eigensolves_folded"] = measure_eigs_folded(hb, torch)
-    if not args.no_extras and not args.no_grid:
+        if not args.serving_only:
+            extras["ensemble"] = measure_ensemble(hb, args.ensemble_n, 4, 32)  # 32 workers: 21 /s vs 18.6 /s with 16 (32 realisations)
+            extras["eigensolves_folded"] = measure_eigs_folded(hb, torch)
+    if not args.no_extras and not args.no_grid and not args.serving_only:
         torch.cuda.empty_cache()
         gstream = torch.cuda.Stream()
         gflush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
