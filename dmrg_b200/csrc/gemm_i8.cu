@@ -4,6 +4,9 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "gemm_i8.cuh"
 #include "runtime.cuh"
@@ -586,16 +589,16 @@ static int z_forced_bn() {
     int f = g_force_bn.load();
     if(f < 0) {
         const char *e = getenv("HEFF_I8_BN");
-        const int   v = e ? atoi(e) : 0;
+        const int   v = e ? atoi(e) : 1;
         int         expect = -1;
-        g_force_bn.compare_exchange_strong(expect, (v == 128 || v == 192 || v == 256) ? v : 0);
+        g_force_bn.compare_exchange_strong(expect, (v == 0 || v == 1 || v == 128 || v == 192 || v == 256) ? v : 1);
         f = g_force_bn.load();
     }
     return f;
 }
 
 int z_choose_bn(int64_t M, int64_t N, int64_t K) {
-    if(const int forced = z_forced_bn()) return forced;
+    if(const int forced = z_forced_bn(); forced >= 128) return forced;
     // cost = waves x width x per-MAC weight.  The weights are measured (B200, 7 slices, the matvec GEMMs of
     // chi=1024, real and complex): with few k-blocks per slice the levels are short and summing them in C
     // costs more than the 128-wide tile's extra operand traffic; with long K the widest tile is best.
@@ -630,18 +633,84 @@ static int z_launch(const CUtensorMap &tA, const CUtensorMap &tB, const ZGemmArg
     return HEFF_OK;
 }
 
-int gemm_i8_ozaki(const ZPlanes &A, const ZPlanes &B, const ZGemmArgs &a, cudaStream_t s) {
-    if(a.M <= 0 || a.N <= 0) return HEFF_OK;
-    if(a.K <= 0 || a.K % 16 || a.nslice < 1 || a.nslice > Z_MAX_SLICES || !z_k_ok(a.K, a.nslice) || (a.cplx && a.N % 2)) return HEFF_BAD_ARG;
-    if(A.kx != a.K || B.kx != a.K || A.rows < a.M || B.rows < a.N || A.nslice < a.nslice || B.nslice < a.nslice) return HEFF_BAD_ARG;
-    if(!a.err || !a.bad_a || !a.bad_b) return HEFF_BAD_ARG;
-    const int   bn = z_choose_bn(a.M, a.N, a.K);
+static int z_launch_bn(int bn, const ZPlanes &A, const ZPlanes &B, const ZGemmArgs &a, cudaStream_t s) {
     CUtensorMap tA, tB;
     HEFF_TRY(make_tmap_planes(&tA, A, Z_BM));
     HEFF_TRY(make_tmap_planes(&tB, B, bn));
     if(bn == 256) return z_launch<256>(tA, tB, a, s);
     if(bn == 192) return z_launch<192>(tA, tB, a, s);
     return z_launch<128>(tA, tB, a, s);
+}
+
+// Autotuned tile width (the default, heff_i8_set_tile_width(1)): the first GEMM of each shape (device, M, N, K,
+// slices) runs once with the model's width to warm up, then once with each width under CUDA events on its own
+// stream; the fastest width is cached for the shape.  Every width sums the same exact level products in the same
+// order, so the extra runs rewrite C with identical bytes and the choice never changes a result.
+struct ZTuneKey {
+    int     dev, ns;
+    int64_t M, N, K;
+    bool    operator<(const ZTuneKey &o) const { return std::tie(dev, ns, M, N, K) < std::tie(o.dev, o.ns, o.M, o.N, o.K); }
+};
+static std::mutex                  g_tune_mu;
+static std::map<ZTuneKey, int>     g_tune;
+
+static int z_tuned_bn(const ZPlanes &A, const ZPlanes &B, const ZGemmArgs &a, cudaStream_t s, int *bn_out) {
+    int dev = 0;
+    HEFF_CUDA(cudaGetDevice(&dev));
+    const ZTuneKey key{dev, a.nslice, a.M, a.N, a.K};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto                        it = g_tune.find(key);
+        if(it != g_tune.end()) {
+            *bn_out = it->second;
+            return HEFF_OK;
+        }
+    }
+    const int   cand[3] = {128, 192, 256};
+    cudaEvent_t ev[4];
+    for(auto &e : ev) HEFF_CUDA(cudaEventCreate(&e));
+    int rc = z_launch_bn(z_choose_bn(a.M, a.N, a.K), A, B, a, s);  // warm-up (attributes, caches)
+    for(int i = 0; i < 3 && rc == HEFF_OK; i++) {
+        if(cudaEventRecord(ev[i], s) != cudaSuccess) rc = HEFF_CUDA_ERROR;
+        if(rc == HEFF_OK) rc = z_launch_bn(cand[i], A, B, a, s);
+    }
+    if(rc == HEFF_OK && cudaEventRecord(ev[3], s) != cudaSuccess) rc = HEFF_CUDA_ERROR;
+    if(rc == HEFF_OK && cudaEventSynchronize(ev[3]) != cudaSuccess) rc = HEFF_CUDA_ERROR;
+    int best = z_choose_bn(a.M, a.N, a.K);
+    if(rc == HEFF_OK) {
+        float bt = 0;
+        for(int i = 0; i < 3; i++) {
+            float ms = 0;
+            if(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]) != cudaSuccess) continue;
+            if(i == 0 || ms < bt) bt = ms, best = cand[i];
+        }
+    }
+    for(auto &e : ev) cudaEventDestroy(e);
+    HEFF_TRY(rc);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = best;
+    }
+    *bn_out = best;
+    return HEFF_OK;
+}
+
+int gemm_i8_ozaki(const ZPlanes &A, const ZPlanes &B, const ZGemmArgs &a, cudaStream_t s) {
+    if(a.M <= 0 || a.N <= 0) return HEFF_OK;
+    if(a.K <= 0 || a.K % 16 || a.nslice < 1 || a.nslice > Z_MAX_SLICES || !z_k_ok(a.K, a.nslice) || (a.cplx && a.N % 2)) return HEFF_BAD_ARG;
+    if(A.kx != a.K || B.kx != a.K || A.rows < a.M || B.rows < a.N || A.nslice < a.nslice || B.nslice < a.nslice) return HEFF_BAD_ARG;
+    if(!a.err || !a.bad_a || !a.bad_b) return HEFF_BAD_ARG;
+    int bn = 0;
+    if(z_forced_bn() == 1)
+        HEFF_TRY(z_tuned_bn(A, B, a, s, &bn));
+    else
+        bn = z_choose_bn(a.M, a.N, a.K);
+    return z_launch_bn(bn, A, B, a, s);
+}
+
+int z_tuned_count() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    return (int)g_tune.size();
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -706,8 +775,10 @@ extern "C" int heff_gemm_i8_emu(int dtype, const void *A, const void *B, void *C
     return HEFF_BAD_ARG;
 }
 
+extern "C" int heff_i8_tuned_shapes(void) { return heff::z_tuned_count(); }
+
 extern "C" int heff_i8_set_tile_width(int bn) {
-    if(bn != 0 && bn != 128 && bn != 192 && bn != 256) return -1;
+    if(bn != 0 && bn != 1 && bn != 128 && bn != 192 && bn != 256) return -1;
     const int prev = z_forced_bn();
     g_force_bn.store(bn);
     return prev;

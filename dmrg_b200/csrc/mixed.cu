@@ -199,7 +199,47 @@ __global__ void __launch_bounds__(32 * TA) mix_mixed_kernel(const float *__restr
     // the MPO's nonzero list (built once per operator) lands in shared memory with the T1 tile, under the same barrier
     for(int i = threadIdx.x; i < wl_bytes / 16; i += NTHREADS) reinterpret_cast<uint4 *>(lmem)[i] = reinterpret_cast<const uint4 *>(wl)[i];
     const int a0 = blockIdx.x * TA, b0 = blockIdx.y * MX_TB;
-    {
+    if((cL & 3) == 0 && a0 + TA <= cL) {
+        // 16-byte loads of 4 consecutive a' (T1's rows are a'-contiguous and 16-byte aligned when cL % 4 == 0), four
+        // per thread in flight before their shared-memory stores; lanes run a'-quads fastest, then 8 b
+        constexpr int Q = TA / 4, NB = 4;
+        const int     items = Q * MX_TB * NP;
+        for(int it0 = threadIdx.x; it0 < items; it0 += NTHREADS * NB) {
+            float4 vr[NB], vi[NB];
+#pragma unroll
+            for(int u = 0; u < NB; u++) {
+                const int it = it0 + u * NTHREADS;
+                vr[u] = vi[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if(it < items) {
+                    const int q = it % Q, rest = it / Q, bl = rest % MX_TB, ms = rest / MX_TB, m = ms / S, s = ms % S, b = b0 + bl;
+                    if(b < cR) {
+                        const int64_t idx = (a0 + 4 * q + (int64_t)cL * m) + M1 * (s + (int64_t)S * b);
+                        vr[u]             = *reinterpret_cast<const float4 *>(T1 + idx);
+                        if(CPLX) vi[u] = *reinterpret_cast<const float4 *>(T1 + idx + M1 * N1);
+                    }
+                }
+            }
+#pragma unroll
+            for(int u = 0; u < NB; u++) {
+                const int it = it0 + u * NTHREADS;
+                if(it < items) {
+                    const int q = it % Q, rest = it / Q, bl = rest % MX_TB, ms = rest / MX_TB;
+                    float    *d = sRe + ms * SSTR + (4 * q) * MX_ROW + bl;
+                    d[0]        = vr[u].x;
+                    d[MX_ROW]   = vr[u].y;
+                    d[2 * MX_ROW] = vr[u].z;
+                    d[3 * MX_ROW] = vr[u].w;
+                    if(CPLX) {
+                        float *e = sIm + ms * SSTR + (4 * q) * MX_ROW + bl;
+                        e[0]          = vi[u].x;
+                        e[MX_ROW]     = vi[u].y;
+                        e[2 * MX_ROW] = vi[u].z;
+                        e[3 * MX_ROW] = vi[u].w;
+                    }
+                }
+            }
+        }
+    } else {
         // a'-fastest loads (coalesced along T1's rows), 8 in flight per thread, two halves of the b range
         const int al = threadIdx.x % TA, bl = threadIdx.x / TA;  // bl < 32
         const int ap = a0 + al;

@@ -277,13 +277,18 @@ int heff_gemm_bf16_f32(const void *A, const void *B, float *C, int64_t M, int64_
  * HEFF_BAD_SHAPE when K is too long for exact INT32 sums (K' * nslices >= 2^19,
  * K' = round16(K), doubled for complex), HEFF_TIMEOUT if a pipeline wait timed out. */
 int heff_gemm_i8_emu(int dtype, const void *A, const void *B, void *C, int64_t M, int64_t N, int64_t K, int nslices, void *stream);
-/* Tile width of the INT8 emulated-FP64 GEMMs: 128, 192 or 256 columns, or 0 for
- * the automatic choice (fewest waves on the device); the initial value comes
- * from the environment variable HEFF_I8_BN.  Results do not depend on it (every
- * width sums the same exact level products in the same order).  Returns the
- * previous setting, or -1 for an invalid width.  Process-wide tuning knob; no
- * counterpart in the reference. */
+/* Tile width of the INT8 emulated-FP64 GEMMs: 128, 192 or 256 columns; 0 for the
+ * cost model (fewest waves weighted by measured per-width costs); 1 (the default)
+ * for the autotuner: the first GEMM of each shape runs once with every width,
+ * timed with CUDA events on its stream (which it synchronises then), and the
+ * fastest width is cached for that shape.  The initial value comes from the
+ * environment variable HEFF_I8_BN.  Results do not depend on it (every width sums
+ * the same exact level products in the same order).  Returns the previous
+ * setting, or -1 for an invalid value.  Process-wide tuning knob; no counterpart
+ * in the reference. */
 int heff_i8_set_tile_width(int bn);
+/* Number of GEMM shapes the INT8 tile-width autotuner has timed so far. */
+int heff_i8_tuned_shapes(void);
 
 /* Tail split of the FP64 (DMMA) GEMMs of the matvec: when a GEMM's tiles leave
  * the last wave of the device partly empty, the tiles of that wave are split

@@ -44,15 +44,15 @@ def rnd(shape, g, cplx):
 # 148 SMs (several tiles per CTA, both TMEM buffers, 7 levels each); (1100,3000,4000): ragged edges, long K
 @pytest.mark.parametrize("M,N,K", [(128, 256, 128), (200, 300, 136), (64, 40, 8), (1000, 700, 1024), (1536, 4096, 2048), (1100, 3000, 4000)])
 @pytest.mark.parametrize("cplx", [False, True])
-@pytest.mark.parametrize("bn", [0, 128, 192, 256])
+@pytest.mark.parametrize("bn", [0, 1, 128, 192, 256])
 def test_i8_emu_gemm_vs_fp64(cuda, M, N, K, cplx, bn):
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K + cplx)
     A, B = rnd((M, K), g, cplx), rnd((N, K), g, cplx)
-    hb.lib().heff_i8_set_tile_width(bn)
+    prev = hb.lib().heff_i8_set_tile_width(bn)
     try:
         rc, C = emu(A, B)
     finally:
-        hb.lib().heff_i8_set_tile_width(0)
+        hb.lib().heff_i8_set_tile_width(prev)
     assert rc == 0, hb.lib().heff_last_error()
     ref = A @ B.T
     e = rel(C, ref)
@@ -104,15 +104,19 @@ def test_i8_emu_tile_widths_bitwise_equal(cuda, cplx):
     g = torch.Generator(device="cuda").manual_seed(21)
     A, B = rnd((700, 520), g, cplx), rnd((900, 520), g, cplx)
     outs = []
+    prev = hb.lib().heff_i8_set_tile_width(0)
     try:
-        for bn in (128, 192, 256):
+        for bn in (128, 192, 256, 1):
             hb.lib().heff_i8_set_tile_width(bn)
+            n0 = hb.lib().heff_i8_tuned_shapes()
             rc, C = emu(A, B)
             assert rc == 0, hb.lib().heff_last_error()
+            if bn == 1:  # the autotuner timed this shape (its three trial runs rewrote C with identical bytes)
+                assert hb.lib().heff_i8_tuned_shapes() >= n0
             outs.append(C.clone())
     finally:
-        hb.lib().heff_i8_set_tile_width(0)
-    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+        hb.lib().heff_i8_set_tile_width(prev)
+    assert all(torch.equal(outs[0], o) for o in outs[1:])
     assert rel(outs[0], A @ B.T) < 5e-13
 
 

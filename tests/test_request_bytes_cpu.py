@@ -56,16 +56,20 @@ def test_null_request_is_zero():
 
 
 def test_int8_tile_width_knob():
-    """heff_i8_set_tile_width accepts 0 (automatic), 128, 192 or 256, returns the previous setting, rejects the rest."""
+    """heff_i8_set_tile_width accepts 0 (cost model), 1 (autotuner, the default), 128, 192 or 256, returns the previous
+    setting, rejects the rest."""
     L = hb.lib()
     prev = L.heff_i8_set_tile_width(0)
     try:
-        assert prev in (0, 128, 192, 256)
+        assert prev in (0, 1, 128, 192, 256)
         assert L.heff_i8_set_tile_width(192) == 0
         assert L.heff_i8_set_tile_width(128) == 192
         assert L.heff_i8_set_tile_width(100) == -1
         assert L.heff_i8_set_tile_width(160) == -1
-        assert L.heff_i8_set_tile_width(0) == 128
+        assert L.heff_i8_set_tile_width(2) == -1
+        assert L.heff_i8_set_tile_width(1) == 128
+        assert L.heff_i8_set_tile_width(0) == 1
+        assert L.heff_i8_tuned_shapes() >= 0
     finally:
         L.heff_i8_set_tile_width(prev)
 
