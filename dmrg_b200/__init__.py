@@ -554,6 +554,10 @@ class MatVecMPOS:
         """FP64-accurate matvecs on the FP64 tensor cores (FP64_DMMA) or emulated on the INT8 tensor cores (FP64_INT8)."""
         check(lib().heff_op_set_fp64_engine(self.handle, int(engine), int(nslices)), "set_fp64_engine")
 
+    def set_graphs(self, enable=True):
+        """CUDA-graph replay of the FP64 matvec (heff_op_set_graphs; on by default, needs a non-default stream)."""
+        check(lib().heff_op_set_graphs(self.handle, int(bool(enable))), "heff_op_set_graphs")
+
     def set_profiling(self, enable=True):
         check(lib().heff_op_set_profiling(self.handle, int(bool(enable))), "set_profiling")
 

@@ -98,6 +98,7 @@ def declare(L, sig):
         sig(L, n, _I, [_P, _P, _I64P, _I, ctypes.POINTER(_P), _I64P, _P, _I64P, _P, _I64P, _P])
     sig(L, "heff_dense_eig", _I, [_I, _I64, _P, _I64, _P, _P, _P])
     sig(L, "heff_op_multpc", _I, [_P, _P, _P, ctypes.c_double])
+    sig(L, "heff_op_set_graphs", _I, [_P, _I])
     sig(L, "heff_op_set_jacobi_blocksize", _I, [_P, _I64])
     sig(L, "heff_op_jacobi_singular", _I, [_P, ctypes.POINTER(ctypes.c_int)])
     sig(L, "heff_gemm_bf16_f32", _I, [_P, _P, _P, _I64, _I64, _I64, _P])

@@ -1,6 +1,9 @@
 // Host-side dispatch of the DMMA GEMM template (gemm_f64.cuh).
+#include <algorithm>
 #include <atomic>
 #include <cstdlib>
+#include <mutex>
+#include <vector>
 
 #include "gemm_f64.cuh"
 
@@ -58,6 +61,19 @@ size_t gemm_split_ws_bytes() {
     return (size_t)4 * device_sm_count() * GemmTile<false>::BM * GemmTile<false>::BN * sizeof(double);
 }
 
+// Every DMMA GEMM kernel (and split reduction) this process has launched; a captured graph's kernel nodes are
+// recognised by their function (their one parameter is a GemmArgs), so a replay can retarget their output.
+static std::mutex               g_gemm_fn_mu;
+static std::vector<const void *> g_gemm_fns;
+static void gemm_fn_register(const void *f) {
+    std::lock_guard<std::mutex> lk(g_gemm_fn_mu);
+    if(std::find(g_gemm_fns.begin(), g_gemm_fns.end(), f) == g_gemm_fns.end()) g_gemm_fns.push_back(f);
+}
+bool gemm_fn_known(const void *f) {
+    std::lock_guard<std::mutex> lk(g_gemm_fn_mu);
+    return std::find(g_gemm_fns.begin(), g_gemm_fns.end(), f) != g_gemm_fns.end();
+}
+
 template<bool CPLX, bool TA, bool TB, bool CJA, int VEC>
 static int launch_gemm(const GemmArgs &a_in, cudaStream_t stream) {
     using G                  = GemmTile<CPLX>;
@@ -93,10 +109,12 @@ static int launch_gemm(const GemmArgs &a_in, cudaStream_t stream) {
     const int64_t ctas = sp.nfull + (tiles - sp.nfull) * sp.split;
     if(ctas > 0x7fffffffLL) return HEFF_BAD_SHAPE;
     dim3 grid((unsigned)ctas, 1u, (unsigned)a.batch);
+    gemm_fn_register(reinterpret_cast<const void *>(kern));
     kern<<<grid, 256, SM::BYTES, stream>>>(a);
     HEFF_LAUNCH_CHECK();
     if(sp.split > 1) {
         const dim3 rgrid((unsigned)(tiles - sp.nfull), (unsigned)(SplitReduce<CPLX>::EPT / SplitReduce<CPLX>::EPB));
+        gemm_fn_register(reinterpret_cast<const void *>(gemm_split_reduce_kernel<CPLX>));
         gemm_split_reduce_kernel<CPLX><<<rgrid, 256, 0, stream>>>(a);
         HEFF_LAUNCH_CHECK();
     }

@@ -368,5 +368,6 @@ size_t gemm_split_ws_bytes();
 // Host launcher.  Returns HEFF_OK or a status code; never synchronises.
 template<bool CPLX>
 int gemm_f64(bool ta, bool tb, bool cja, const GemmArgs &args, cudaStream_t stream);
+bool gemm_fn_known(const void *f);  // a DMMA GEMM or split-reduction kernel (single GemmArgs parameter)
 
 }  // namespace heff

@@ -361,6 +361,10 @@ int dot_device(const typename Scalar<CPLX>::T *x, const typename Scalar<CPLX>::T
     return HEFF_OK;
 }
 
+const void *permute_kernel_fn(bool cplx) {
+    return cplx ? reinterpret_cast<const void *>(permute_mps_kernel<double2>) : reinterpret_cast<const void *>(permute_mps_kernel<double>);
+}
+
 template<bool CPLX>
 int permute_mps(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename Scalar<CPLX>::T *xp, cudaStream_t s) {
     const int64_t n = d.size_mps();

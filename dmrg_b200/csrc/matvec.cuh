@@ -46,6 +46,10 @@ struct MatvecScratch {
     }
 };
 
+// Host-side address of the matvec's input permutation kernel (its first parameter is the input vector): a captured
+// matvec graph is retargeted to a new input through it.
+const void *permute_kernel_fn(bool cplx);
+
 // Tail-split scratch to reserve beside a matvec scratch of `scratch_bytes`: enough partial tiles for the best
 // split of large GEMMs (gemm_split_ws_bytes), at least 16 MB so small-bond GEMMs with few tiles can split finely.
 inline size_t matvec_split_bytes(size_t scratch_bytes) {

@@ -453,6 +453,122 @@ cudaEvent_t *op_prof_slot(heff_op *op) {
     return op->prof_events.data() + 5 * (op->prof_used++);
 }
 
+// ---- CUDA graph of the FP64 matvec ----------------------------------------------------------------------------
+// A small matvec is a handful of short kernels (permute, GEMM 1 [+ split reduction], MPO mix, GEMM 2 [+ split
+// reduction]) whose launch costs are comparable to their run times; a sweep or an eigensolve applies the same
+// operator shape tens to hundreds of times.  The first product of a shape runs as plain launches (which also perform
+// every one-time set-up outside a capture) and is then recorded as a graph; later products patch the graph's two
+// data-dependent parameters -- the permutation kernel's input and the output pointer in the GemmArgs of the last
+// GEMM's kernels -- and launch it.  The graph is rebuilt when the shape or any operator buffer changes; a stream
+// that cannot be captured (the legacy default stream) keeps the plain launches.
+struct MatvecGraph {
+    cudaGraph_t                       g  = nullptr;
+    cudaGraphExec_t                   ex = nullptr;
+    MatvecDims                        d{};
+    bool                              cplx = false;
+    const void                       *L = nullptr, *Rp = nullptr, *W = nullptr, *scr = nullptr, *split = nullptr;
+    size_t                            split_bytes = 0;
+    cudaGraphNode_t                   perm        = nullptr;
+    cudaKernelNodeParams              perm_p{};
+    std::vector<void *>               perm_args;
+    std::vector<cudaGraphNode_t>      outs;
+    std::vector<cudaKernelNodeParams> out_p;
+    std::vector<GemmArgs>             out_a;
+    ~MatvecGraph() {
+        if(ex) cudaGraphExecDestroy(ex);
+        if(g) cudaGraphDestroy(g);
+    }
+    bool matches(const heff_op *op, bool c) const {
+        return c == cplx && d.S == op->d.S && d.cL == op->d.cL && d.cR == op->d.cR && d.DL == op->d.DL && d.DR == op->d.DR && L == op->L &&
+               Rp == op->Rp && W == op->W && scr == op->scratch && split == op->split_ws && split_bytes == op->split_bytes;
+    }
+};
+
+void op_graph_release(heff_op *op) {
+    delete op->mg;
+    op->mg = nullptr;
+}
+
+template<bool CPLX>
+static int plain_apply(heff_op *op, const void *x, void *y) {
+    using T = typename Scalar<CPLX>::T;
+    MatvecScratch<CPLX> ws;
+    ws.carve(reinterpret_cast<T *>(op->scratch), op->d);
+    ws.split_ws    = op->split_ws;
+    ws.split_bytes = op->split_bytes;
+    return matvec_fp64<CPLX>(op->d, reinterpret_cast<const T *>(x), reinterpret_cast<T *>(y), reinterpret_cast<const T *>(op->L),
+                             reinterpret_cast<const T *>(op->Rp), reinterpret_cast<const T *>(op->W), ws, op->stream, op_prof_slot(op));
+}
+
+// Records the matvec of the current shape (x, y as placeholders) and finds the nodes to retarget.  Any failure
+// turns graphs off for this operator and leaves the plain launches in place.
+template<bool CPLX>
+static void graph_capture(heff_op *op, const void *x, void *y) {
+    auto give_up = [&](MatvecGraph *G) {
+        delete G;
+        op->graphs = false;
+        (void)cudaGetLastError();
+    };
+    MatvecGraph *G = new MatvecGraph();
+    G->d = op->d, G->cplx = CPLX, G->L = op->L, G->Rp = op->Rp, G->W = op->W, G->scr = op->scratch, G->split = op->split_ws;
+    G->split_bytes = op->split_bytes;
+    if(cudaStreamBeginCapture(op->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return give_up(G);
+    const int   rc = plain_apply<CPLX>(op, x, y);
+    cudaGraph_t g  = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(op->stream, &g);
+    G->g = g;
+    if(rc != HEFF_OK || e != cudaSuccess || !g) return give_up(G);
+    if(cudaGraphInstantiate(&G->ex, g, 0) != cudaSuccess) return give_up(G);
+    size_t nn = 0;
+    if(cudaGraphGetNodes(g, nullptr, &nn) != cudaSuccess) return give_up(G);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if(cudaGraphGetNodes(g, nodes.data(), &nn) != cudaSuccess) return give_up(G);
+    const void *pf = permute_kernel_fn(CPLX);
+    for(cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if(cudaGraphNodeGetType(nd, &t) != cudaSuccess) return give_up(G);
+        if(t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams p{};
+        if(cudaGraphKernelNodeGetParams(nd, &p) != cudaSuccess || !p.kernelParams) return give_up(G);
+        if(p.func == pf) {
+            if(G->perm) return give_up(G);
+            G->perm   = nd;
+            G->perm_p = p;
+            G->perm_args.assign(p.kernelParams, p.kernelParams + 5);  // (x, xp, S, cL, n)
+        } else if(gemm_fn_known(p.func)) {
+            const GemmArgs a = *reinterpret_cast<const GemmArgs *>(p.kernelParams[0]);
+            if(a.C == y) {
+                G->outs.push_back(nd);
+                G->out_p.push_back(p);
+                G->out_a.push_back(a);
+            }
+        }
+    }
+    if(!G->perm || G->outs.empty()) return give_up(G);
+    op->mg = G;
+}
+
+template<bool CPLX>
+static int graph_replay(heff_op *op, const void *x, void *y) {
+    MatvecGraph         *G  = op->mg;
+    const void          *xv = x;
+    std::vector<void *>  pa = G->perm_args;
+    pa[0]                   = const_cast<void *>(reinterpret_cast<const void *>(&xv));
+    cudaKernelNodeParams pp = G->perm_p;
+    pp.kernelParams         = pa.data();
+    HEFF_CUDA(cudaGraphExecKernelNodeSetParams(G->ex, G->perm, &pp));
+    for(size_t i = 0; i < G->outs.size(); i++) {
+        GemmArgs a             = G->out_a[i];
+        a.C                    = y;
+        void                *args[1] = {&a};
+        cudaKernelNodeParams q = G->out_p[i];
+        q.kernelParams         = args;
+        HEFF_CUDA(cudaGraphExecKernelNodeSetParams(G->ex, G->outs[i], &q));
+    }
+    HEFF_CUDA(cudaGraphLaunch(G->ex, op->stream));
+    return HEFF_OK;
+}
+
 template<bool CPLX>
 static int apply_impl(heff_op *op, const void *x, void *y) {
     using T = typename Scalar<CPLX>::T;
@@ -468,12 +584,17 @@ static int apply_impl(heff_op *op, const void *x, void *y) {
         op->num_mv++;
         return HEFF_OK;
     }
-    MatvecScratch<CPLX> ws;
-    ws.carve(reinterpret_cast<T *>(op->scratch), op->d);
-    ws.split_ws    = op->split_ws;
-    ws.split_bytes = op->split_bytes;
-    HEFF_TRY(matvec_fp64<CPLX>(op->d, reinterpret_cast<const T *>(x), reinterpret_cast<T *>(y), reinterpret_cast<const T *>(op->L),
-                               reinterpret_cast<const T *>(op->Rp), reinterpret_cast<const T *>(op->W), ws, op->stream, op_prof_slot(op)));
+    if(op->graphs && !op->profiling && op->stream) {
+        if(op->mg && op->mg->matches(op, CPLX)) {
+            HEFF_TRY(graph_replay<CPLX>(op, x, y));
+        } else {
+            op_graph_release(op);
+            HEFF_TRY(plain_apply<CPLX>(op, x, y));  // this product, and every one-time set-up, outside a capture
+            graph_capture<CPLX>(op, x, y);          // recorded for the next products of this shape
+        }
+    } else {
+        HEFF_TRY(plain_apply<CPLX>(op, x, y));
+    }
     op->num_mv++;
     return HEFF_OK;
 }
@@ -501,6 +622,7 @@ extern "C" int heff_op_create(heff_op **op, heff_dtype dtype, int nsites, const 
 
 extern "C" int heff_op_destroy(heff_op *op) {
     if(!op) return HEFF_OK;
+    op_graph_release(op);
     if(op->destroy_hook) op->destroy_hook(op);
     emu_destroy(op);
     for(cudaEvent_t e : op->prof_events) cudaEventDestroy(e);

@@ -5,6 +5,10 @@
 #include "matvec.cuh"
 #include "multi.cuh"
 
+namespace heff {
+struct MatvecGraph;  // op.cu
+}
+
 struct heff_op {
     bool               cplx = false;
     heff::MatvecDims   d{};
@@ -63,6 +67,10 @@ struct heff_op {
     int                emu_slices    = 7;
     void              *emu           = nullptr;
     bool               emu_stale     = true;
+    // CUDA graph of the FP64 DMMA matvec (heff_op_set_graphs, on by default): captured at the second product of a
+    // shape on a non-default stream and replayed with the input and output retargeted
+    bool               graphs        = true;
+    heff::MatvecGraph *mg            = nullptr;
     // mixed-precision state (owned by the mixed path; null until first use)
     void              *mixed         = nullptr;
     int (*mixed_apply)(heff_op *, const void *, void *) = nullptr;

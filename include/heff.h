@@ -208,6 +208,12 @@ int64_t heff_op_num_mv(const heff_op *op);
  * (layout, GEMM 1, MPO mix, GEMM 2).  heff_op_stage_times synchronises the op's
  * stream and returns the summed milliseconds per stage and the matvec count. */
 int heff_op_set_profiling(heff_op *op, int enable);
+/* CUDA graphs for the FP64 matvec (on by default; no counterpart in the reference):
+ * on an operator created with a non-default stream, the first product of a shape
+ * runs as plain kernel launches and is recorded as a graph; later products of that
+ * shape replay it with the input and output retargeted (one launch instead of
+ * four to six).  Results are bitwise identical either way.  0 turns it off. */
+int heff_op_set_graphs(heff_op *op, int enable);
 int heff_op_stage_times(heff_op *op, double ms[4], int64_t *count, int reset);
 /* Device-side status of the operator's tensor-core pipeline: *code = 0 when every
  * bounded wait in the tensor-core kernels completed, nonzero when one timed out
