@@ -25,6 +25,7 @@
 #include <complex>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "blas1.cuh"
@@ -549,9 +550,69 @@ struct Davidson {
     }
 };
 
+template<class T>
+__global__ void eig_pick_column_kernel(const T *__restrict__ evecs, int64_t n, int64_t col, T *__restrict__ x) {
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const T v = evecs[i + n * col];
+        if constexpr(std::is_same<T, double2>::value)
+            x[i] = make_double2(v.x, -v.y);  // get_matrix holds conj(H) for a Hermitian H: its eigenvectors are conjugated
+        else
+            x[i] = v;
+    }
+}
+
+// Interior eigenpair (closest to cfg.target) of a small operator by the dense path: the reference switches to a
+// dense eigensolver at problem sizes <= eig_max_size = 4096 (settings.h:249, AlgorithmFinite.cpp:318), and Krylov
+// methods converge poorly to interior eigenvalues.  get_matrix + the device dense eigensolver, then the eigenvalue
+// nearest the target and its eigenvector.
+template<bool CPLX>
+static int eigs_dense_target(heff_op *op, const heff_eig_config &cfg, void *x_out, heff_eig_result &res) {
+    using T          = typename Scalar<CPLX>::T;
+    auto          t0 = std::chrono::steady_clock::now();
+    const int64_t n  = op->d.size_mps();
+    const size_t  es = sizeof(T), nn = (size_t)n * n;
+    const size_t  need = es * 2 * nn + sizeof(double) * n + 512;
+    if(op->dense_bytes < need) {
+        if(op->dense_ws) {
+            HEFF_CUDA(cudaStreamSynchronize(op->stream));
+            cudaFree(op->dense_ws);
+            op->dense_ws    = nullptr;
+            op->dense_bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&op->dense_ws, need);
+        if(e != cudaSuccess) {
+            set_last_cuda_error(e, "dense eigensolver buffers", __FILE__, __LINE__);
+            return HEFF_OOM;
+        }
+        op->dense_bytes = need;
+    }
+    T      *M     = reinterpret_cast<T *>(op->dense_ws);
+    T      *evecs = M + nn;
+    double *evals = reinterpret_cast<double *>(evecs + nn);
+    HEFF_TRY((int)heff_op_get_matrix(op, M));
+    HEFF_TRY((int)heff_dense_eig(CPLX ? HEFF_C128 : HEFF_F64, n, M, n, evals, evecs, op->stream));
+    std::vector<double> w(n);
+    HEFF_CUDA(cudaMemcpyAsync(w.data(), evals, sizeof(double) * n, cudaMemcpyDeviceToHost, op->stream));
+    HEFF_CUDA(cudaStreamSynchronize(op->stream));
+    int64_t best = 0;
+    for(int64_t i = 1; i < n; i++)
+        if(std::fabs(w[i] - cfg.target) < std::fabs(w[best] - cfg.target)) best = i;
+    if(x_out) {
+        eig_pick_column_kernel<T><<<(int)std::min<int64_t>((n + 255) / 256, 1024), 256, 0, op->stream>>>(evecs, n, best, reinterpret_cast<T *>(x_out));
+        HEFF_LAUNCH_CHECK();
+    }
+    HEFF_CUDA(cudaStreamSynchronize(op->stream));
+    res.eigval    = w[best];
+    res.resnorm   = 0.0;
+    res.converged = 1;
+    res.seconds   = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return HEFF_OK;
+}
+
 template<bool CPLX>
 static int eigs_impl(heff_op *op, const heff_eig_config &cfg, const void *x0, void *x_out, heff_eig_result &res) {
     using T          = typename Scalar<CPLX>::T;
+    if(cfg.ritz == HEFF_RITZ_TARGET && op->d.size_mps() <= 2048 && !op->sequential && op->W) return eigs_dense_target<CPLX>(op, cfg, x_out, res);
     auto       t0    = std::chrono::steady_clock::now();
     const bool mixed = cfg.mixed && op->precision == HEFF_PREC_MIXED && op->mixed_apply;
     Davidson<CPLX> D(op, cfg, res);

@@ -635,6 +635,7 @@ extern "C" int heff_op_destroy(heff_op *op) {
     if(op->eig_ws) cudaFree(op->eig_ws);
     if(op->Rtmp) cudaFree(op->Rtmp);
     if(op->arena_vec) cudaFree(op->arena_vec);
+    if(op->dense_ws) cudaFree(op->dense_ws);
     for(void *p : op->seq_W) cudaFree(p);
     if(op->pipe) {
         if(op->pipe->aux) cudaStreamDestroy(op->pipe->aux);
@@ -751,6 +752,13 @@ extern "C" int heff_op_set_fp64_engine(heff_op *op, int engine, int nslices) {
         op->emu_slices = nslices;
     }
     op->fp64_engine = engine;
+    return HEFF_OK;
+}
+
+extern "C" int heff_op_set_graphs(heff_op *op, int enable) {
+    if(!op) return HEFF_BAD_ARG;
+    op->graphs = enable != 0;
+    if(!op->graphs) op_graph_release(op);
     return HEFF_OK;
 }
 

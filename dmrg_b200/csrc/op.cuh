@@ -67,6 +67,9 @@ struct heff_op {
     int                emu_slices    = 7;
     void              *emu           = nullptr;
     bool               emu_stale     = true;
+    // dense interior solve (heff_eigs with HEFF_RITZ_TARGET at rows() <= 4096): matrix, eigenvalues, eigenvectors
+    void              *dense_ws      = nullptr;
+    size_t             dense_bytes   = 0;
     // CUDA graph of the FP64 DMMA matvec (heff_op_set_graphs, on by default): captured at the second product of a
     // shape on a non-default stream and replayed with the input and output retargeted
     bool               graphs        = true;

@@ -313,7 +313,9 @@ int heff_gemm_set_tail_split(int mode);
 typedef enum { HEFF_RITZ_SA = 0, HEFF_RITZ_LA = 1, HEFF_RITZ_TARGET = 2 } heff_ritz;
 
 typedef struct {
-    int     ritz;        /* heff_ritz: smallest / largest algebraic, or closest to `target` */
+    int     ritz;        /* heff_ritz: smallest / largest algebraic, or closest to `target` (interior:
+                            at rows() <= 2048 solved densely, get_matrix + heff_dense_eig, as the
+                            reference's dense path for small problems, AlgorithmFinite.cpp:318) */
     double  target;      /* target eigenvalue for HEFF_RITZ_TARGET */
     double  tol;         /* ||H x - theta x|| <= tol * ||H||_est (PRIMME eps, solver_primme.cpp:364); default 1e-12 */
     int     max_basis;   /* Davidson basis size (<= 128), default 24 */

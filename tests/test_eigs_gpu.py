@@ -36,15 +36,23 @@ def test_eigs_small_vs_dense(cuda, c, ritz):
     op.close()
 
 
-def test_eigs_target_interior(cuda):
-    th, W, L, R = ph.heff_inputs(6, D=3, cplx=False, seed=5, chiR=6)
+@pytest.mark.parametrize("chi,chiR,c", [(6, 6, False), (7, 5, True), (16, 16, False), (12, 10, True)])
+def test_eigs_target_interior(cuda, chi, chiR, c):
+    """Closest-to-target interior eigenpairs: at rows() <= 2048 the dense path (get_matrix + the device dense
+    eigensolver), as the reference switches to a dense solver for small problems; eigenvalue and eigenvector."""
+    th, W, L, R = ph.heff_inputs(chi, D=3, cplx=c, seed=5 + chi, chiR=chiR)
     H = dense(th, W, L, R)
     w = np.linalg.eigvalsh(H)
     target = 0.5 * (w[0] + w[-1]) + 0.01
-    op = hb.MatVecMPOS([W], L, R)
-    e, res = op.eigs(ritz="TARGET", target=target, tol=1e-11, max_basis=64, min_basis=16)
+    op = hb.MatVecMPOS([W], L, R, cplx=c)
+    x = torch.empty(th.size, dtype=torch.complex128 if c else torch.float64, device="cuda")
+    e, res = op.eigs(x_out=x, ritz="TARGET", target=target, tol=1e-11, max_basis=64, min_basis=16)
     want = w[np.argmin(np.abs(w - target))]
+    assert res["converged"] == 1
     assert abs(e - want) < 1e-9 * np.max(np.abs(w))
+    xv = x.cpu().numpy()
+    assert abs(np.linalg.norm(xv) - 1) < 1e-12
+    assert np.linalg.norm(H @ xv - e * xv) < 1e-9 * np.max(np.abs(w))
     op.close()
 
 
