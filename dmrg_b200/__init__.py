@@ -250,7 +250,7 @@ def xdmrg(h, energy_target, one_site=False, **kw):
 
 def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, precision=PREC_FP64, seed=0, ritz="SA", target=0.0,
           energy_shift_per_site=0.0, algorithm=0, precond=-1, fp64_engine=FP64_DMMA, expansion_alpha=0.0, warmup_sweeps=-1, bond_min=0,
-          stream=None):
+          jcb_blocksize=0, eig_max_matvecs=0, stream=None):
     """DMRG of the random-field Ising chain on the device (heff_dmrg_run); returns the result dict.  algorithm 0: two-site
     ground state, 1: two-site folded spectrum, 2 / 3: the same with one-site DMRG and forward subspace expansion."""
     from ._sigs import DmrgConfig, DmrgResult
@@ -276,6 +276,8 @@ def fdmrg(h, J=1.0, chi_max=64, sweeps=10, trunc_lim=1e-12, eig_tol=1e-12, preci
     cfg.expansion_alpha = float(expansion_alpha)
     cfg.warmup_sweeps = int(warmup_sweeps)
     cfg.bond_min = int(bond_min)
+    cfg.jcb_blocksize = int(jcb_blocksize)
+    cfg.eig_max_matvecs = int(eig_max_matvecs)
     res = DmrgResult()
     check(lib().heff_dmrg_run(ctypes.byref(cfg), ctypes.byref(res), _stream_handle(stream)), "heff_dmrg_run")
     return res.as_dict()

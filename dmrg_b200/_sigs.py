@@ -34,7 +34,8 @@ class DmrgConfig(ctypes.Structure):
                 ("trunc_lim", ctypes.c_double), ("eig_tol", ctypes.c_double), ("ritz", ctypes.c_int), ("target", ctypes.c_double),
                 ("precision", ctypes.c_int), ("seed", ctypes.c_int64), ("energy_shift_per_site", ctypes.c_double), ("algorithm", ctypes.c_int),
                 ("precond", ctypes.c_int), ("fp64_engine", ctypes.c_int), ("expansion_alpha", ctypes.c_double),
-                ("warmup_sweeps", ctypes.c_int), ("bond_min", ctypes.c_int64)]
+                ("warmup_sweeps", ctypes.c_int), ("bond_min", ctypes.c_int64), ("jcb_blocksize", ctypes.c_int64),
+                ("eig_max_matvecs", ctypes.c_int64)]
 
 
 class DmrgResult(ctypes.Structure):
