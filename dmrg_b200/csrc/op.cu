@@ -1,5 +1,7 @@
 // heff_op: the MatVecMPOS<T> / MatVecMPO<T> operator object behind the C ABI
 // (source/math/eig/matvec/matvec_mpos.h:23-180, matvec_mpos.cpp:40-130, 963-984).
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -484,6 +486,31 @@ struct MatvecGraph {
     }
 };
 
+// Step trace of the graph path on stderr (environment variable HEFF_GRAPHS_TRACE=1), for diagnosing a failure.
+static bool graph_trace() {
+    static const bool on = [] {
+        const char *e = getenv("HEFF_GRAPHS_TRACE");
+        return e && atoi(e) != 0;
+    }();
+    return on;
+}
+#define GTRACE(...)                                \
+    do {                                           \
+        if(graph_trace()) {                        \
+            fprintf(stderr, "[heff graph] " __VA_ARGS__); \
+            fputc('\n', stderr);                  \
+            fflush(stderr);                        \
+        }                                          \
+    } while(0)
+
+bool graphs_default() {
+    static const bool on = [] {
+        const char *e = getenv("HEFF_GRAPHS");
+        return e && atoi(e) != 0;
+    }();
+    return on;
+}
+
 void op_graph_release(heff_op *op) {
     delete op->mg;
     op->mg = nullptr;
@@ -512,15 +539,19 @@ static void graph_capture(heff_op *op, const void *x, void *y) {
     MatvecGraph *G = new MatvecGraph();
     G->d = op->d, G->cplx = CPLX, G->L = op->L, G->Rp = op->Rp, G->W = op->W, G->scr = op->scratch, G->split = op->split_ws;
     G->split_bytes = op->split_bytes;
+    GTRACE("capture begin (S=%lld cL=%lld cR=%lld DL=%lld DR=%lld cplx=%d)", (long long)op->d.S, (long long)op->d.cL, (long long)op->d.cR,
+           (long long)op->d.DL, (long long)op->d.DR, (int)CPLX);
     if(cudaStreamBeginCapture(op->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return give_up(G);
     const int   rc = plain_apply<CPLX>(op, x, y);
     cudaGraph_t g  = nullptr;
     const cudaError_t e = cudaStreamEndCapture(op->stream, &g);
+    GTRACE("capture end rc=%d err=%d graph=%p", rc, (int)e, (void *)g);
     G->g = g;
     if(rc != HEFF_OK || e != cudaSuccess || !g) return give_up(G);
     if(cudaGraphInstantiate(&G->ex, g, 0) != cudaSuccess) return give_up(G);
     size_t nn = 0;
     if(cudaGraphGetNodes(g, nullptr, &nn) != cudaSuccess) return give_up(G);
+    GTRACE("instantiated, %zu nodes", nn);
     std::vector<cudaGraphNode_t> nodes(nn);
     if(cudaGraphGetNodes(g, nodes.data(), &nn) != cudaSuccess) return give_up(G);
     const void *pf = permute_kernel_fn(CPLX);
@@ -530,13 +561,17 @@ static void graph_capture(heff_op *op, const void *x, void *y) {
         if(t != cudaGraphNodeTypeKernel) continue;
         cudaKernelNodeParams p{};
         if(cudaGraphKernelNodeGetParams(nd, &p) != cudaSuccess || !p.kernelParams) return give_up(G);
+        GTRACE("kernel node func=%p permute=%d gemm=%d", p.func, (int)(p.func == pf), (int)gemm_fn_known(p.func));
         if(p.func == pf) {
-            if(G->perm) return give_up(G);
+            const void *x0 = nullptr;
+            std::memcpy(&x0, p.kernelParams[0], sizeof(x0));  // the node's argument storage need not be aligned for the type
+            if(G->perm || x0 != x) return give_up(G);
             G->perm   = nd;
             G->perm_p = p;
             G->perm_args.assign(p.kernelParams, p.kernelParams + 5);  // (x, xp, S, cL, n)
         } else if(gemm_fn_known(p.func)) {
-            const GemmArgs a = *reinterpret_cast<const GemmArgs *>(p.kernelParams[0]);
+            GemmArgs a;
+            std::memcpy(&a, p.kernelParams[0], sizeof(a));  // byte copy: GemmArgs holds 16-byte-aligned members
             if(a.C == y) {
                 G->outs.push_back(nd);
                 G->out_p.push_back(p);
@@ -544,6 +579,7 @@ static void graph_capture(heff_op *op, const void *x, void *y) {
             }
         }
     }
+    GTRACE("perm=%p outs=%zu", (void *)G->perm, G->outs.size());
     if(!G->perm || G->outs.empty()) return give_up(G);
     op->mg = G;
 }
@@ -556,6 +592,8 @@ static int graph_replay(heff_op *op, const void *x, void *y) {
     pa[0]                   = const_cast<void *>(reinterpret_cast<const void *>(&xv));
     cudaKernelNodeParams pp = G->perm_p;
     pp.kernelParams         = pa.data();
+    pp.extra                = nullptr;
+    GTRACE("replay: set input");
     HEFF_CUDA(cudaGraphExecKernelNodeSetParams(G->ex, G->perm, &pp));
     for(size_t i = 0; i < G->outs.size(); i++) {
         GemmArgs a             = G->out_a[i];
@@ -563,8 +601,10 @@ static int graph_replay(heff_op *op, const void *x, void *y) {
         void                *args[1] = {&a};
         cudaKernelNodeParams q = G->out_p[i];
         q.kernelParams         = args;
+        q.extra                = nullptr;
         HEFF_CUDA(cudaGraphExecKernelNodeSetParams(G->ex, G->outs[i], &q));
     }
+    GTRACE("replay: launch");
     HEFF_CUDA(cudaGraphLaunch(G->ex, op->stream));
     return HEFF_OK;
 }

@@ -6,7 +6,8 @@
 #include "multi.cuh"
 
 namespace heff {
-struct MatvecGraph;  // op.cu
+struct MatvecGraph;     // op.cu
+bool graphs_default();  // op.cu: environment variable HEFF_GRAPHS (1 on, default off)
 }
 
 struct heff_op {
@@ -70,9 +71,9 @@ struct heff_op {
     // dense interior solve (heff_eigs with HEFF_RITZ_TARGET at rows() <= 4096): matrix, eigenvalues, eigenvectors
     void              *dense_ws      = nullptr;
     size_t             dense_bytes   = 0;
-    // CUDA graph of the FP64 DMMA matvec (heff_op_set_graphs, on by default): captured at the second product of a
+    // CUDA graph of the FP64 DMMA matvec (heff_op_set_graphs; default from HEFF_GRAPHS): recorded after the first product of a
     // shape on a non-default stream and replayed with the input and output retargeted
-    bool               graphs        = true;
+    bool               graphs        = heff::graphs_default();
     heff::MatvecGraph *mg            = nullptr;
     // mixed-precision state (owned by the mixed path; null until first use)
     void              *mixed         = nullptr;

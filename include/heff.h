@@ -208,7 +208,8 @@ int64_t heff_op_num_mv(const heff_op *op);
  * (layout, GEMM 1, MPO mix, GEMM 2).  heff_op_stage_times synchronises the op's
  * stream and returns the summed milliseconds per stage and the matvec count. */
 int heff_op_set_profiling(heff_op *op, int enable);
-/* CUDA graphs for the FP64 matvec (on by default; no counterpart in the reference):
+/* CUDA graphs for the FP64 matvec (off by default, or on for every operator when the
+ * environment variable HEFF_GRAPHS=1; no counterpart in the reference):
  * on an operator created with a non-default stream, the first product of a shape
  * runs as plain kernel launches and is recorded as a graph; later products of that
  * shape replay it with the input and output retargeted (one launch instead of

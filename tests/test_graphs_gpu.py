@@ -17,6 +17,7 @@ def test_graph_replay_matches_plain_launches(cuda, chi, chiR, D, c):
     th, W, L, R = ph.heff_inputs(chi, D=D, cplx=c, seed=chi + D, chiR=chiR)
     st = torch.cuda.Stream()
     opg = hb.MatVecMPOS([W], L, R, cplx=c, stream=st)
+    opg.set_graphs(True)
     opp = hb.MatVecMPOS([W], L, R, cplx=c, stream=st)
     opp.set_graphs(False)
     dt = torch.complex128 if c else torch.float64
