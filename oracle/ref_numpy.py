@@ -219,3 +219,95 @@ def matvec_flops(S, cL, cR, DL, DR, cplx=False):
     a complex multiply-add counts 8 real FLOPs (x4)."""
     f = 2.0 * S * cL * cL * cR * DL + 2.0 * cL * cR * S * DL * S * DR + 2.0 * S * cL * cR * cR * DR
     return 4.0 * f if cplx else f
+
+
+def dmrg1_expansion_model(mpos, chi_max, sweeps, alpha0=1e-3, trunc_lim=1e-12, seed=0):
+    """Host model of the one-site DMRG sweep with forward subspace expansion (the device driver, algorithm 2), in the
+    driver's index maps, for small chains: site tensors M[i] [d, chi_i, chi_{i+1}], environments of the sites < i and
+    > i, the expansion term of EnvBase::get_expansion_term (expansion_term_einsum; the R side read by its index meaning
+    [s', b', (a, m)]), the enlarged-bond SVDs of expand_environment_1site (merge_expansion_term_PR / _PL), dense local
+    eigensolves, and the mixing factor alpha0 halved every sweep and off for the last two.  Returns the energy of the
+    last local solve per sweep and the final bond dimensions."""
+    L = len(mpos)
+    d = mpos[0].shape[2]
+    rng = np.random.default_rng(seed)
+    M = []
+    for _ in range(L):
+        v = rng.uniform(-0.5, 0.5, d)
+        M.append((v / np.linalg.norm(v)).reshape(d, 1, 1))
+    Le, Re = [None] * (L + 1), [None] * (L + 1)
+    Le[0], Re[L - 1] = np.ones((1, 1, 1)), np.ones((1, 1, 1))
+
+    def renv(i):
+        Re[i] = env_update_einsum("R", Re[i + 1], M[i + 1], mpos[i + 1])
+
+    def lenv(i):
+        Le[i + 1] = env_update_einsum("L", Le[i], M[i], mpos[i])
+
+    def svd(A, rmax):
+        U, S, VT = np.linalg.svd(A, full_matrices=False)
+        tail = np.sqrt(np.cumsum(S[::-1] ** 2))[::-1]
+        k = max(1, min(int(np.count_nonzero(tail >= trunc_lim)), rmax))
+        return U[:, :k], S[:k], VT[:k], k
+
+    def solve(i):
+        shape = M[i].shape
+        n = int(np.prod(shape))
+        H = np.stack([matvec_einsum(np.eye(n)[:, k].reshape(shape, order="F"), mpos[i], Le[i], Re[i]).ravel(order="F")
+                      for k in range(n)], axis=1)
+        w, v = np.linalg.eigh((H + H.T) / 2)
+        M[i] = v[:, 0].reshape(shape, order="F")
+        return w[0]
+
+    def rows(T):  # [s, a, b] -> [a, (s, b)]
+        return T.transpose(1, 0, 2).reshape(T.shape[1], -1, order="F")
+
+    def unrows(X, k, cb):  # [a, (s, b)] -> [s, a, b]
+        return X.reshape(k, d, cb, order="F").transpose(1, 0, 2)
+
+    for i in range(L - 2, -1, -1):
+        renv(i)
+    energies = []
+    E = None
+    for sweep in range(sweeps):
+        alpha = alpha0 * 2.0 ** (-sweep) if sweep + 2 < sweeps else 0.0
+        for i in range(L - 1):
+            if alpha > 0:
+                _, ca, c = M[i].shape
+                cb = M[i + 1].shape[2]
+                P = expansion_term_einsum("R", Re[i + 1], M[i + 1], mpos[i + 1], alpha)
+                DL = mpos[i + 1].shape[0]
+                Psem = P.ravel(order="F").reshape(d, cb, c * DL, order="F").transpose(0, 2, 1)  # [s', (a, m), b']
+                X = np.concatenate([rows(M[i + 1]), rows(Psem)], axis=0)
+                U, S, VT, k = svd(X, min(d * ca, d * cb, chi_max))
+                M[i] = ((M[i].reshape(d * ca, c, order="F") @ U[:c]) * S).reshape(d, ca, k, order="F")
+                M[i + 1] = unrows(VT, k, cb)
+                renv(i)
+            E = solve(i)
+            _, ca, c = M[i].shape
+            cb = M[i + 1].shape[2]
+            U, S, VT, k = svd(M[i].reshape(d * ca, c, order="F"), chi_max)
+            S = S / np.linalg.norm(S)
+            M[i] = U.reshape(d, ca, k, order="F")
+            M[i + 1] = unrows((S[:, None] * VT) @ rows(M[i + 1]), k, cb)
+            lenv(i)
+        for i in range(L - 1, 0, -1):
+            if alpha > 0:
+                _, ca, c = M[i - 1].shape
+                cb = M[i].shape[2]
+                PL = expansion_term_einsum("L", Le[i - 1], M[i - 1], mpos[i - 1], alpha)
+                X = np.concatenate([M[i - 1].ravel(order="F"), PL.ravel(order="F")]).reshape(d * ca, -1, order="F")
+                U, S, VT, k = svd(X, min(d * ca, d * cb, chi_max))
+                M[i - 1] = U.reshape(d, ca, k, order="F")
+                M[i] = unrows((S[:, None] * VT[:, :c]) @ rows(M[i]), k, cb)
+                lenv(i - 1)
+            E = solve(i)
+            _, c, cb = M[i].shape
+            ca = M[i - 1].shape[1]
+            U, S, VT, k = svd(rows(M[i]), chi_max)
+            S = S / np.linalg.norm(S)
+            M[i] = unrows(VT, k, cb)
+            M[i - 1] = ((M[i - 1].reshape(d * ca, c, order="F") @ U) * S).reshape(d, ca, k, order="F")
+            renv(i - 1)
+        energies.append(E)
+    return energies, [m.shape[2] for m in M[:-1]]
