@@ -448,10 +448,7 @@ def measure_eigs_folded(hb, torch, chi=512):
         return e, r, time.perf_counter() - t0
 
     out = {}
-    opb = hb.MatVecMPOS([W], L, R, cplx=False)
-    opb.set_jacobi_blocksize(128)  # the reference's starting block size (eigs_jcb_min_blocksize, settings.h:261)
-    for name, op, kw in (("fp64", op64, {"mixed": False}), ("fp64_jacobi", op64, {"mixed": False, "precond": 1}),
-                         ("fp64_block_jacobi_128", opb, {"mixed": False, "precond": 1}), ("mixed", opm, {"mixed": True})):
+    for name, op, kw in (("fp64", op64, {"mixed": False}), ("fp64_jacobi", op64, {"mixed": False, "precond": 1}), ("mixed", opm, {"mixed": True})):
         solve(op, **kw)
         runs = [solve(op, **kw) for _ in range(2)]
         t = statistics.median(r[2] for r in runs)
@@ -460,12 +457,10 @@ def measure_eigs_folded(hb, torch, chi=512):
                      "converged": r["converged"]}
     op64.close()
     opm.close()
-    opb.close()
     out["workload"] = "lowest eigenpair, real H_eff, two-site MPO squared D=9, chi=512, tol 1e-12 (the folded-spectrum solve's shape)"
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     out["abs_dE_mixed_vs_fp64"] = abs(out["mixed"]["E"] - out["fp64"]["E"])
     out["abs_dE_jacobi_vs_fp64"] = abs(out["fp64_jacobi"]["E"] - out["fp64"]["E"])
-    out["abs_dE_block_jacobi_vs_fp64"] = abs(out["fp64_block_jacobi_128"]["E"] - out["fp64"]["E"])
     return out
 
 

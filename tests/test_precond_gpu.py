@@ -162,13 +162,19 @@ def test_block_jacobi_of_whole_operator_is_the_inverse(cuda):
 
 @pytest.mark.parametrize("c", [False, True])
 def test_block_jacobi_eigs_vs_dense(cuda, c):
-    """The preconditioned Davidson with block-Jacobi expansion vectors converges to the dense eigenvalues; the folded
-    shape (MPO squared, D=9) is where the reference's PRIMME set-up uses it (optimize_folded_spectrum.cpp:303-304)."""
+    """The preconditioned Davidson with block-Jacobi expansion vectors converges to the dense eigenvalues.  The blocks are
+    formed at the shift of the first MultPc (readyCalcPc), so the caller sets it the way PRIMME's preconditioner shift
+    is set for a smallest-eigenvalue solve: at a lower bound of the spectrum (here w[0] - 1; in the folded spectrum the
+    operator is positive semidefinite and the bound is 0), where every block B - shift I is positive definite."""
     th, W, L, R = ph.heff_inputs(8, D=3, cplx=c, seed=22, chiR=7)
     w = np.linalg.eigvalsh(dense(th, W, L, R))
+    x = hb.to_device(th)
+    y = torch.empty_like(x)
     for bs in (1, 16, 64):
         op = hb.MatVecMPOS([W], L, R, cplx=c)
         op.set_jacobi_blocksize(bs)
+        if bs > 1:
+            op.MultPc(x, y, float(w[0] - 1.0))  # forms the blocks at the lower bound
         e, res = op.eigs(ritz="SA", tol=1e-12, mixed=False, precond=1)
         assert res["converged"] == 1, (bs, res)
         assert abs(e - w[0]) < 1e-10 * max(1.0, abs(w[0])), bs

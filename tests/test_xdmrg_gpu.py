@@ -18,12 +18,19 @@ def spectrum(h):
     return np.linalg.eigvalsh(H)
 
 
+# The chain's spectrum is symmetric (E <-> -E), so energy density 0.5 falls exactly between the pairs +-E_k, whose
+# folded eigenvalues (E_k - E_t)^2 coincide; a variance minimiser then has no unique answer.  As the reference moves
+# its target off the symmetric point (energy_spectrum_shift, settings.h:427), the target is offset by 0.01, a
+# fraction of the level spacing at L=10.
+OFFSET = 0.01
+
+
 @pytest.mark.parametrize("density", [0.5, 0.3])
 def test_xdmrg_finds_eigenstate_near_target(cuda, density):
     h = ph.random_fields(4242, 10)
     lev = ph.free_fermion_levels(h)
     emin, emax = -lev.sum(), lev.sum()
-    et = emin + density * (emax - emin)
+    et = emin + density * (emax - emin) + OFFSET
     r = hb.xdmrg(h, et, chi_max=32, sweeps=12, eig_tol=1e-12, seed=1)
     w = spectrum(h)
     assert r["variance"] < 1e-10, r
@@ -35,7 +42,7 @@ def test_xdmrg_finds_eigenstate_near_target(cuda, density):
 def test_xdmrg_mixed_matches_fp64(cuda):
     h = ph.random_fields(4242, 10)
     lev = ph.free_fermion_levels(h)
-    et = -lev.sum() + 0.3 * 2 * lev.sum()  # energy density 0.3 of the spectral width
+    et = -lev.sum() + 0.3 * 2 * lev.sum() + OFFSET  # energy density 0.3 of the spectral width
     r64 = hb.xdmrg(h, et, chi_max=32, sweeps=12, eig_tol=1e-12, seed=1)
     rmx = hb.xdmrg(h, et, chi_max=32, sweeps=12, eig_tol=1e-12, seed=1, precision=hb.PREC_MIXED)
     assert r64["variance"] < 1e-10 and rmx["variance"] < 1e-10
