@@ -661,12 +661,14 @@ def main():
         clocks.start()
         time.sleep(0.3)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        launches0 = int(hb.lib().heff_matvec_launches())
         for k in range(args.steps):
             flush.fill_(float(k))  # L2 flush outside the timed events
             evs[k][0].record(stream)
             op.MultAx(x, y)
             evs[k][1].record(stream)
         stream.synchronize()
+        launches = int(hb.lib().heff_matvec_launches()) - launches0
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -751,7 +753,7 @@ def main():
                      "gemm2": stage_ms[3] / max(cnt, 1)},
         "e2e": {"value": ws * F / e2e_t / 1e12, "unit": UNIT, "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io,
                 "ms_per_step": e2e_t * 1e3, "api": "heff_op_multax_host (C ABI, pinned host buffers)"},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": launches,
         "clocks": clk,
         "cpu_baseline": cpu,
     }

@@ -106,6 +106,7 @@ def declare(L, sig):
     sig(L, "heff_gemm_i8_emu", _I, [_I, _P, _P, _P, _I64, _I64, _I64, _I, _P])
     sig(L, "heff_i8_set_tile_width", _I, [_I])
     sig(L, "heff_i8_tuned_shapes", _I, [])
+    sig(L, "heff_matvec_launches", _I64, [])
     sig(L, "heff_gemm_set_tail_split", _I, [_I])
     sig(L, "heff_op_set_fp64_engine", _I, [_P, _I, _I])
     sig(L, "heff_ensemble_run", _I, [ctypes.POINTER(DmrgConfig), _I, _I, ctypes.POINTER(DmrgResult), ctypes.POINTER(ctypes.c_int), _DP])

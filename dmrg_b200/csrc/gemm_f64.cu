@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "gemm_f64.cuh"
+#include "runtime.cuh"
 
 namespace heff {
 
@@ -112,6 +113,7 @@ static int launch_gemm(const GemmArgs &a_in, cudaStream_t stream) {
     gemm_fn_register(reinterpret_cast<const void *>(kern));
     kern<<<grid, 256, SM::BYTES, stream>>>(a);
     HEFF_LAUNCH_CHECK();
+    count_launches(sp.split > 1 ? 2 : 1);
     if(sp.split > 1) {
         const dim3 rgrid((unsigned)(tiles - sp.nfull), (unsigned)(SplitReduce<CPLX>::EPT / SplitReduce<CPLX>::EPB));
         gemm_fn_register(reinterpret_cast<const void *>(gemm_split_reduce_kernel<CPLX>));

@@ -161,6 +161,7 @@ int matvec_fp64(const MatvecDims &d, const typename Scalar<CPLX>::T *x, typename
     if(ev) HEFF_CUDA(cudaEventRecord(ev[0], s));
     permute_mps_kernel<<<grid_1d(n), 256, 0, s>>>(x, ws.xp, d.S, d.cL, n);
     HEFF_LAUNCH_CHECK();
+    count_launches(2);  // the permutation and the MPO mix below (the GEMM launcher counts its own kernels)
     if(ev) HEFF_CUDA(cudaEventRecord(ev[1], s));
     GemmArgs g1{};
     g1.M     = (int)(d.cL * d.DL);

@@ -476,6 +476,7 @@ struct MatvecGraph {
     std::vector<cudaGraphNode_t>      outs;
     std::vector<cudaKernelNodeParams> out_p;
     std::vector<GemmArgs>             out_a;
+    int                               nkernels = 0;
     ~MatvecGraph() {
         if(ex) cudaGraphExecDestroy(ex);
         if(g) cudaGraphDestroy(g);
@@ -559,6 +560,7 @@ static void graph_capture(heff_op *op, const void *x, void *y) {
         cudaGraphNodeType t;
         if(cudaGraphNodeGetType(nd, &t) != cudaSuccess) return give_up(G);
         if(t != cudaGraphNodeTypeKernel) continue;
+        G->nkernels++;
         cudaKernelNodeParams p{};
         if(cudaGraphKernelNodeGetParams(nd, &p) != cudaSuccess || !p.kernelParams) return give_up(G);
         GTRACE("kernel node func=%p permute=%d gemm=%d", p.func, (int)(p.func == pf), (int)gemm_fn_known(p.func));
@@ -606,6 +608,7 @@ static int graph_replay(heff_op *op, const void *x, void *y) {
     }
     GTRACE("replay: launch");
     HEFF_CUDA(cudaGraphLaunch(G->ex, op->stream));
+    count_launches(G->nkernels);
     return HEFF_OK;
 }
 

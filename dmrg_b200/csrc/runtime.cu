@@ -1,3 +1,4 @@
+#include <atomic>
 // Library runtime: thread-local error text, device queries and the per-(device, stream)
 // scratch workspaces used by the stateless entry points (heff_matvec_*, heff_expval_*, ...).
 #include <cstdarg>
@@ -22,6 +23,9 @@ void set_last_error_msg(const char *fmt, ...) {
     vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
     va_end(ap);
 }
+
+static std::atomic<int64_t> g_matvec_launches{0};
+void count_launches(int64_t n) { g_matvec_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int device_sm_count() {
     static int cache[64] = {0};
@@ -89,3 +93,5 @@ int release_workspaces() {
 
 extern "C" const char *heff_last_error(void) { return heff::g_last_error; }
 extern "C" const char *heff_version(void) { return "heff_b200 0.1 (sm_100a)"; }
+
+extern "C" int64_t heff_matvec_launches(void) { return heff::g_matvec_launches.load(); }

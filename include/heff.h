@@ -294,6 +294,10 @@ int heff_gemm_i8_emu(int dtype, const void *A, const void *B, void *C, int64_t M
  * setting, or -1 for an invalid value.  Process-wide tuning knob; no counterpart
  * in the reference. */
 int heff_i8_set_tile_width(int bn);
+/* Kernels launched so far by the FP64 matvec path (its permutation and MPO mix) and by every DMMA
+ * GEMM (with its tail-split reduction), graph replays included, process-wide; read it around a
+ * timed region of matvecs to count their launches.  No counterpart in the reference. */
+int64_t heff_matvec_launches(void);
 /* Number of GEMM shapes the INT8 tile-width autotuner has timed so far. */
 int heff_i8_tuned_shapes(void);
 
