@@ -464,6 +464,31 @@ def measure_eigs_folded(hb, torch, chi=512):
     return out
 
 
+def measure_xdmrg(hb, L, chi, sweeps, one_site=False, seed=4242, offset=None):
+    """The excited-state configuration's sweep: random-field Ising chain (h ~ U[0.5,1.5] from splitmix64), energy
+    density 0.5 (E_t = 0 for the symmetric spectrum, moved off the symmetric point by `offset`, a fraction of the level
+    spacing), folded spectrum with the MPO squared, FP64, local solves preconditioned with 128-row Jacobi blocks and up
+    to 60000 matvecs.  Reports the variance, the energy and, where the spectrum can be listed (L <= 20), the distance to
+    the nearest exact eigenvalue (free-fermion levels E0 + sum of a subset of 2 Lambda_k)."""
+    h = np.array(splitmix_fields(seed, L))
+    B = np.diag(h) + np.diag(np.ones(L - 1), 1)
+    lev = np.linalg.svd(B, compute_uv=False)
+    off = offset if offset is not None else (1e-3 if L <= 14 else 1e-4)
+    t0 = time.perf_counter()
+    r = hb.xdmrg(h, 0.0 + off, one_site=one_site, chi_max=chi, sweeps=sweeps, eig_tol=1e-12, seed=1, jcb_blocksize=128,
+                 eig_max_matvecs=60000)
+    secs = time.perf_counter() - t0
+    out = {"L": L, "chi_max": chi, "sweeps": sweeps, "one_site": one_site, "target": off, "variance": r["variance"],
+           "energy": r["energy"], "chi_mid": r["chi_mid"], "matvecs": r["num_mv"], "unconverged_local_solves": r["unconverged_solves"],
+           "seconds": secs, "objective_per_sweep": list(r["energy_per_sweep"][: r["sweeps_done"]])}
+    if L <= 20:
+        e = np.array([0.0])
+        for x in lev:
+            e = np.concatenate([e, e + 2 * x])
+        out["distance_to_nearest_eigenvalue"] = float(np.min(np.abs(-lev.sum() + e - r["energy"])))
+    return out
+
+
 def serving_specs(n_req, chi_lo, chi_hi, rate, precision, seed=2024):
     """The serving stream's requests: Poisson arrivals at `rate`/s, chi log-uniform in [chi_lo, chi_hi], 70% float64 /
     30% complex128, D=3 (H, lowest eigenpair) or D=9 (MPO squared: lowest eigenpair of the folded operator) with equal
@@ -588,6 +613,8 @@ def main():
     ap.add_argument("--serving-chi-max", type=int, default=2048)
     ap.add_argument("--serving-rate", type=float, default=4.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving streams (after the headline matvec)")
+    ap.add_argument("--xdmrg", default="", help="comma-separated L:chi:sweeps excited-state sweeps to run after the headline "
+                                                "matvec (e.g. 16:256:7,32:512:8); not part of the default run")
     ap.add_argument("--ensemble-n", type=int, default=32, help="realisations in the ensemble sample")
     ap.add_argument("--no-grid", action="store_true", help="skip the chi x D precision grid and the SVD timing")
     args = ap.parse_args()
@@ -689,6 +716,8 @@ def main():
             t_e2e.append(time.perf_counter() - t0)
         clk = clocks.stop()
         extras = {} if (args.no_extras or args.serving_only) else measure_mixed_and_eigs(hb, torch, op, mpos, L, R, x, y, flush, stream, F)
+    if args.xdmrg:
+        extras["xdmrg"] = [measure_xdmrg(hb, *[int(v) for v in spec.split(":")]) for spec in args.xdmrg.split(",")]
     if not args.no_extras and not args.no_serving:
         op.close()
         del x, y, flush

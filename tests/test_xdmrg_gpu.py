@@ -51,3 +51,20 @@ def test_xdmrg_mixed_matches_fp64(cuda):
     # the converged energy is an eigenvalue of H: E0 + 2 * (sum of a subset of Lambda_k)
     w = spectrum(h)
     assert np.min(np.abs(w - r64["energy"])) < 1e-9
+
+
+def test_xdmrg_block_jacobi_mid_spectrum_L12(cuda):
+    """Energy density 0.5 (+ the offset) at L=12 with chi_max=64 (exact at the middle bond), the local solves
+    preconditioned with 128-row Jacobi blocks (the reference's eigs_jcb_min_blocksize) and up to 60000 matvecs: the
+    variance falls below 1e-10 at an exact eigenvalue."""
+    h = ph.random_fields(4242, 12)
+    lev = ph.free_fermion_levels(h)
+    et = 0.0 + 1e-3  # energy density 0.5: E_min + 0.5 (E_max - E_min) = 0 for the symmetric spectrum
+    r = hb.xdmrg(h, et, chi_max=64, sweeps=7, eig_tol=1e-12, seed=1, jcb_blocksize=128, eig_max_matvecs=60000)
+    assert r["variance"] < 1e-10, r
+    e = np.array([0.0])
+    for x in lev:
+        e = np.concatenate([e, e + 2 * x])
+    w = -lev.sum() + e
+    assert np.min(np.abs(w - r["energy"])) < 1e-9
+
