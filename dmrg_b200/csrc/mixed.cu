@@ -13,6 +13,7 @@
 // adds ~sqrt(K) 2^-24).  The eigensolver uses this path for its inner iterations and restores FP64
 // accuracy by refinement with the FP64 matvec.  The environment operands (L, R') are split once per
 // operator; x and T2 are split per matvec.
+#include <cstdlib>
 #include <algorithm>
 #include <cuda_bf16.h>
 
@@ -307,8 +308,18 @@ __global__ void __launch_bounds__(32 * TA) mix_mixed_kernel(const float *__restr
         }
 }
 
-// Tile height: 16 a' when the staging fits in ~100 KB (two or more CTAs per SM), else 8.
-static int mx_ta(int64_t NP, int cf) { return (size_t)cf * 4 * NP * mx_sstr<16>() <= 100 * 1024 ? 16 : 8; }
+// Tile height: 16 a' when the staging fits in ~100 KB (two or more CTAs per SM), else 8; the environment variable
+// HEFF_MIX_TA (8 or 16) overrides it for measurements.
+static int mx_ta(int64_t NP, int cf) {
+    static const int forced = [] {
+        const char *e = getenv("HEFF_MIX_TA");
+        const int   v = e ? atoi(e) : 0;
+        return (v == 8 || v == 16) ? v : 0;
+    }();
+    if(forced == 8) return 8;
+    if(forced == 16 && (size_t)cf * 4 * NP * mx_sstr<16>() <= 200 * 1024) return 16;
+    return (size_t)cf * 4 * NP * mx_sstr<16>() <= 100 * 1024 ? 16 : 8;
+}
 static size_t mx_smem(int64_t NP, int cf, int ta, int wl_bytes) {
     return (size_t)cf * 4 * NP * (ta == 16 ? mx_sstr<16>() : mx_sstr<8>()) + (size_t)wl_bytes;
 }
