@@ -240,7 +240,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     ws.op->precision = (heff_precision)cfg.precision;
     if(cfg.fp64_engine != HEFF_FP64_DMMA && cfg.fp64_engine != HEFF_FP64_INT8) return HEFF_BAD_ARG;
     ws.op->fp64_engine = cfg.fp64_engine;
-    HEFF_TRY(heff_op_set_jacobi_blocksize(ws.op, cfg.jcb_blocksize > 0 ? cfg.jcb_blocksize : 1));
+    HEFF_TRY(heff_op_set_jacobi_blocksize(ws.op, cfg.jcb_blocksize > 0 ? cfg.jcb_blocksize : (folded ? 128 : 1)));
     // --- model (host copies stay alive until the stream has consumed them): H, or (H - E_t)^2 for xDMRG
     std::vector<std::vector<double>>    Wh(L);
     std::vector<std::array<int64_t, 4>> wd(L);
@@ -282,7 +282,7 @@ static int dmrg_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, DmrgW
     ecfg.target      = cfg.target;
     ecfg.mixed       = cfg.precision == HEFF_PREC_MIXED;
     ecfg.precond     = cfg.precond >= 0 ? cfg.precond : (cfg.algorithm == 1 ? 1 : 0);  // H^2: Jacobi (optimize_folded_spectrum.cpp:303-304)
-    ecfg.max_matvecs = cfg.eig_max_matvecs > 0 ? cfg.eig_max_matvecs : (folded ? 20000 : 4000);
+    ecfg.max_matvecs = cfg.eig_max_matvecs > 0 ? cfg.eig_max_matvecs : (folded ? 60000 : 4000);
     double energy    = 0;
     for(int sweep = 0; sweep < cfg.sweeps; sweep++) {
         const int64_t chi_lim = sweep_bond_limit(cfg, sweep);
@@ -532,7 +532,7 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
     ws.op->precision = (heff_precision)cfg.precision;
     if(cfg.fp64_engine != HEFF_FP64_DMMA && cfg.fp64_engine != HEFF_FP64_INT8) return HEFF_BAD_ARG;
     ws.op->fp64_engine = cfg.fp64_engine;
-    HEFF_TRY(heff_op_set_jacobi_blocksize(ws.op, cfg.jcb_blocksize > 0 ? cfg.jcb_blocksize : 1));
+    HEFF_TRY(heff_op_set_jacobi_blocksize(ws.op, cfg.jcb_blocksize > 0 ? cfg.jcb_blocksize : (folded ? 128 : 1)));
     std::vector<std::vector<double>>    Wh(L);
     std::vector<std::array<int64_t, 4>> wd(L);
     for(int i = 0; i < L; i++) {
@@ -577,7 +577,7 @@ static int dmrg1_run_ws(const heff_dmrg_config &cfg, heff_dmrg_result &res, Dmrg
     ecfg.target      = cfg.target;
     ecfg.mixed       = cfg.precision == HEFF_PREC_MIXED;
     ecfg.precond     = cfg.precond >= 0 ? cfg.precond : (folded ? 1 : 0);
-    ecfg.max_matvecs = cfg.eig_max_matvecs > 0 ? cfg.eig_max_matvecs : (folded ? 20000 : 4000);
+    ecfg.max_matvecs = cfg.eig_max_matvecs > 0 ? cfg.eig_max_matvecs : (folded ? 60000 : 4000);
     double              energy = 0, t_env = 0, t_eig = 0, t_svd = 0;
     auto                now  = [] { return std::chrono::steady_clock::now(); };
     auto                secs = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };

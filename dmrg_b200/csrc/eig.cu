@@ -620,9 +620,20 @@ static int eigs_impl(heff_op *op, const heff_eig_config &cfg, const void *x0, vo
     double theta = 0, rnorm = INFINITY;
     bool   conv  = false;
     if(mixed) {
-        HEFF_TRY(D.run(x0, true, cfg.mixed_tol > 0 ? cfg.mixed_tol : 1e-5, cfg.max_matvecs, theta, rnorm, conv));
+        const double mtol = cfg.mixed_tol > 0 ? cfg.mixed_tol : 1e-5;
+        HEFF_TRY(D.run(x0, true, mtol, cfg.max_matvecs, theta, rnorm, conv));
         res.num_mv_phase1 = res.num_mv;
-        HEFF_TRY(D.refine(theta, rnorm, conv));
+        if(std::fabs(theta) < 10.0 * mtol * std::max(D.anorm, 1e-300)) {
+            // The eigenvalue sits within the split-BF16 operator's error (~4e-5 of its norm) of zero -- the folded
+            // spectrum's (E_k - E_t)^2 near convergence: corrections solved on that operator cannot resolve it, so
+            // the solve finishes in FP64 from the phase-1 vector (preconditioned when asked).
+            if(cfg.precond == 1)
+                HEFF_TRY(D.run_pc(D.x, cfg.tol, cfg.max_matvecs, theta, rnorm, conv));
+            else
+                HEFF_TRY(D.run(D.x, false, cfg.tol, cfg.max_matvecs, theta, rnorm, conv));
+        } else {
+            HEFF_TRY(D.refine(theta, rnorm, conv));
+        }
     } else if(cfg.precond == 1) {
         HEFF_TRY(D.run_pc(x0, cfg.tol, cfg.max_matvecs, theta, rnorm, conv));
     } else {

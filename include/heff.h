@@ -391,9 +391,11 @@ typedef struct {
     int64_t       bond_min;              /* bond limit of the warm-up sweeps (0: 8, the xDMRG bond_min of
                                             settings.h:432) */
     int64_t       jcb_blocksize;         /* Jacobi block size of the preconditioned local solves
-                                            (heff_op_set_jacobi_blocksize); 0: 1 (diagonal) */
+                                            (heff_op_set_jacobi_blocksize); 0: 128 for the folded spectrum (the
+                                            reference's eigs_jcb_min_blocksize, settings.h:261), 1 (diagonal)
+                                            otherwise */
     int64_t       eig_max_matvecs;       /* matvec limit of one local solve; 0: 4000 for the ground state,
-                                            20000 for the folded spectrum (the reference allows eigs_iter_max =
+                                            60000 for the folded spectrum (the reference allows eigs_iter_max =
                                             100000, settings.h:251) */
 } heff_dmrg_config;
 

@@ -67,4 +67,10 @@ def test_xdmrg_block_jacobi_mid_spectrum_L12(cuda):
         e = np.concatenate([e, e + 2 * x])
     w = -lev.sum() + e
     assert np.min(np.abs(w - r["energy"])) < 1e-9
+    # mixed precision: split-BF16 products while the folded eigenvalue is resolvable, FP64 once it sits within the
+    # BF16 operator's error of zero; the same eigenstate as the FP64 run
+    rm = hb.xdmrg(h, et, chi_max=64, sweeps=7, eig_tol=1e-12, seed=1, jcb_blocksize=128, eig_max_matvecs=60000, precision=hb.PREC_MIXED)
+    assert rm["variance"] < 1e-10, rm
+    assert abs(rm["energy"] - r["energy"]) < 1e-9
+    assert rm["num_mv_mixed"] > 0
 
