@@ -1,7 +1,7 @@
 """H_eff matvec parity: CUDA path (through the C ABI) vs the CPU oracle.
 
-Tolerance: ||y_gpu - y_oracle|| / ||y_oracle|| <= 1e-12 (FP64 path), the bound the
-north star states for the FP64 matvec against the reference's Eigen matvec.
+Tolerance: ||y_gpu - y_oracle|| / ||y_oracle|| <= 1e-12 (FP64 path), the parity bound for the
+FP64 matvec against the reference's Eigen contraction sequence.
 """
 import numpy as np
 import pytest
