@@ -40,7 +40,7 @@ template<bool CPLX>
 struct GemmTile;
 template<>
 struct GemmTile<false> {
-    static constexpr int BM = 128, BN = 128, BK = 16, WM = 64, WN = 32, STAGES = 3;
+    static constexpr int BM = 128, BN = 128, BK = 32, WM = 64, WN = 32, STAGES = 3;  // 212 KB of stages: one barrier per 8 k-steps
     static constexpr int PAD_MN = 4;  // leading dim == 4 (mod 16) doubles: conflict-free 8-byte fragment loads
     static constexpr int PAD_K  = 4;
 };
