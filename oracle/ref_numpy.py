@@ -311,3 +311,41 @@ def dmrg1_expansion_model(mpos, chi_max, sweeps, alpha0=1e-3, trunc_lim=1e-12, s
             renv(i - 1)
         energies.append(E)
     return energies, [m.shape[2] for m in M[:-1]]
+
+
+def gauss_jordan_inverse(A, floor_rel=1e-14):
+    """Host model of the block-Jacobi inversion kernel (jcb_invert_kernel): in-place Gauss-Jordan elimination with
+    partial (row) pivoting, lowest row on ties, pivots below floor_rel x max|A| floored to that value with their sign
+    (counted), row interchanges undone as column interchanges in reverse order.  Returns (inverse, floored pivots)."""
+    A = np.array(A, dtype=np.complex128 if np.iscomplexobj(A) else np.float64, copy=True)
+    bs = A.shape[0]
+    amax = float(np.max(np.abs(A))) if A.size else 0.0
+    floor = floor_rel * (amax if amax > 0 else 1.0)
+    perm = np.zeros(bs, dtype=int)
+    floored = 0
+    for k in range(bs):
+        p = k + int(np.argmax(np.abs(A[k:, k])))
+        perm[k] = p
+        if p != k:
+            A[[k, p], :] = A[[p, k], :]
+        f = A[:, k].copy()
+        f[k] = 0
+        piv = A[k, k]
+        if not abs(piv) >= floor:
+            piv = (-floor if np.real(piv) < 0 else floor)
+            floored += 1
+        inv = 1.0 / piv
+        A[k, :] *= inv
+        A[k, k] = inv
+        rowk = A[k, :].copy()
+        for i in range(bs):
+            if i == k:
+                continue
+            ai = A[i, :].copy()
+            ai[k] = 0
+            A[i, :] = ai - f[i] * rowk
+    for k in range(bs - 1, -1, -1):
+        p = perm[k]
+        if p != k:
+            A[:, [k, p]] = A[:, [p, k]]
+    return A, floored
