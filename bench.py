@@ -464,7 +464,7 @@ def measure_eigs_folded(hb, torch, chi=512):
     return out
 
 
-def measure_xdmrg(hb, L, chi, sweeps, one_site=False, seed=4242, offset=None, precision=None):
+def measure_xdmrg(hb, L, chi, sweeps, one_site=False, seed=4242, offset=None, precision=None, jcb=128, max_mv=60000):
     """The excited-state configuration's sweep: random-field Ising chain (h ~ U[0.5,1.5] from splitmix64), energy
     density 0.5 (E_t = 0 for the symmetric spectrum, moved off the symmetric point by `offset`, a fraction of the level
     spacing), folded spectrum with the MPO squared, FP64, local solves preconditioned with 128-row Jacobi blocks and up
@@ -476,10 +476,11 @@ def measure_xdmrg(hb, L, chi, sweeps, one_site=False, seed=4242, offset=None, pr
     off = offset if offset is not None else (1e-3 if L <= 14 else 1e-4)
     t0 = time.perf_counter()
     prec = hb.PREC_FP64 if precision is None else precision
-    r = hb.xdmrg(h, 0.0 + off, one_site=one_site, chi_max=chi, sweeps=sweeps, eig_tol=1e-12, seed=1, jcb_blocksize=128,
-                 eig_max_matvecs=60000, precision=prec)
+    r = hb.xdmrg(h, 0.0 + off, one_site=one_site, chi_max=chi, sweeps=sweeps, eig_tol=1e-12, seed=1, jcb_blocksize=jcb,
+                 eig_max_matvecs=max_mv, precision=prec)
     secs = time.perf_counter() - t0
     out = {"L": L, "chi_max": chi, "sweeps": sweeps, "one_site": one_site, "precision": "mixed" if prec == hb.PREC_MIXED else "fp64",
+           "jacobi_block": jcb, "local_solve_matvec_limit": max_mv,
            "target": off, "variance": r["variance"], "mixed_matvecs": r["num_mv_mixed"],
            "energy": r["energy"], "chi_mid": r["chi_mid"], "matvecs": r["num_mv"], "unconverged_local_solves": r["unconverged_solves"],
            "seconds": secs, "objective_per_sweep": list(r["energy_per_sweep"][: r["sweeps_done"]])}
@@ -618,8 +619,9 @@ def main():
     ap.add_argument("--serving-chi-max", type=int, default=2048)
     ap.add_argument("--serving-rate", type=float, default=4.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving streams (after the headline matvec)")
-    ap.add_argument("--xdmrg", default="", help="comma-separated L:chi:sweeps[:mixed] excited-state sweeps to run after the "
-                                                "headline matvec (e.g. 16:256:7,14:128:7:mixed); not part of the default run")
+    ap.add_argument("--xdmrg", default="", help="comma-separated L:chi:sweeps[:mixed|fp64[:jacobi block[:local matvec limit]]] "
+                                                "excited-state sweeps to run after the headline matvec (e.g. 16:256:7,14:128:7:mixed,"
+                                                "32:512:8:fp64:1:20000); not part of the default run")
     ap.add_argument("--ensemble-n", type=int, default=32, help="realisations in the ensemble sample")
     ap.add_argument("--ensemble-sweeps", type=int, default=4)
     ap.add_argument("--ensemble-serial-n", type=int, default=0, help="one-at-a-time sample (0: all realisations)")
@@ -730,7 +732,8 @@ def main():
         runs = []
         for spec in args.xdmrg.split(","):
             f = spec.split(":")
-            runs.append(measure_xdmrg(hb, int(f[0]), int(f[1]), int(f[2]), precision=hb.PREC_MIXED if f[3:] == ["mixed"] else None))
+            runs.append(measure_xdmrg(hb, int(f[0]), int(f[1]), int(f[2]), precision=hb.PREC_MIXED if f[3:4] == ["mixed"] else None,
+                                      jcb=int(f[4]) if len(f) > 4 else 128, max_mv=int(f[5]) if len(f) > 5 else 60000))
         extras["xdmrg"] = runs
     if not args.no_extras and not args.no_serving:
         op.close()
