@@ -1,0 +1,76 @@
+"""Replay of HDF5 dumps on the device.
+
+* The reference's own SVD test matrices and SVD bench matrices (HDF5 files written by the reference through h5pp,
+  committed under tests/golden/reference_h5) go through the device SVD with the reference's settings (truncation
+  limit 1e-8, tests/svd/main.cpp:71; rank_max and threshold attributes, bench/svd/main.cpp:41-42).  The rank must
+  equal the oracle's (LAPACK gesdd + the rank rule of svd.cpp:257-280); singular values agree to 1e-13 of the largest
+  and the truncated products to 1e-12 of the matrix norm.  The bench file's matrices are the ones on which the
+  reference's MKL gesdd returned info = 1 and -13.
+* The golden contraction cases, written into a ``dmrg-contractions.h5`` in the layout of contraction_tblis.cpp:72-84,
+  replay through heff_expval and heff_matvec to the golden expectation values and products.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import dmrg_b200 as hb
+from dmrg_b200 import replay
+from oracle import ref_numpy as rn
+
+import h5writer
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_h5")
+
+
+def check_against_oracle(r, A):
+    U, S, VT, k, err = rn.svd_truncated(A, r["rank_max"], r["truncation_lim"])
+    assert r["rank"] == k, (r["name"], r["rank"], k)
+    smax = S[0]
+    assert np.max(np.abs(r["S"] - S)) <= 1e-13 * smax
+    assert abs(r["truncation_error"] - err) <= 1e-13 * smax
+    Ud, VTd = r["U"], r["VT"]
+    m, n = A.shape
+    assert np.linalg.norm(Ud.conj().T @ Ud - np.eye(k)) < 1e-13 * max(m, n)
+    assert np.linalg.norm(VTd @ VTd.conj().T - np.eye(k)) < 1e-13 * max(m, n)
+    assert np.linalg.norm((Ud * r["S"]) @ VTd - (U * S) @ VT) <= 1e-12 * np.linalg.norm(A)
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(FIXTURES, "svdmatrix_*.h5"))), ids=os.path.basename)
+def test_reference_svd_test_matrices(cuda, path):
+    (r,) = replay.replay_svds(path)
+    (d,) = replay.svd_dumps(path)
+    assert r["truncation_lim"] == 1e-8 and r["shape"] == d["A"].shape
+    check_against_oracle(r, d["A"])
+
+
+def test_reference_svd_bench_matrices(cuda):
+    path = os.path.join(FIXTURES, "svd-failed.h5")
+    dumps = {d["name"]: d for d in replay.svd_dumps(path)}
+    res = replay.replay_svds(path)
+    assert [r["name"] for r in res] == [f"svd_lapacke_{i}" for i in range(4)]
+    for r in res:
+        assert "reference_S" not in r  # the dumped factors come from failed LAPACK calls
+        check_against_oracle(r, dumps[r["name"]]["A"])
+    assert [r["rank"] for r in res] == [58, 20, 20, 20]
+
+
+def test_replay_golden_contractions(cuda, golden, tmp_path):
+    root = {}
+    for i in range(10):
+        g = lambda k: golden[f"mv{i}_{k}"]
+        # h5pp stores the column-major tensors row-major with the same dimensions: a C-ordered copy of each
+        root[f"contraction_{i}"] = {k: np.ascontiguousarray(g(k)) for k in ("mps", "mpo", "envL", "envR")}
+    path = str(tmp_path / "dmrg-contractions.h5")
+    h5writer.write(path, root)
+    res = replay.replay_contractions(path)
+    assert [r["name"] for r in res] == [f"contraction_{i}" for i in range(10)]
+    for i, r in enumerate(res):
+        g = lambda k: golden[f"mv{i}_{k}"]
+        scale = np.linalg.norm(g("mps")) * np.linalg.norm(g("res"))
+        assert abs(r["energy"] - complex(g("expval")[0])) <= 1e-13 * scale
+        assert np.linalg.norm(r["Hpsi"] - g("res")) <= 1e-12 * np.linalg.norm(g("res"))
+        assert r["dims"]["mps"] == g("mps").shape
