@@ -221,8 +221,11 @@ class H5File:
         self._buf = mmap.mmap(self._fh.fileno(), 0, access=mmap.ACCESS_READ)
         self._headers = {}
         self._gheaps = {}
-        base = self._find_superblock()
-        self._parse_superblock(base)
+        try:
+            self._parse_superblock(self._find_superblock())
+        except Exception:
+            self.close()
+            raise
 
     # --- context management
     def close(self):
