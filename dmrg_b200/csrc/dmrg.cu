@@ -13,10 +13,12 @@
 // All device memory (MPS, environments, operator, eigensolver basis, SVD scratch) is allocated once per
 // workspace and reused for every bond and every realisation, so a sweep step never allocates or
 // synchronises the device -- realisations on different streams overlap.
+#include <algorithm>
 #include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -774,9 +776,29 @@ int dmrg_run(const heff_dmrg_config &cfg, heff_dmrg_result &res, cudaStream_t s)
     return dmrg_any_ws(cfg, res, ws);
 }
 
+// Estimated device time of one realisation, in units of one chi=32 two-site split (~0.75 ms): per bond and sweep, a
+// local eigensolve (~30 launch-bound matvecs at small chi, about 1.8 units; folded spectra need about ten times the
+// iterations) plus the Jacobi SVD of the (2 chi_b) x (2 chi_b) split, whose time grows as chi_b^2.2 over 32..256
+// (64^2: 0.75 ms, 512^2: 23-72 ms).  The bond dimension at bond b of an L-site spin-1/2 chain is
+// min(2^min(b, L-b), chi_max).  Only the ordering of realisations by this estimate matters.
+static double realisation_cost(const heff_dmrg_config &c) {
+    const bool   folded = c.algorithm == 1 || c.algorithm == 3;
+    const double eig    = folded ? 18.0 : 1.8;
+    double       t      = 0;
+    for(int b = 1; b < c.L; b++) {
+        const int    e   = std::min(b, c.L - b);
+        const double chb = e >= 62 ? (double)c.chi_max : std::min<double>((double)(int64_t(1) << e), (double)std::max<int64_t>(c.chi_max, 1));
+        t += eig + std::pow(chb / 32.0, 2.2);
+    }
+    return t * std::max(c.sweeps, 1);
+}
+
 // Many independent realisations: nthreads workers, each with its own stream and workspace (sized for the
-// largest chain and bond dimension), take realisations from a shared counter.  Different streams overlap
-// on the device; nthreads = 1 runs them one at a time.
+// largest chain and bond dimension), take realisations from a shared counter, longest first by
+// realisation_cost (a list schedule: the longest chains do not start last while the other workers idle; input
+// order with HEFF_ENSEMBLE_ORDER=input, for measurements).  Results stay at their input index, and each
+// realisation's result does not depend on the worker or the order.  Different streams overlap on the device;
+// nthreads = 1 runs them one at a time.
 int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_result *results, int *status, double *seconds) {
     int     Lmax   = 2;
     int64_t chimax = 1;
@@ -786,6 +808,17 @@ int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_re
     }
     int dev = 0;
     HEFF_CUDA(cudaGetDevice(&dev));
+    std::vector<int> order(n);
+    for(int i = 0; i < n; i++) order[i] = i;
+    static const bool input_order = [] {
+        const char *e = getenv("HEFF_ENSEMBLE_ORDER");
+        return e && std::strcmp(e, "input") == 0;
+    }();
+    if(!input_order) {
+        std::vector<double> cost(n);
+        for(int i = 0; i < n; i++) cost[i] = realisation_cost(cfgs[i]);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    }
     std::atomic<int>         next{0};
     std::vector<int>         rcs(nthreads, HEFF_OK);
     std::vector<std::thread> pool;
@@ -810,9 +843,10 @@ int ensemble_run(const heff_dmrg_config *cfgs, int n, int nthreads, heff_dmrg_re
         pool.emplace_back([&, t] {
             cudaSetDevice(dev);
             while(true) {
-                const int i = next.fetch_add(1);
-                if(i >= n) break;
-                status[i] = dmrg_any_ws(cfgs[i], results[i], *wss[t]);
+                const int k = next.fetch_add(1);
+                if(k >= n) break;
+                const int i = order[k];
+                status[i]   = dmrg_any_ws(cfgs[i], results[i], *wss[t]);
             }
         });
     }
