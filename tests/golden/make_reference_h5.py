@@ -7,6 +7,10 @@ present where the GPU tests run) and records each file's size and sha256 in mani
   the 1e-8 limit (98 x 90).
 * bench/svd/data/svd-failed.h5: the SVD bench's matrices on which the reference's MKL gesdd returned info = 1 or -13
   (bench/svd/main.cpp:89-108), with their rank_max and threshold attributes.
+* tests/testmatrices/lapacke_matrix-{1,2}{A,B}.h5: real symmetric 8 x 8 and 64 x 64 matrices with the eigenvalues and
+  eigenvectors the reference's LAPACK computed for them, a state theta and its overlaps |<v_i|theta>| with the
+  eigenvectors (the dense eigenproblem of a small H_eff, solved with ?syevr when the problem is small,
+  AlgorithmFinite.cpp:318).
 
 Run from the repository root with the reference checked out at REFERENCE (default /root/reference):
     python tests/golden/make_reference_h5.py
@@ -21,7 +25,8 @@ REFERENCE = os.environ.get("REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "reference_h5")
 
-FILES = [f"tests/svd/testmatrices/svdmatrix_{n}.h5" for n in (6, 96, 0, 17, 170, 101, 48)] + ["bench/svd/data/svd-failed.h5"]
+FILES = ([f"tests/svd/testmatrices/svdmatrix_{n}.h5" for n in (6, 96, 0, 17, 170, 101, 48)] + ["bench/svd/data/svd-failed.h5"]
+         + [f"tests/testmatrices/lapacke_matrix-{n}.h5" for n in ("1A", "1B", "2A", "2B")])
 
 
 def main():

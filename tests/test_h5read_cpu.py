@@ -29,7 +29,7 @@ REFERENCE = "/root/reference"
 def test_committed_fixtures_intact():
     with open(os.path.join(FIXTURES, "manifest.json")) as fh:
         manifest = json.load(fh)
-    assert len(manifest) == 8
+    assert len(manifest) == 12
     for name, meta in manifest.items():
         with open(os.path.join(FIXTURES, name), "rb") as fh:
             data = fh.read()
@@ -76,16 +76,19 @@ def test_reference_svd_bench_file():
         assert f["svd_lapacke_1/U"].shape == (0, 0)
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE, "tests/testmatrices")), reason="reference tree absent")
 @pytest.mark.parametrize("name", ["lapacke_matrix-1A.h5", "lapacke_matrix-1B.h5", "lapacke_matrix-2A.h5", "lapacke_matrix-2B.h5"])
 def test_reference_eigenproblem_fixtures(name):
-    """tests/testmatrices/lapacke_matrix-*.h5 hold a real symmetric matrix with its eigenpairs: A V = V diag(w)."""
-    with H5File(os.path.join(REFERENCE, "tests/testmatrices", name)) as f:
+    """tests/testmatrices/lapacke_matrix-*.h5 hold a real symmetric matrix with the eigenpairs the reference's LAPACK
+    computed, a state theta and its overlaps |<v_i|theta>|: A V = V diag(w), and the overlaps follow."""
+    with H5File(os.path.join(FIXTURES, name)) as f:
         A, w, V = f["matrix"].read(), f["eigvals"].read().ravel(), f["eigvecs"].read()
-    assert A.shape[0] == A.shape[1] == len(w) == V.shape[0]
+        th, ov = f["theta"].read().ravel(), f["overlaps"].read().ravel()
+    assert A.shape[0] == A.shape[1] == len(w) == V.shape[0] == th.size
     assert np.allclose(A, A.T, atol=1e-12 * np.abs(A).max())
     assert np.linalg.norm(A @ V - V * w) < 1e-8 * np.linalg.norm(A)
     assert np.allclose(np.sort(w), np.linalg.eigvalsh(A), atol=1e-8 * np.abs(w).max())
+    assert th.dtype == np.complex128 and abs(np.linalg.norm(th) - 1) < 1e-12
+    assert np.max(np.abs(np.abs(V.T @ th) - ov)) < 1e-12
 
 
 def write(tmp_path, root, name="t.h5"):

@@ -8,6 +8,10 @@
   reference's MKL gesdd returned info = 1 and -13.
 * The golden contraction cases, written into a ``dmrg-contractions.h5`` in the layout of contraction_tblis.cpp:72-84,
   replay through heff_expval and heff_matvec to the golden expectation values and products.
+* The reference's dense eigenproblem fixtures (tests/testmatrices/lapacke_matrix-*.h5: a real symmetric 8 x 8 or
+  64 x 64 matrix with the eigenvalues and eigenvectors its LAPACK computed, a state theta and the overlaps
+  |<v_i|theta>|) go through the device dense eigensolver (heff_dense_eig, the ?syevr of the small-problem path):
+  eigenvalues to 1e-13 of the largest, overlaps with theta to 1e-10 (eigenvalue gaps >= 0.12).
 """
 import glob
 import os
@@ -17,6 +21,7 @@ import pytest
 
 import dmrg_b200 as hb
 from dmrg_b200 import replay
+from dmrg_b200.h5read import H5File
 from oracle import ref_numpy as rn
 
 import h5writer
@@ -74,3 +79,18 @@ def test_replay_golden_contractions(cuda, golden, tmp_path):
         assert abs(r["energy"] - complex(g("expval")[0])) <= 1e-13 * scale
         assert np.linalg.norm(r["Hpsi"] - g("res")) <= 1e-12 * np.linalg.norm(g("res"))
         assert r["dims"]["mps"] == g("mps").shape
+
+
+@pytest.mark.parametrize("name", ["lapacke_matrix-1A.h5", "lapacke_matrix-1B.h5", "lapacke_matrix-2A.h5", "lapacke_matrix-2B.h5"])
+def test_reference_dense_eigenproblems(cuda, name):
+    with H5File(os.path.join(FIXTURES, name)) as f:
+        A, w, V = f["matrix"].read(), f["eigvals"].read().ravel(), f["eigvecs"].read()
+        th, ov = f["theta"].read().ravel(), f["overlaps"].read().ravel()
+    n = A.shape[0]
+    ev, Vd = hb.dense_eig(hb.to_device(np.asfortranarray(A)), n)
+    ev, Vd = ev.cpu().numpy(), hb.to_host(Vd, (n, n))
+    order = np.argsort(w)
+    scale = np.abs(w).max()
+    assert np.max(np.abs(ev - w[order])) <= 1e-13 * scale
+    assert np.max(np.abs(np.abs(Vd.T @ th) - ov[order])) < 1e-10
+    assert np.linalg.norm(A @ Vd - Vd * ev) <= 1e-12 * scale * n
