@@ -10,12 +10,16 @@ The reference can dump the operands of its hot path to HDF5 through h5pp:
   attributes such as ``rank_max``, ``truncation_lim`` and LAPACK's ``info``;
 * the reference's SVD tests and bench read the same layouts: one root dataset ``svdmatrix`` per file
   (tests/svd/main.cpp:69-87, truncation limit 1e-8) and groups ``svd_<...>`` with ``A``, ``U``, ``S``, ``V`` and
-  attributes ``rank_max`` and ``threshold`` (bench/svd/main.cpp:89-108).
+  attributes ``rank_max`` and ``threshold`` (bench/svd/main.cpp:89-108);
+* the reference's eigensolver bench reads ``eigs.h5`` (bench/eig/main.cpp:45-62, 151-160): groups ``eigs-<...>``
+  holding the folded-spectrum local problem of an xDMRG step, ``mps`` (complex; its real part is the initial guess),
+  ``mpo2`` [D, D, spin, spin], ``envL2``, ``envR2`` (float64), with the solve's recorded attributes ``eval`` (the
+  lowest eigenvalue of H^2 found), ``rnorm``, ``iter``, ``mv``, ``op``, ``time``, ``dims`` and ``size``.
 
-``contraction_dumps`` / ``svd_dumps`` read those files with :mod:`dmrg_b200.h5read` (no HDF5 library needed) and
-return host arrays in the reference's column-major layout; ``replay_contractions`` / ``replay_svds`` run every dumped
-operand set through the device kernels (``heff_expval`` + ``heff_matvec``, ``heff_svd``) and return the results,
-next to the dumped reference outputs where the dump holds them.
+``contraction_dumps`` / ``svd_dumps`` / ``eig_dumps`` read those files with :mod:`dmrg_b200.h5read` (no HDF5 library
+needed) and return host arrays in the reference's column-major layout; ``replay_contractions`` / ``replay_svds`` /
+``replay_eigs`` run every dumped problem through the device (``heff_expval`` + ``heff_matvec``, ``heff_svd``, an
+operator + ``heff_eigs``) and return the results next to the dumped reference outputs where the dump holds them.
 """
 import re
 
@@ -23,7 +27,7 @@ import numpy as np
 
 from .h5read import H5Dataset, H5File, H5Group
 
-__all__ = ["contraction_dumps", "svd_dumps", "replay_contractions", "replay_svds"]
+__all__ = ["contraction_dumps", "svd_dumps", "eig_dumps", "replay_contractions", "replay_svds", "replay_eigs"]
 
 
 def _numbered(names, prefix):
@@ -161,4 +165,63 @@ def replay_svds(path, truncation_lim=None, rank_max=None, stream=None):
         if "S" in d and d.get("info", 0) == 0:
             r["reference_S"] = d["S"]
         res.append(r)
+    return res
+
+
+def _attr_value(v):
+    if isinstance(v, np.ndarray):
+        return v.tolist()
+    if isinstance(v, np.generic):
+        return v.item()
+    return v
+
+
+def eig_dumps(path):
+    """Every ``eigs-<...>`` group of an eigensolver bench file: dicts with ``name``, ``mps`` (the dumped state, complex
+    as stored), ``mpo2``, ``envL2``, ``envR2`` (Fortran-ordered float64; the bench reads them as real,
+    bench/eig/main.cpp:59-62) and ``attrs`` (the recorded solve: eval, rnorm, iter, mv, op, time, dims, size).  The
+    operands must form a contraction (contraction_tblis.cpp:56-60), in h5pp's layout or the reversed one."""
+    out = []
+    with H5File(path) as f:
+        for name in _numbered(f.root.keys(), "eigs-"):
+            g = f.root[name]
+            if not isinstance(g, H5Group):
+                continue
+            raw = {"mps": g["mps"].read(), "mpo": g["mpo2"].read(), "envL": g["envL2"].read(), "envR": g["envR2"].read()}
+            ops = {k: np.asfortranarray(v) for k, v in raw.items()}
+            if not _contraction_dims_ok(ops["mps"], ops["mpo"], ops["envL"], ops["envR"]):
+                ops = {k: np.asfortranarray(v.transpose()) for k, v in raw.items()}
+                if not _contraction_dims_ok(ops["mps"], ops["mpo"], ops["envL"], ops["envR"]):
+                    raise ValueError(f"{path}:{name}: operand dimensions do not form a contraction")
+            out.append({"name": name, "mps": ops["mps"], "mpo2": np.asfortranarray(np.real(ops["mpo"]).astype(np.float64)),
+                        "envL2": np.asfortranarray(np.real(ops["envL"]).astype(np.float64)),
+                        "envR2": np.asfortranarray(np.real(ops["envR"]).astype(np.float64)),
+                        "attrs": {k: _attr_value(v) for k, v in g.attrs.items()}})
+    return out
+
+
+def replay_eigs(path, tol=1e-12, precision=None, max_size=None, **eig_kw):
+    """Solves every dumped problem as the reference's eigensolver bench does (bench/eig/main.cpp:64-71, 125-135): the
+    lowest eigenpair (Ritz SA) of the single-MPO operator MatVecMPO(envL2, envR2, mpo2) at tolerance ``tol``, started
+    from the real part of the dumped state, here with the device Davidson solver (heff_eigs).  ``max_size`` skips
+    problems with more rows (the bench skips size > 1024).  Returns dicts with ``name``, ``rows``, ``eigval``,
+    ``reference_eval`` (the dump's ``eval``, when recorded), ``resnorm``, ``num_mv``, ``seconds``, ``converged``."""
+    from . import PREC_FP64, MatVecMPOS, to_device
+
+    res = []
+    for d in eig_dumps(path):
+        rows = int(np.prod(d["mps"].shape))
+        if max_size is not None and rows > max_size:
+            continue
+        op = MatVecMPOS([d["mpo2"]], d["envL2"], d["envR2"], cplx=False, precision=PREC_FP64 if precision is None else precision)
+        try:
+            x0 = to_device(np.asfortranarray(np.real(d["mps"]).astype(np.float64)))
+            ev, r = op.eigs(x0=x0, ritz="SA", tol=tol, **eig_kw)
+        finally:
+            op.close()
+        out = {"name": d["name"], "rows": rows, "eigval": ev, "resnorm": r["resnorm"], "num_mv": r["num_mv"], "seconds": r["seconds"],
+               "converged": bool(r["converged"])}
+        if "eval" in d["attrs"]:
+            out["reference_eval"] = float(d["attrs"]["eval"])
+        res.append(out)
     return res

@@ -218,3 +218,22 @@ def test_svd_dumps_layouts(tmp_path):
     b = replay.svd_dumps(os.path.join(FIXTURES, "svd-failed.h5"))
     assert [x["name"] for x in b] == [f"svd_lapacke_{i}" for i in range(4)]
     assert [x["info"] for x in b] == [1, -13, -13, -13] and b[0]["truncation_lim"] == np.finfo(float).eps
+
+
+def test_eig_dumps_layout(tmp_path):
+    """The eigensolver bench's eigs.h5 layout (bench/eig/main.cpp:45-62): eigs-<n> groups with a complex mps, real
+    mpo2/envL2/envR2 and the recorded solve's attributes."""
+    rng = np.random.default_rng(12)
+    g = contraction_group(rng, 4, 5, 6, 9, False)
+    mps = g["mps"] + 1j * rng.standard_normal(g["mps"].shape)
+    root = {f"eigs-{i}": {"mps": mps, "mpo2": g["mpo"], "envL2": g["envL"], "envR2": g["envR"],
+                          "__attrs__": {"eval": 0.25 * i, "rnorm": 1e-13, "iter": np.int64(40), "mv": np.int64(321),
+                                        "dims": np.array([4, 5, 6], dtype=np.int64), "size": np.int64(120)}} for i in (2, 0, 1)}
+    root["eigs_other"] = {"x": np.zeros(1)}
+    got = replay.eig_dumps(write(tmp_path, root, "eigs.h5"))
+    assert [e["name"] for e in got] == ["eigs-0", "eigs-1", "eigs-2"]
+    for i, e in enumerate(got):
+        assert np.array_equal(e["mps"], mps) and np.array_equal(e["mpo2"], g["mpo"])
+        assert np.array_equal(e["envL2"], g["envL"]) and np.array_equal(e["envR2"], g["envR"])
+        assert e["envL2"].flags.f_contiguous and e["mpo2"].dtype == np.float64
+        assert e["attrs"]["eval"] == 0.25 * i and e["attrs"]["dims"] == [4, 5, 6] and e["attrs"]["mv"] == 321

@@ -22,6 +22,7 @@ import pytest
 import dmrg_b200 as hb
 from dmrg_b200 import replay
 from dmrg_b200.h5read import H5File
+from oracle import physics as ph
 from oracle import ref_numpy as rn
 
 import h5writer
@@ -94,3 +95,47 @@ def test_reference_dense_eigenproblems(cuda, name):
     assert np.max(np.abs(ev - w[order])) <= 1e-13 * scale
     assert np.max(np.abs(np.abs(Vd.T @ th) - ov[order])) < 1e-10
     assert np.linalg.norm(A @ Vd - Vd * ev) <= 1e-12 * scale * n
+
+
+def folded_env(rng, chi, base=3):
+    """Real environment of an MPO squared: slice (m, m~) is the transpose of slice (m~, m), the symmetry the
+    environments of H^2 have, which makes H_eff symmetric for the uncompressed square of a Hermitian MPO."""
+    E = np.zeros((chi, chi, base * base))
+    for m in range(base):
+        for mt in range(m, base):
+            X = rng.standard_normal((chi, chi))
+            if m == mt:
+                X = 0.5 * (X + X.T)
+            E[:, :, m + base * mt] = X
+            E[:, :, mt + base * m] = X.T
+    return np.asfortranarray(E)
+
+
+def test_replay_eigensolver_bench_dump(cuda, tmp_path):
+    """An eigs.h5 in the layout the reference's eigensolver bench reads (bench/eig/main.cpp:45-62): folded local
+    problems (the two-site Ising MPO squared, D=9) at chi 6 x 7 and 10 x 10, each with the lowest eigenvalue of its
+    dense operator recorded as ``eval``.  replay_eigs solves them like the bench (Ritz SA, tol 1e-12, started from the
+    real part of the stored state) on the device and must reach those eigenvalues."""
+    from oracle import clib
+
+    root = {}
+    for i, (cl, cr) in enumerate([(6, 7), (10, 10)]):
+        rng = np.random.default_rng(40 + i)
+        W = ph.ising_two_site_mpo(0.7, 1.3, squared=True)
+        L, R = folded_env(rng, cl), folded_env(rng, cr)
+        mps = rng.standard_normal((4, cl, cr)) + 1j * rng.standard_normal((4, cl, cr))
+        H = clib.dense_heff(mps.shape, W, L, R)
+        assert np.abs(H - H.T).max() < 1e-12 * np.abs(H).max()
+        w = np.linalg.eigvalsh(H)
+        root[f"eigs-{i}"] = {"mps": np.ascontiguousarray(mps), "mpo2": np.ascontiguousarray(W), "envL2": np.ascontiguousarray(L),
+                             "envR2": np.ascontiguousarray(R),
+                             "__attrs__": {"eval": float(w[0]), "size": np.int64(mps.size), "dims": np.array(mps.shape, dtype=np.int64)}}
+    path = str(tmp_path / "eigs.h5")
+    h5writer.write(path, root)
+    res = replay.replay_eigs(path)
+    assert [r["name"] for r in res] == ["eigs-0", "eigs-1"]
+    for r in res:
+        assert r["converged"] and r["num_mv"] > 0
+        assert abs(r["eigval"] - r["reference_eval"]) <= 1e-10 * max(1.0, abs(r["reference_eval"]))
+    small = replay.replay_eigs(path, max_size=300)
+    assert [r["name"] for r in small] == ["eigs-0"]
