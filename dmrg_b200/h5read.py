@@ -290,6 +290,7 @@ class H5File:
         b = self._buf
         a = self.base + addr
         msgs = []
+        seen = set()
         if b[a:a + 4] == b"OHDR":
             c = self._cursor(addr)
             c.skip(4)
@@ -318,6 +319,9 @@ class H5File:
                         cs = self.base + caddr
                         if b[cs:cs + 4] != b"OCHK":
                             raise H5FormatError("continuation block signature")
+                        if cs in seen:
+                            raise H5FormatError("object header continuation cycle")
+                        seen.add(cs)
                         blocks.append((cs + 4, clen - 8))
                     else:
                         msgs.append((mtype, mflags, data))
@@ -342,6 +346,9 @@ class H5File:
                     if mtype == 0x10:
                         cc = _Cursor(data, 0, self.so, self.sl)
                         caddr, clen = cc.off(), cc.length()
+                        if caddr in seen:
+                            raise H5FormatError("object header continuation cycle")
+                        seen.add(caddr)
                         blocks.append((self.base + caddr, clen))
                     msgs.append((mtype, mflags, data))
             msgs = [m for m in msgs if m[0] != 0x10]
