@@ -9,7 +9,10 @@ operands are HDF5 files:
   holding ``A`` (or ``A_real``/``A_cplx``), ``U``, ``S``, ``VT`` and attributes ``rank_max``, ``truncation_lim`` ...;
 * the SVD test matrices of tests/svd/main.cpp:69-87 (one root dataset ``svdmatrix``) and the SVD bench file of
   bench/svd/main.cpp:89-108 (groups ``svd_<n>`` with ``A``, ``U``, ``S``, ``V`` and attributes ``rank_max``,
-  ``threshold``).
+  ``threshold``);
+* the eigensolver bench's ``eigs.h5`` (bench/eig/main.cpp:45-62: groups ``eigs-<n>`` holding ``mps``, ``mpo2``,
+  ``envL2``, ``envR2`` and the recorded solve as attributes) and the dense eigenproblem fixtures
+  tests/testmatrices/lapacke_matrix-*.h5 (``matrix``, ``eigvals``, ``eigvecs``, ``theta``, ``overlaps``).
 
 This module implements the part of the published HDF5 file format (HDF Group, "HDF5 File Format Specification",
 versions 2.0/3.0) those files use: superblocks v0-v3; object headers v1 and v2 with continuation blocks; groups stored
@@ -25,7 +28,6 @@ and ``np.asfortranarray`` of the result is the reference's in-memory layout.
 """
 import mmap
 import os
-import struct
 import zlib
 
 import numpy as np
