@@ -2,7 +2,6 @@
 device driver's index maps): from a random product state the expansion alone grows the bonds, and the sweep reaches
 the exact ground energy (free fermions) of the random-field Ising chain; with a vanishing mixing factor it cannot
 leave the product state."""
-import numpy as np
 
 from oracle import physics as ph
 from oracle import ref_numpy as rn

@@ -5,7 +5,6 @@ import scipy.sparse.linalg as sla
 import torch
 
 import dmrg_b200 as hb
-import oracle
 from oracle import physics as ph
 from oracle import ref_numpy as rn
 

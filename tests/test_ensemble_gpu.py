@@ -4,7 +4,6 @@ Bar: every realisation's energy is the same run alone and in the overlapped ense
 reduce in a fixed order, so in practice bit-identical), and matches exact diagonalisation to 1e-10 where
 chi_max covers the exact Schmidt rank (chi_max >= 2^(L/2)).
 """
-import numpy as np
 import pytest
 
 import dmrg_b200 as hb

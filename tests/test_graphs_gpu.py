@@ -2,7 +2,6 @@
 shape runs as plain launches and is recorded; later products replay the graph with the input and output pointers
 retargeted.  Every product must equal the plain launches' bit for bit, for fresh input/output pairs, across rebinds of
 the shape (sweeps, server arenas), with the tail split of the GEMMs on, and inside eigensolves."""
-import numpy as np
 import pytest
 import torch
 

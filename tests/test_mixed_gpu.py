@@ -7,12 +7,10 @@ FP64 oracle to 1e-4 relative; eigenvalues from mixed solves with FP64 refinement
 """
 import ctypes
 
-import numpy as np
 import pytest
 import torch
 
 import dmrg_b200 as hb
-import oracle
 from oracle import physics as ph
 from oracle import ref_numpy as rn
 

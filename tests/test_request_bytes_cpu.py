@@ -6,7 +6,6 @@ BF16 operands for mixed precision, the INT8 digit planes for the INT8 engine, an
 """
 import ctypes
 
-import numpy as np
 
 import dmrg_b200 as hb
 from dmrg_b200._sigs import Request
