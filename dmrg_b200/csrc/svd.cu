@@ -57,6 +57,7 @@ struct JS<double> {
     __device__ static double absv(double a) { return fabs(a); }
     __device__ static double re(double a) { return a; }
     __device__ static double unit(double a) { return a >= 0 ? 1.0 : -1.0; }
+    __device__ static double unit_r(double a, double) { return a >= 0 ? 1.0 : -1.0; }  // a / |a| given 1 / |a|
     __device__ static double conj(double a) { return a; }
     __device__ static double mul(double a, double b) { return a * b; }
     __device__ static double axpy(double a, double x, double y) { return fma(a, x, y); }  // y + a x, a real
@@ -80,6 +81,7 @@ struct JS<double2> {
         const double r = hypot(a.x, a.y);
         return r > 0 ? make_double2(a.x / r, a.y / r) : make_double2(1.0, 0.0);
     }
+    __device__ static double2 unit_r(double2 a, double rinv) { return make_double2(a.x * rinv, a.y * rinv); }
     __device__ static double2 conj(double2 a) { return make_double2(a.x, -a.y); }
     __device__ static double2 mul(double2 a, double2 b) { return cmul(a, b); }
     __device__ static double2 axpy(double a, double2 x, double2 y) { return make_double2(fma(a, x.x, y.x), fma(a, x.y, y.y)); }
@@ -420,6 +422,125 @@ __global__ void eye_kernel(T *__restrict__ V, int64_t ldv, int npad) {
         V[e] = (e % ldv == e / ldv) ? JS<T>::one() : JS<T>::zero();
 }
 
+// Small matrices (at most 64 padded columns, G and V together in shared memory): one CTA runs the whole cyclic
+// one-sided Jacobi -- every sweep of nc - 1 steps over the nc / 2 disjoint column pairs of the round-robin
+// tournament on the first nc (even) columns, one warp per pair -- with the block path's rotation (Rutishauser form),
+// relative criterion and absolute floor, and no host round trip between sweeps.  On the block path each sweep costs a norm ordering on the host, two
+// synchronisations and B - 1 launches, most of the time of a 64 x 64 split.  G (m x npad, column stride ldg) and V
+// (npad x npad, the identity on entry) are read from and written back to global memory; sweeps_out receives the
+// number of sweeps run (max_sweeps when the last one still rotated).
+constexpr int    JSMALL_THR  = 1024;
+constexpr size_t JSMALL_SMEM = 200 * 1024;
+template<class T>
+static size_t jacobi_small_bytes(int64_t m, int64_t npad) {
+    return (size_t)(m * npad + npad * npad) * sizeof(T);
+}
+template<class T>
+__device__ __forceinline__ T warp_sum(T v);
+template<>
+__device__ __forceinline__ double warp_sum(double v) {
+    for(int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template<>
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+    for(int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+template<class T>
+__global__ void __launch_bounds__(JSMALL_THR, 1) jacobi_small_kernel(T *__restrict__ G, int64_t ldg, int m, T *__restrict__ V, int npad, int nc,
+                                                                    double tol, int max_sweeps, int *__restrict__ sweeps_out) {
+    using S = JS<T>;
+    extern __shared__ __align__(16) unsigned char js_smem[];
+    T *sG = reinterpret_cast<T *>(js_smem);  // m x npad, column-major, column stride m
+    T *sV = sG + (int64_t)m * npad;           // npad x npad, column-major
+    __shared__ double s_norm[64];
+    __shared__ double s_gmax;
+    __shared__ int    s_rot;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for(int64_t e = tid; e < (int64_t)m * npad; e += JSMALL_THR) sG[e] = G[(e % m) + ldg * (e / m)];
+    for(int e = tid; e < npad * npad; e += JSMALL_THR) sV[e] = V[e];
+    const double eps       = 2.220446049250313e-16;
+    double       floor_abs = 0.0;  // first sweep: relative criterion only
+    int          done      = max_sweeps;
+    for(int sweep = 0; sweep < max_sweeps; sweep++) {
+        __syncthreads();  // the previous sweep's flag has been read by every thread
+        if(tid == 0) s_rot = 0;
+        __syncthreads();
+        for(int step = 0; step < nc - 1; step++) {
+            if(warp < nc / 2) {
+                int p, q;
+                rr_pair(nc, step, warp, p, q);
+                T     *gp = sG + (int64_t)m * p, *gq = sG + (int64_t)m * q;
+                double app = 0.0, aqq = 0.0;
+                T      apq = S::zero();
+                for(int i = lane; i < m; i += 32) {
+                    const T x = gp[i], y = gq[i];
+                    app += S::abs2(x);
+                    aqq += S::abs2(y);
+                    apq = S::fma_cj(x, y, apq);  // += conj(x) y
+                }
+                app = warp_sum(app);
+                aqq = warp_sum(aqq);
+                apq = warp_sum(apq);
+                // the block path's criterion |apq| > max(tol sqrt(app aqq), floor, 1e-300) (the first one on squares), and
+                // the rotation with one reciprocal of |apq| shared by the angle and the phase: every step waits on this
+                // chain of reciprocals and square roots
+                const double h = S::absv(apq);
+                if(h > 1e-300 && h > floor_abs && h * h > tol * tol * (app * aqq)) {  // the same value in every lane
+                    const double rh  = 1.0 / h;
+                    const double th  = 0.5 * (aqq - app) * rh;
+                    const double t   = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(fma(th, th, 1.0)));
+                    const double c   = rsqrt(fma(t, t, 1.0));
+                    const double sn  = t * c;
+                    const double tau = sn / (1.0 + c);
+                    const T      ph = S::unit_r(apq, rh), phc = S::conj(ph);
+                    // col_p' = col_p - s (conj(e) col_q + tau col_p), col_q' = col_q + s (e col_p - tau col_q), on G and V
+                    for(int i = lane; i < m; i += 32) {
+                        const T x = gp[i], y = gq[i];
+                        gp[i]     = rot_lo(x, y, phc, sn, tau);
+                        gq[i]     = rot_lo(y, x, ph, -sn, -tau);
+                    }
+                    T *vp = sV + (int64_t)npad * p, *vq = sV + (int64_t)npad * q;
+                    for(int i = lane; i < npad; i += 32) {
+                        const T x = vp[i], y = vq[i];
+                        vp[i]     = rot_lo(x, y, phc, sn, tau);
+                        vq[i]     = rot_lo(y, x, ph, -sn, -tau);
+                    }
+                    if(lane == 0) s_rot = 1;
+                }
+            }
+            __syncthreads();
+        }
+        // squared column norms: their maximum sets the next sweep's absolute floor m eps^2 max ||G_j||^2
+        for(int c = warp; c < nc; c += JSMALL_THR / 32) {
+            double v = 0.0;
+            for(int i = lane; i < m; i += 32) v += S::abs2(sG[(int64_t)m * c + i]);
+            v = warp_sum(v);
+            if(lane == 0) s_norm[c] = v;
+        }
+        __syncthreads();
+        if(tid == 0) {
+            double g = 0.0;
+            for(int c = 0; c < nc; c++) g = fmax(g, s_norm[c]);
+            s_gmax = g;
+        }
+        __syncthreads();
+        if(s_rot == 0) {  // uniform: read after the barrier by every thread
+            done = sweep + 1;
+            break;
+        }
+        floor_abs = (double)m * eps * eps * s_gmax;
+    }
+    __syncthreads();
+    for(int64_t e = tid; e < (int64_t)m * npad; e += JSMALL_THR) G[(e % m) + ldg * (e / m)] = sG[e];
+    for(int e = tid; e < npad * npad; e += JSMALL_THR) V[e] = sV[e];
+    if(tid == 0) *sweeps_out = done;
+}
+
 int &last_svd_sweeps() {
     static thread_local int n = 0;
     return n;
@@ -493,7 +614,27 @@ static int svd_truncated_t(const T *A, int64_t lda, int64_t m, int64_t n, int64_
     // are long enough to share out
     int CL = 1;
     while(CL < 4 && (int64_t)(B / 2) * CL * 2 <= device_sm_count() && m >= 128 * CL * 2) CL *= 2;
-    for(; sweep < JOUTER; sweep++) {
+    const size_t small     = jacobi_small_bytes<T>(m, npad);
+    const bool   use_small = npad <= 64 && small <= JSMALL_SMEM;
+    if(use_small) {
+        static int attr_done[64] = {0};
+        int        dev           = 0;
+        HEFF_CUDA(cudaGetDevice(&dev));
+        if(dev < 0 || dev >= 64 || !attr_done[dev]) {
+            HEFF_CUDA(cudaFuncSetAttribute(jacobi_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JSMALL_SMEM));
+            if(dev >= 0 && dev < 64) attr_done[dev] = 1;
+        }
+        // the tournament runs over the n columns rounded up to even, not over the padding to 32: padded columns are
+        // zero and never rotate
+        const int nc = (int)std::min<int64_t>(npad, (n + 1) / 2 * 2);
+        jacobi_small_kernel<T><<<1, JSMALL_THR, small, s>>>(G, ldg, (int)m, V, npad, nc, tol, JOUTER, drot);
+        HEFF_LAUNCH_CHECK();
+        int ran = 0;
+        HEFF_CUDA(cudaMemcpyAsync(&ran, drot, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HEFF_CUDA(cudaStreamSynchronize(s));
+        sweep = ran - 1;
+    }
+    for(; !use_small && sweep < JOUTER; sweep++) {
         col_norms_kernel<T><<<(npad * 32 + 255) / 256, 256, 0, s>>>(G, ldg, (int)m, npad, sig);
         HEFF_LAUNCH_CHECK();
         HEFF_CUDA(cudaMemcpyAsync(hn.data(), sig, sizeof(double) * npad, cudaMemcpyDeviceToHost, s));
