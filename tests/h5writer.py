@@ -4,7 +4,8 @@ It writes the structures the reference's h5pp dumps contain, following the publi
 superblock v0; groups as symbol tables (v1 B-tree + symbol node + local heap) or, with ``links=True``, as a version-2
 object header holding link messages; datasets in version-1 (or, with ``ohdr_v2=True``, version-2) object headers with
 dataspace v1, float64 / int64 / h5pp complex compound / fixed and variable-length string datatypes, and compact,
-contiguous or chunked (v1 B-tree index, optional shuffle + deflate + fletcher32 filters) layouts; attributes.
+contiguous or chunked (v1 B-tree index, optional shuffle + deflate + fletcher32 filters) layouts through layout
+messages version 1-3, or version 4 with a single-chunk or implicit index; attribute messages version 1-3.
 Checksums of version-2 headers and fletcher32 are written as zeros: the reader under test does not verify them.
 """
 import struct
@@ -104,38 +105,94 @@ class Writer:
             return _int_type(), _dataspace(a.shape), np.ascontiguousarray(a).tobytes()
         raise TypeError(a.dtype)
 
-    def attribute(self, name, value):
+    def attribute(self, name, value, version=1):
+        """Attribute message: version 1 pads name, datatype and dataspace to 8 bytes; 2 does not; 3 adds the name's
+        character-set byte."""
         dt, ds, raw = self.encode(value)
         nm = name.encode() + b"\x00"
-        return struct.pack("<BBHHH", 1, 0, len(nm), len(dt), len(ds)) + _pad8(nm) + _pad8(dt) + _pad8(ds) + raw
+        if version == 1:
+            return struct.pack("<BBHHH", 1, 0, len(nm), len(dt), len(ds)) + _pad8(nm) + _pad8(dt) + _pad8(ds) + raw
+        head = struct.pack("<BBHHH", version, 0, len(nm), len(dt), len(ds)) + (b"\x00" if version == 3 else b"")
+        return head + nm + dt + ds + raw
 
     # --- datasets
-    def dataset(self, value, layout="contiguous", chunk=None, filters=(), attrs=None, ohdr_v2=False):
+    def dataset(self, value, layout="contiguous", chunk=None, filters=(), attrs=None, ohdr_v2=False, layout_version=3, index="btree",
+                attr_version=1):
+        """layout_version 1 or 2: the old layout message (dimensions + element size as 4-byte fields); 3: the
+        default; 4 with index "single" (one chunk, optionally filtered) or "implicit" (unfiltered chunks stored in
+        order), otherwise the v1 B-tree through a version-3 message."""
         dt, ds, raw = self.encode(value)
         shape = np.asarray(value).shape
         esize = len(raw) // max(1, int(np.prod(shape)))
         msgs = [(0x01, 0, ds), (0x03, 1, dt)]
-        if layout == "compact":
+        dims4 = b"".join(struct.pack("<I", d) for d in list(shape) + [esize])
+        if layout in ("compact", "contiguous") and layout_version in (1, 2):
+            cls = 0 if layout == "compact" else 1
+            body = bytes([layout_version, len(shape) + 1, cls]) + bytes(5)
+            if cls == 1:
+                body += struct.pack("<Q", self.alloc(raw)) + dims4
+            else:
+                body += dims4 + struct.pack("<I", len(raw)) + raw
+            msgs.append((0x08, 0, body))
+        elif layout == "compact":
             msgs.append((0x08, 0, bytes([3, 0]) + struct.pack("<H", len(raw)) + raw))
         elif layout == "contiguous":
             addr = self.alloc(raw)
             msgs.append((0x08, 0, bytes([3, 1]) + struct.pack("<QQ", addr, len(raw))))
+        elif layout_version == 4 and index in ("single", "implicit"):
+            chunk = list(chunk)
+            cdims = b"".join(struct.pack("<I", c) for c in chunk + [esize])
+            if index == "single":
+                assert list(chunk) == list(shape), "a single chunk covers the dataset"
+                payload = raw
+                for f in filters:
+                    if f == "shuffle" and esize > 1:
+                        payload = np.frombuffer(payload, np.uint8).reshape(-1, esize).T.tobytes()
+                    elif f == "deflate":
+                        payload = zlib.compress(payload, 6)
+                if filters:
+                    msgs.append((0x0B, 0, self.filter_pipeline(filters, esize)))
+                addr = self.alloc(payload)
+                flags = 0x02 if filters else 0
+                body = bytes([4, 2, flags, len(shape) + 1, 4]) + cdims + bytes([1])
+                if filters:
+                    body += struct.pack("<QI", len(payload), 0)
+                msgs.append((0x08, 0, body + struct.pack("<Q", addr)))
+            else:
+                assert not filters, "implicit indices hold unfiltered chunks"
+                full = np.frombuffer(raw, np.uint8).reshape(tuple(shape) + (esize,))
+                grid = [-(-d // c) for d, c in zip(shape, chunk)]
+                blob = b""
+                for idx in np.ndindex(*grid):
+                    offs = [i * c for i, c in zip(idx, chunk)]
+                    blk = np.zeros(tuple(chunk) + (esize,), np.uint8)
+                    src = tuple(slice(o, min(o + c, d)) for o, c, d in zip(offs, chunk, shape))
+                    blk[tuple(slice(0, sl.stop - sl.start) for sl in src)] = full[src]
+                    blob += blk.tobytes()
+                addr = self.alloc(blob)
+                msgs.append((0x08, 0, bytes([4, 2, 0, len(shape) + 1, 4]) + cdims + bytes([2]) + struct.pack("<Q", addr)))
         else:
-            fl = b""
-            for f in filters:
-                vals = {"shuffle": [esize], "deflate": [6], "fletcher32": []}[f]
-                fid = {"deflate": 1, "shuffle": 2, "fletcher32": 3}[f]
-                fl += struct.pack("<HHHH", fid, 0, 0, len(vals)) + b"".join(struct.pack("<I", v) for v in vals)
-                if len(vals) % 2:
-                    fl += bytes(4)
             if filters:
-                msgs.append((0x0B, 0, bytes([1, len(filters)]) + bytes(6) + fl))
+                msgs.append((0x0B, 0, self.filter_pipeline(filters, esize)))
             btree = self.chunk_btree(np.asarray(value), raw, esize, chunk, filters)
-            msgs.append((0x08, 0, bytes([3, 2, len(shape) + 1]) + struct.pack("<Q", btree)
-                         + b"".join(struct.pack("<I", c) for c in chunk) + struct.pack("<I", esize)))
+            if layout_version in (1, 2):
+                body = bytes([layout_version, len(shape) + 1, 2]) + bytes(5) + struct.pack("<Q", btree)
+            else:
+                body = bytes([3, 2, len(shape) + 1]) + struct.pack("<Q", btree)
+            msgs.append((0x08, 0, body + b"".join(struct.pack("<I", c) for c in chunk) + struct.pack("<I", esize)))
         for k, v in (attrs or {}).items():
-            msgs.append((0x0C, 0, self.attribute(k, v)))
+            msgs.append((0x0C, 0, self.attribute(k, v, attr_version)))
         return self.ohdr_v2(msgs) if ohdr_v2 else self.ohdr_v1(msgs)
+
+    def filter_pipeline(self, filters, esize):
+        fl = b""
+        for f in filters:
+            vals = {"shuffle": [esize], "deflate": [6], "fletcher32": []}[f]
+            fid = {"deflate": 1, "shuffle": 2, "fletcher32": 3}[f]
+            fl += struct.pack("<HHHH", fid, 0, 0, len(vals)) + b"".join(struct.pack("<I", v) for v in vals)
+            if len(vals) % 2:
+                fl += bytes(4)
+        return bytes([1, len(filters)]) + bytes(6) + fl
 
     def chunk_btree(self, a, raw, esize, chunk, filters):
         shape = a.shape

@@ -237,3 +237,32 @@ def test_eig_dumps_layout(tmp_path):
         assert np.array_equal(e["envL2"], g["envL"]) and np.array_equal(e["envR2"], g["envR"])
         assert e["envL2"].flags.f_contiguous and e["mpo2"].dtype == np.float64
         assert e["attrs"]["eval"] == 0.25 * i and e["attrs"]["dims"] == [4, 5, 6] and e["attrs"]["mv"] == 321
+
+
+def test_layout_and_attribute_message_versions(tmp_path):
+    """Layout messages version 1/2 (compact, contiguous, chunked) and version 4 (single chunk, filtered or not;
+    implicit index), and attribute messages version 2 and 3: each read back exactly."""
+    rng = np.random.default_rng(21)
+    X = rng.standard_normal((9, 7))
+    Z = rng.standard_normal((6, 5)) + 1j * rng.standard_normal((6, 5))
+    root = {
+        "v1_contig": {"__data__": X, "__layout_version__": 1},
+        "v2_compact": {"__data__": X[:2], "__layout__": "compact", "__layout_version__": 2},
+        "v1_chunked": {"__data__": Z, "__layout__": "chunked", "__chunk__": (4, 2), "__layout_version__": 1, "__filters__": ("deflate",)},
+        "v4_single": {"__data__": X, "__layout__": "chunked", "__chunk__": X.shape, "__layout_version__": 4, "__index__": "single"},
+        "v4_single_f": {"__data__": Z, "__layout__": "chunked", "__chunk__": Z.shape, "__layout_version__": 4, "__index__": "single",
+                        "__filters__": ("shuffle", "deflate")},
+        "v4_implicit": {"__data__": X, "__layout__": "chunked", "__chunk__": (4, 3), "__layout_version__": 4, "__index__": "implicit"},
+        "attrs_v2": {"__data__": np.zeros(1), "__attrs__": {"rank_max": np.int64(7), "svd_lib": "lapacke"}, "__attr_version__": 2},
+        "attrs_v3": {"__data__": np.zeros(1), "__attrs__": {"threshold": 1e-12, "dims": np.array([4, 5, 6])}, "__attr_version__": 3},
+    }
+    with H5File(write(tmp_path, root)) as f:
+        assert np.array_equal(f["v1_contig"].read(), X)
+        assert np.array_equal(f["v2_compact"].read(), X[:2])
+        assert np.array_equal(f["v1_chunked"].read(), Z)
+        assert np.array_equal(f["v4_single"].read(), X)
+        assert np.array_equal(f["v4_single_f"].read(), Z)
+        assert np.array_equal(f["v4_implicit"].read(), X)
+        assert f["attrs_v2"].attrs == {"rank_max": 7, "svd_lib": "lapacke"}
+        a3 = f["attrs_v3"].attrs
+        assert a3["threshold"] == 1e-12 and np.array_equal(a3["dims"], [4, 5, 6])
