@@ -428,6 +428,52 @@ def measure_svd(hb, torch, chis=(512, 1024), reps=3):
     return out
 
 
+def measure_svd_reference_matrices(hb, torch, reps=5):
+    """The device SVD on the reference's own SVD inputs: the HDF5 test matrices of tests/svd/main.cpp:69-87 (normalised
+    complex two-site states, truncation limit 1e-8) and the SVD bench's matrices (bench/svd/main.cpp:89-108, their
+    rank_max and threshold), committed under tests/golden/reference_h5 and read through dmrg_b200.replay.  Per matrix:
+    the median of `reps` device SVDs (heff_svd_z / heff_svd_d, host-synchronised) against LAPACK gesdd through numpy
+    on the host cores with the same rank rule; ranks and singular values compared."""
+    import glob
+
+    from dmrg_b200 import replay
+
+    rows = []
+    files = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "reference_h5", "svd*.h5")))
+    for path in files:
+        for d in replay.svd_dumps(path):
+            A = np.asfortranarray(d["A"].astype(np.complex128 if np.iscomplexobj(d["A"]) else np.float64))
+            m, n = A.shape
+            rmax, lim = d["rank_max"], d["truncation_lim"]
+            Ad = hb.to_device(A)
+            hb.svd(Ad, m, n, rmax, lim)
+            torch.cuda.synchronize()
+            tg = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                U, S, VT, k, err = hb.svd(Ad, m, n, rmax, lim)
+                torch.cuda.synchronize()
+                tg.append(time.perf_counter() - t0)
+            tc = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                Sc = np.linalg.svd(A, compute_uv=False)  # LAPACK ?gesdd
+                kc, _ = truncation_rank(Sc[np.nonzero(Sc)], rmax, lim)
+                tc.append(time.perf_counter() - t0)
+            Sg = S.cpu().numpy()
+            rows.append({"name": f"{os.path.basename(path)}:{d['name']}", "shape": [m, n], "rank": k, "rank_gesdd": kc,
+                         "gpu_ms": 1e3 * statistics.median(tg), "gesdd_ms": 1e3 * statistics.median(tc),
+                         "max_sigma_err_rel": float(np.max(np.abs(Sg[:min(k, kc)] - Sc[:min(k, kc)])) / Sc[0]) if min(k, kc) else 0.0})
+            del Ad, U, S, VT
+    g = [r["gpu_ms"] for r in rows]
+    c = [r["gesdd_ms"] for r in rows]
+    return {"matrices": len(rows), "ranks_equal": all(r["rank"] == r["rank_gesdd"] for r in rows),
+            "max_sigma_err_rel": max(r["max_sigma_err_rel"] for r in rows), "gpu_ms_median": statistics.median(g),
+            "gesdd_ms_median": statistics.median(c), "per_matrix": rows,
+            "workload": "the reference's SVD test and bench matrices (HDF5, 2x8 .. 138x90, complex and real), their truncation "
+                        "limits and rank limits; device one-sided Jacobi vs numpy gesdd on the host cores"}
+
+
 def measure_eigs_folded(hb, torch, chi=512):
     """Eigensolves at the excited-state configuration's shape: real H_eff with the merged uncompressed MPO squared
     (D=9) at chi_max=512, environments with the MPO-squared swap symmetry (generated on the device), lowest
@@ -769,6 +815,10 @@ def main():
         del gflush
         torch.cuda.empty_cache()
         extras["svd"] = measure_svd(hb, torch)
+        try:
+            extras["svd_reference_matrices"] = measure_svd_reference_matrices(hb, torch)
+        except Exception as e:  # a measurement extra never takes the headline line down
+            extras["svd_reference_matrices"] = {"error": f"{type(e).__name__}: {e}"}
 
     tot_ms, e2e_t = reduce_max_over_ranks([sum(step_ms), statistics.median(t_e2e)], dist)
     ms_per_step = tot_ms / args.steps
