@@ -486,11 +486,11 @@ __global__ void __launch_bounds__(JSMALL_THR, 1) jacobi_small_kernel(T *__restri
                 app = warp_sum(app);
                 aqq = warp_sum(aqq);
                 apq = warp_sum(apq);
-                // the block path's criterion |apq| > max(tol sqrt(app aqq), floor, 1e-300) (the first one on squares), and
-                // the rotation with one reciprocal of |apq| shared by the angle and the phase: every step waits on this
-                // chain of reciprocals and square roots
+                // the block path's criterion |apq| > max(tol sqrt(app aqq), floor, 1e-300), in the same form (squaring |apq|
+                // would underflow for entries below ~1e-81), and the rotation with one reciprocal of |apq| shared by the
+                // angle and the phase: every step waits on this chain of reciprocals and square roots
                 const double h = S::absv(apq);
-                if(h > 1e-300 && h > floor_abs && h * h > tol * tol * (app * aqq)) {  // the same value in every lane
+                if(h > 1e-300 && h > floor_abs && h > tol * sqrt(app * aqq)) {  // the same value in every lane
                     const double rh  = 1.0 / h;
                     const double th  = 0.5 * (aqq - app) * rh;
                     const double t   = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(fma(th, th, 1.0)));
