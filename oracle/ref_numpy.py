@@ -349,3 +349,60 @@ def gauss_jordan_inverse(A, floor_rel=1e-14):
         if p != k:
             A[:, [k, p]] = A[:, [p, k]]
     return A, floored
+
+
+def round_robin_pair(n, step, k):
+    """Pair k of step `step` in the circle-method tournament over n (even) columns: every pair once per n - 1 steps."""
+    if k == 0:
+        return n - 1, step
+    return (step + k) % (n - 1), (step - k + (n - 1)) % (n - 1)
+
+
+def jacobi_small_model(A, max_sweeps=60):
+    """Host model of the single-CTA one-sided Jacobi SVD (jacobi_small_kernel) in its index maps: the columns padded
+    to a multiple of 32 (zeros), the tournament over the n columns rounded up to even, steps of disjoint pairs; per
+    pair the squared norms app, aqq and apq = a_p^H a_q, skipped unless |apq| > max(1e-300, floor,
+    tol sqrt(app aqq)) with tol = max(1e-14, 8 eps sqrt(m)) and floor = m eps^2 max ||G_j||^2 of the previous sweep
+    (0 in the first); else the Rutishauser-form rotation col_p' = col_p - s (conj(e) col_q + tau col_p),
+    col_q' = col_q + s (e col_p - tau col_q) with e = apq / |apq|, applied to G and V; sweeps until one rotates
+    nothing.  Returns (sigma descending over min(m, n), G, V, sweeps run)."""
+    m, n = A.shape
+    npad = (n + 31) // 32 * 32
+    nc = min(npad, (n + 1) // 2 * 2)
+    cplx = np.iscomplexobj(A)
+    G = np.zeros((m, npad), dtype=np.complex128 if cplx else np.float64)
+    G[:, :n] = A
+    V = np.eye(npad, dtype=G.dtype)
+    eps = 2.220446049250313e-16
+    tol = max(1e-14, 8.0 * eps * np.sqrt(m))
+    floor = 0.0
+    sweeps = max_sweeps
+    for sweep in range(max_sweeps):
+        rotated = False
+        for step in range(nc - 1):
+            for k in range(nc // 2):
+                p, q = round_robin_pair(nc, step, k)
+                x, y = G[:, p].copy(), G[:, q].copy()
+                app, aqq, apq = np.vdot(x, x).real, np.vdot(y, y).real, np.vdot(x, y)
+                h = abs(apq)
+                if h > 1e-300 and h > floor and h > tol * np.sqrt(app * aqq):
+                    th = 0.5 * (aqq - app) / h
+                    t = (1.0 if th >= 0 else -1.0) / (abs(th) + np.sqrt(1.0 + th * th))
+                    c = 1.0 / np.sqrt(1.0 + t * t)
+                    s = t * c
+                    tau = s / (1.0 + c)
+                    e = apq / h
+                    ec = np.conj(e)
+                    G[:, p] = x - s * (ec * y + tau * x)
+                    G[:, q] = y + s * (e * x - tau * y)
+                    vx, vy = V[:, p].copy(), V[:, q].copy()
+                    V[:, p] = vx - s * (ec * vy + tau * vx)
+                    V[:, q] = vy + s * (e * vx - tau * vy)
+                    rotated = True
+        gmax = float(np.max(np.sum(np.abs(G[:, :nc]) ** 2, axis=0)))
+        if not rotated:
+            sweeps = sweep + 1
+            break
+        floor = m * eps * eps * gmax
+    sig = np.sort(np.linalg.norm(G, axis=0))[::-1]
+    return sig[: min(m, n)], G, V, sweeps
